@@ -1,0 +1,309 @@
+"""Benchmark: extend + shadow ray throughput of the wavefront path tracer on
+the traversal-throughput scene (64 level-5 icospheres, 1,310,720 triangles),
+16M closest-hit rays + 16M Light::Visible shadow queries per step per GPU.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl crt|reference]
+
+* value   : (extend + shadow rays) / s over all ranks, device-resident
+            inputs, CUDA events on the launching stream, max over ranks.
+* e2e     : the same through the public host-buffer API (crt_trace_closest
+            / crt_trace_shadow on pinned host arrays; copies inside).
+* roofline: the extend kernel (the dominant launch), 48 algorithmic bytes
+            per ray (32 B ray in + 16 B hit out) over its event-timed
+            duration, against the measured HBM copy bandwidth.
+* cpu_baseline: the reference's own BVH traversal and visibility test
+            (oracle/_ref, host-compiled) on the host cores, bounded sample.
+--impl reference runs that reference CPU implementation as the timed arm.
+Multi-GPU: one process per GPU (torchrun), each traces its own batch
+(weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_RAYS = 16 << 20
+EXTEND_BYTES = 48  # per ray: 32 B in + 16 B hit out
+SHADOW_BYTES = 49  # per query: 48 B in + 1 B out
+METRIC = "extend+shadow Mrays/s (icosphere field 1.31M tris, 16M+16M rays/GPU)"
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the extend kernel from the committed ncu
+    summary (profiles/extend_icospheres_ncu.md), or None."""
+    p = os.path.join(ROOT, "profiles", "extend_icospheres_ncu.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_bytes_per_launch_16M:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpus):
+        self.gpus = set(gpus)
+        self.proc = None
+        self.path = os.path.join("/tmp", f"crt_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9 or not c[0].isdigit() or int(c[0]) not in self.gpus:
+                continue
+            try:
+                sm.append(float(c[1]))
+                smax.append(float(c[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def reference_cpu(tris, rays, queries, threads):
+    """Times the reference's host-compiled traversal (oracle/_ref) or, if it
+    is absent, reports None. Returns (Mrays/s, seconds, kind)."""
+    import oracle
+
+    if not oracle.ref_available():
+        return None
+    ref = oracle.RefScene(tris)
+    t0 = time.perf_counter()
+    ref.trace_closest(rays, threads)
+    ref.visible(queries, threads)
+    dt = time.perf_counter() - t0
+    ref.close()
+    return (len(rays) + len(queries)) / dt / 1e6, dt
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU implementation of the path
+    (rank 0 only), on the same scene, metric and unit."""
+    if rank != 0:
+        return
+    import oracle
+    from cudaraytracer_b200 import scenes
+
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcrtref.so not built (needs the reference tree)"}))
+        return
+    threads = os.cpu_count() or 1
+    tris = scenes.icosphere_field(with_env=False).triangles()
+    n_ext, n_sh = 4 << 20, 1 << 20
+    rays = scenes.random_rays(tris, n_ext, seed=5)
+    q = scenes.random_shadow_queries(tris, n_sh, seed=6)
+    ref = oracle.RefScene(tris)
+    for _ in range(args.warmup):
+        ref.trace_closest(rays[: 1 << 18], threads)
+        ref.visible(q[: 1 << 16], threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref.trace_closest(rays, threads)
+        ref.visible(q, threads)
+        times.append(time.perf_counter() - t0)
+    ref.close()
+    dt = sum(times)
+    value = args.steps * (n_ext + n_sh) / dt / 1e6
+    sample = f"{n_ext} extend rays + {n_sh} shadow queries per step (bounded sample of the 16M+16M batch)"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "icosphere field 1.31M tris; extend + shadow rays", "threads": threads},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="crt", choices=["crt", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank, local_rank, world = dist_env()
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from cudaraytracer_b200 import Context, Scene, scenes
+
+    tris = scenes.icosphere_field(with_env=False).triangles()
+    rays_np = scenes.random_rays(tris, N_RAYS, seed=5 + rank)
+    q_np = scenes.random_shadow_queries(tris, N_RAYS, seed=1005 + rank)
+    ctx = Context(local_rank)
+    scene = Scene.from_triangles(ctx, tris)
+    info = scene.info()
+    dev = torch.device("cuda", local_rank)
+    rays = torch.from_numpy(rays_np).to(dev)
+    qs = torch.from_numpy(q_np).to(dev)
+    hits = torch.empty((N_RAYS, 4), dtype=torch.float32, device=dev)
+    occ = torch.empty((N_RAYS,), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        scene.trace_closest(rays, hits)
+        scene.trace_shadow(qs, occ)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(range(world) if world > 1 else [local_rank]) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        scene.trace_closest(rays, hits)
+        ev[k][1].record(stream)
+        scene.trace_shadow(qs, occ)
+        ev[k][2].record(stream)
+    torch.cuda.synchronize()
+    ext_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
+    sh_ms = sum(e[1].elapsed_time(e[2]) for e in ev)
+    total_ms = ev[0][0].elapsed_time(ev[-1][2])
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    clocks = sampler.stop() if sampler else None
+
+    # e2e through the host-buffer API: pinned host inputs, results back.
+    pin_r = torch.from_numpy(rays_np).pin_memory()
+    pin_q = torch.from_numpy(q_np).pin_memory()
+    pin_h = torch.empty((N_RAYS, 4), dtype=torch.float32).pin_memory()
+    pin_o = torch.empty((N_RAYS,), dtype=torch.uint8).pin_memory()
+    rn, qn, hn, on = pin_r.numpy(), pin_q.numpy(), pin_h.numpy(), pin_o.numpy()
+    e2e_steps = max(2, min(args.steps, 5))
+    scene.trace_closest(rn, hn)
+    scene.trace_shadow(qn, on)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        scene.trace_closest(rn, hn)
+        scene.trace_shadow(qn, on)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_val = world * e2e_steps * 2 * N_RAYS / e2e_s / 1e6
+
+    if rank == 0:
+        value = world * args.steps * 2 * N_RAYS / (total_ms * 1e-3) / 1e6
+        peak, peak_kind = measured_peaks()
+        ext_launch_ms = ext_ms / args.steps
+        achieved = EXTEND_BYTES * N_RAYS / (ext_launch_ms * 1e-3) / 1e9
+        traffic = profiled_traffic()
+        cpu = None
+        if not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            n_ext, n_sh = 4 << 20, 1 << 20
+            r = reference_cpu(tris, rays_np[:n_ext], q_np[:n_sh], threads)
+            if r is not None:
+                cpu = {"value": round(r[0], 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                       "sample": f"{n_ext} extend rays + {n_sh} shadow queries of the same batch, "
+                                 f"{r[1]:.1f} s of CPU work on {threads} threads"}
+        out = {
+            "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "icosphere field (64 x level-5 icospheres, 1,310,720 tris); per GPU and step "
+                                   "16M closest-hit rays + 16M shadow queries",
+                       "l2": "inputs 1.28 GB per step > 126 MB L2 (no flush needed)",
+                       "bvh_nodes": info["num_bvh_nodes"], "bvh_depth": info["bvh_depth"],
+                       "bvh_build_ms": round(info["build_ms"], 2), "parallelism": f"replicas x{world}"},
+            "extend_ms_per_launch": round(ext_launch_ms, 4),
+            "shadow_ms_per_launch": round(sh_ms / args.steps, 4),
+            "extend_mrays_s": round(N_RAYS / (ext_launch_ms * 1e-3) / 1e6, 1),
+            "shadow_mrays_s": round(N_RAYS / (sh_ms / args.steps * 1e-3) / 1e6, 1),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4),
+                         "traffic": None if traffic is None else round(traffic),
+                         "peak_kind": peak_kind, "kernel": "k_trace_closest (extend)",
+                         "algorithmic_bytes_per_launch": EXTEND_BYTES * N_RAYS},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_val, 2), "unit": "Mrays/s",
+                    "h2d_bytes_per_step": N_RAYS * (32 + 48), "d2h_bytes_per_step": N_RAYS * (16 + 1)},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(out))
+    del scene
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

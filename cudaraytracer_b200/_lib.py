@@ -1,0 +1,116 @@
+"""ctypes binding of libcrt.so (the C ABI declared in include/crt.h).
+
+The CUDA extension is the product path: there is no CPU fallback. Loading
+fails loudly if libcrt.so is missing, and every call raises CrtError when the
+library returns a non-zero crt_status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcrt.so")
+
+STATUS = {
+    0: "CRT_OK",
+    1: "CRT_ERR_INVALID",
+    2: "CRT_ERR_IO",
+    3: "CRT_ERR_PARSE",
+    4: "CRT_ERR_CUDA",
+    5: "CRT_ERR_OOM",
+    6: "CRT_ERR_CAPACITY",
+    7: "CRT_ERR_TIMEOUT",
+}
+
+
+class CrtError(RuntimeError):
+    """A crt_* call returned a non-zero status."""
+
+    def __init__(self, status: int, func: str, message: str):
+        self.status = status
+        self.code = STATUS.get(status, str(status))
+        super().__init__(f"{func}: {self.code}: {message}")
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [
+        ("num_triangles", C.c_int64),
+        ("num_bvh_nodes", C.c_int64),
+        ("bvh_depth", C.c_int32),
+        ("num_meshes", C.c_int32),
+        ("num_materials", C.c_int32),
+        ("num_lights", C.c_int32),
+        ("bounds_min", C.c_float * 3),
+        ("bounds_max", C.c_float * 3),
+        ("build_ms", C.c_float),
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("spp", C.c_int32),
+        ("max_bounces", C.c_int32),
+        ("rr", C.c_float),
+        ("fovy", C.c_float),
+        ("denoise", C.c_int32),
+        ("has_env", C.c_int32),
+    ]
+
+
+def build(force: bool = False) -> None:
+    """Compiles libcrt.so in-tree with nvcc for sm_100a (make in csrc/)."""
+    csrc = os.path.join(_HERE, "csrc")
+    cmd = ["make", "-C", csrc, "-j", str(max(1, os.cpu_count() or 1))]
+    if force:
+        subprocess.run(["make", "-C", csrc, "clean"], check=True, capture_output=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("building libcrt.so failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
+
+
+_lib = None
+_lock = threading.Lock()
+
+_VP = C.c_void_p
+_SIGS = {
+    "crt_create": (C.c_int, [C.c_int, C.POINTER(_VP)]),
+    "crt_destroy": (None, [_VP]),
+    "crt_last_error": (C.c_char_p, []),
+    "crt_version": (C.c_char_p, []),
+    "crt_scene_from_triangles": (C.c_int, [_VP, _VP, C.c_int64, C.POINTER(_VP)]),
+    "crt_scene_free": (None, [_VP]),
+    "crt_scene_info": (C.c_int, [_VP, C.POINTER(SceneInfo)]),
+    "crt_trace_closest": (C.c_int, [_VP, _VP, C.c_int64, _VP]),
+    "crt_trace_closest_device": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
+    "crt_trace_shadow": (C.c_int, [_VP, _VP, C.c_int64, _VP]),
+    "crt_trace_shadow_device": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
+}
+
+
+def lib() -> C.CDLL:
+    """Loads libcrt.so (raises if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: run cudaraytracer_b200._lib.build() "
+                    "(or __graft_entry__.build()); there is no CPU fallback"
+                )
+            L = C.CDLL(LIB_PATH)
+            for name, (res, args) in _SIGS.items():
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+            _lib = L
+        return _lib
+
+
+def check(status: int, func: str) -> None:
+    if status != 0:
+        msg = lib().crt_last_error()
+        raise CrtError(status, func, msg.decode() if msg else "")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib(), name)(*args), name)

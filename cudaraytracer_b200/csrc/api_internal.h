@@ -1,0 +1,59 @@
+// Internal definitions behind the opaque handles of include/crt.h.
+#pragma once
+#include "common.cuh"
+#include "bvh_build.h"
+#include "trace.cuh"
+#include <new>
+#include <exception>
+
+namespace crt {
+
+// Device buffer that only grows.
+struct DeviceScratch {
+    void *p = nullptr;
+    size_t cap = 0;
+    void reserve(size_t bytes);
+    ~DeviceScratch();
+};
+
+// Runs f and maps exceptions to a crt_status + last-error message.
+template <class F>
+crt_status guard(F &&f) {
+    try {
+        f();
+        set_last_error("");
+        return CRT_OK;
+    } catch (const Error &e) {
+        set_last_error(e.what());
+        return e.status;
+    } catch (const std::bad_alloc &) {
+        set_last_error("host allocation failed");
+        return CRT_ERR_OOM;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return CRT_ERR_INVALID;
+    }
+}
+
+struct Scene;
+
+}  // namespace crt
+
+struct crt_ctx {
+    int device = 0;
+    cudaStream_t streams[2] = {nullptr, nullptr};
+    cudaStream_t stream = nullptr;
+    crt::DeviceScratch stage[2];
+};
+
+namespace crt {
+struct Scene {
+    crt_ctx *ctx = nullptr;
+    float *d_verts = nullptr;
+    BvhBuffers bvh;
+    virtual ~Scene();
+    virtual void fill_info(crt_scene_info_t &) const {}
+};
+}  // namespace crt
+
+struct crt_scene : crt::Scene {};

@@ -1,0 +1,153 @@
+// BVH layout and traversal shared by the extend, shadow and shade kernels.
+//
+// Layout in HBM (all 16-byte aligned, read with 128-bit __ldg loads):
+//   nodes: 64 B per interior node, the boxes of BOTH children in the parent so
+//          one node fetch (4 x float4) decides the whole step:
+//            [0] c0.lo.x c0.hi.x c0.lo.y c0.hi.y
+//            [1] c1.lo.x c1.hi.x c1.lo.y c1.hi.y
+//            [2] c0.lo.z c0.hi.z c1.lo.z c1.hi.z
+//            [3] link0 link1 (int bits) , 0, 0
+//          link >= 0 : interior node index
+//          link <  0 : leaf, ~((first << 4) | count), count in [0, 15]
+//   tris:  48 B per triangle in leaf order: v0 (w = original primitive index
+//          as int bits), v1, v2. Edges are formed in-kernel exactly as the
+//          reference does (e1 = v1 - v0, Src/Core/triangle.cu:102-103), so
+//          the stored vertices give bit-identical arithmetic.
+// The reference node is a 32 B {triIndex, count/right, Bounds3D} with the
+// child boxes stored in the children (Src/Core/bvh.h:25-33) and a 176 B AoS
+// triangle (Src/Core/triangle.h:43-57).
+#pragma once
+#include "common.cuh"
+#include <limits.h>
+
+namespace crt {
+
+constexpr int kLeafMaxCount = 15;
+constexpr int kStackSize = 64;
+constexpr int kSentinel = INT_MIN;  // never a valid link: first < 2^27 - 1
+constexpr float kTriTMax = 1e8f;    // Triangle::IsIntersect default tMax
+
+struct BvhView {
+    const float4 *nodes;  // 4 float4 per node
+    const float4 *tris;   // 3 float4 per triangle
+    int num_tris;
+};
+
+__host__ __device__ __forceinline__ int leaf_link(int first, int count) { return ~((first << 4) | count); }
+
+#ifdef __CUDACC__
+
+struct Hit {
+    float t;
+    int slot;  // triangle slot in leaf order (-1 = miss)
+    float b1, b2;
+};
+
+// Triangle::IsIntersect (Src/Core/triangle.cu:100-133) with tMin = 0 and
+// tMax = 1e8 as BVH::IsIntersect passes them (Src/Core/bvh.cu:271):
+// back faces culled (det <= 0), reciprocal of the determinant correctly
+// rounded (the reference divides 1.f by a double and rounds to float, which
+// is the same value), strict t < closest so ties keep the first triangle
+// visited. Returns true and updates `hit` when accepted.
+__device__ __forceinline__ bool intersect_triangle(V3 o, V3 d, float4 a, float4 b, float4 c,
+                                                   int slot, Hit &hit) {
+    V3 v0 = v3(a.x, a.y, a.z);
+    V3 e1 = vsub(v3(b.x, b.y, b.z), v0);
+    V3 e2 = vsub(v3(c.x, c.y, c.z), v0);
+    V3 s = vsub(o, v0);
+    V3 s1 = vcross(d, e2);
+    V3 s2 = vcross(s, e1);
+    float det = vdot(e1, s1);
+    if (det == 0.f || det < 0.f) return false;
+    float inv = rrcp(det);
+    float t = rmul(inv, vdot(s2, e2));
+    if (t >= hit.t) return false;
+    float b1 = rmul(inv, vdot(s1, s));
+    if (b1 < 0.f || b1 > 1.f) return false;
+    float b2 = rmul(inv, vdot(s2, d));
+    if (b2 < 0.f || radd(b1, b2) > 1.f) return false;
+    if (t < 0.f || t > kTriTMax) return false;
+    hit.t = t;
+    hit.slot = slot;
+    hit.b1 = b1;
+    hit.b2 = b2;
+    return true;
+}
+
+// Conservative slab test of one child box. Returns entry distance in `tnear`.
+// lo/hi include the ray interval [tmin, closest]; the padding keeps the test
+// conservative against rounding so a different tree cannot cull the box of
+// the reference's closest triangle.
+__device__ __forceinline__ bool slab(float lox, float hix, float loy, float hiy, float loz, float hiz,
+                                     V3 o, V3 inv, float tmin, float tmax, float &tnear) {
+    float tx0 = (lox - o.x) * inv.x, tx1 = (hix - o.x) * inv.x;
+    float ty0 = (loy - o.y) * inv.y, ty1 = (hiy - o.y) * inv.y;
+    float tz0 = (loz - o.z) * inv.z, tz1 = (hiz - o.z) * inv.z;
+    float lo = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+    float hi = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+    tnear = lo;
+    return lo <= hi * 1.00000095f;
+}
+
+// Closest hit with the reference's semantics (BVH::IsIntersect,
+// Src/Core/bvh.cu:253-306): boxes pruned by [tmin, closest], triangles
+// accepted on [0, 1e8] with closest initialised to tmax. When t_exit > 0 the
+// traversal stops at the first accepted hit with t < t_exit (used by the
+// shadow predicate, whose answer is fixed once such a hit exists).
+template <bool kEarlyExit>
+__device__ __forceinline__ Hit closest_hit(const BvhView &bvh, V3 o, V3 d, float tmin, float tmax,
+                                           float t_exit = 0.f) {
+    Hit hit;
+    hit.t = tmax;
+    hit.slot = -1;
+    hit.b1 = hit.b2 = 0.f;
+    V3 inv = v3(rrcp(d.x), rrcp(d.y), rrcp(d.z));
+    int stack[kStackSize];
+    int sp = 0;
+    stack[sp++] = kSentinel;
+    int link = 0;  // root interior node
+    while (link != kSentinel) {
+        // Descend interior nodes until a leaf link or an empty stack.
+        while (link >= 0) {
+            const float4 *n = bvh.nodes + 4 * (size_t)link;
+            float4 n0 = __ldg(n + 0), n1 = __ldg(n + 1), n2 = __ldg(n + 2);
+            int4 n3 = __ldg(reinterpret_cast<const int4 *>(n + 3));
+            float t0, t1;
+            bool h0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, tmin, hit.t, t0);
+            bool h1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, tmin, hit.t, t1);
+            if (h0 && h1) {
+                int near = n3.x, far = n3.y;
+                if (t1 < t0) { near = n3.y; far = n3.x; }
+                stack[sp++] = far;
+                link = near;
+            } else if (h0) {
+                link = n3.x;
+            } else if (h1) {
+                link = n3.y;
+            } else {
+                link = stack[--sp];
+            }
+        }
+        if (link == kSentinel) break;
+        // Leaf.
+        int code = ~link;
+        int first = code >> 4, count = code & 15;
+        for (int k = 0; k < count; ++k) {
+            int slot = first + k;
+            const float4 *tp = bvh.tris + 3 * (size_t)slot;
+            float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            bool acc = intersect_triangle(o, d, a, b, c, slot, hit);
+            if (kEarlyExit && acc && hit.t < t_exit) return hit;
+        }
+        link = stack[--sp];
+    }
+    return hit;
+}
+
+__device__ __forceinline__ int tri_prim(const BvhView &bvh, int slot) {
+    return __float_as_int(__ldg(bvh.tris + 3 * (size_t)slot).w);
+}
+
+#endif  // __CUDACC__
+
+}  // namespace crt

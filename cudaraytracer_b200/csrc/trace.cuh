@@ -1,0 +1,54 @@
+// Ray-query device functions shared by the standalone trace kernels and the
+// wavefront shade stage.
+#pragma once
+#include "bvh.cuh"
+
+namespace crt {
+
+#ifdef __CUDACC__
+
+// Hit point of a closest-hit record: b0*v0 + b1*v1 + b2*v2 with
+// b0 = 1 - b1 - b2, evaluated in the reference's order
+// (Src/Core/triangle.cu:121-127).
+__device__ __forceinline__ V3 hit_point(const BvhView &bvh, const Hit &h) {
+    const float4 *tp = bvh.tris + 3 * (size_t)h.slot;
+    float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+    float b0 = rsub(rsub(1.f, h.b1), h.b2);
+    return V3{radd(radd(rmul(b0, a.x), rmul(h.b1, b.x)), rmul(h.b2, c.x)),
+              radd(radd(rmul(b0, a.y), rmul(h.b1, b.y)), rmul(h.b2, c.y)),
+              radd(radd(rmul(b0, a.z), rmul(h.b1, b.z)), rmul(h.b2, c.z))};
+}
+
+// Light::Visible (Src/Core/light.cu:5-27). Both endpoints are pushed 1e-4
+// along their normals; the ray runs from the light point toward the shading
+// point starting 1e-2 along it, with box tMin 1e-6. The point is occluded iff
+// the closest hit lies more than 0.1 from the shading point AND its distance
+// to the light differs from the sample distance by more than 0.1. (The
+// reference compares float distances with the double 0.1, i.e. x >= 0.1f.)
+// Any accepted hit with t < t_exit already fixes the answer to "occluded"
+// (the closest hit is then at least as near, hence more than 0.1 short of the
+// shading point on both tests), so traversal stops there.
+__device__ __forceinline__ bool visible(const BvhView &bvh, V3 hp, V3 hn, V3 lp, V3 ln) {
+    V3 h = vadd(hp, vscale(hn, 1e-4f));
+    V3 l = vadd(lp, vscale(ln, 1e-4f));
+    V3 diff = vsub(h, l);
+    float sd = vnorm(diff);
+    V3 dir = vnormalized(diff);
+    V3 o = vadd(l, vscale(dir, 1e-2f));
+    float t_exit = sd * 0.9999f - 0.1101f;
+    Hit hit = closest_hit<true>(bvh, o, dir, 1e-6f, 1e8f, t_exit);
+    if (hit.slot < 0) return true;
+    if (hit.t < t_exit) return false;
+    V3 thp = hit_point(bvh, hit);
+    float td = vnorm(vsub(thp, l));
+    if (vnorm(vsub(h, thp)) >= 0.1f && fabsf(rsub(td, sd)) >= 0.1f) return false;
+    return true;
+}
+
+#endif
+
+// Host launchers (trace.cu).
+void launch_trace_closest(const BvhView &bvh, const float4 *d_rays, int64_t n, float4 *d_hits, cudaStream_t s);
+void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_t *d_occ, cudaStream_t s);
+
+}  // namespace crt

@@ -1,0 +1,131 @@
+/*
+ * crt.h — C ABI of the B200 wavefront path tracer (libcrt.so).
+ *
+ * Plain C types only: opaque handles, POD structs, pointers and sizes.
+ * Every entry point returns a crt_status; no C++ exception crosses the ABI.
+ * Host-buffer entry points copy inputs host->device and results back inside
+ * the call; "_device" variants take device pointers and a CUDA stream
+ * (passed as void*, NULL = the context's stream) and do not synchronise.
+ *
+ * Reference interfaces these replace (DarrenChen-CN/CudaRayTracer):
+ *   Scene(const std::string&)          Src/Core/scene.cpp:50
+ *   BVH::BVH / CreateBVH               Src/Core/bvh.cu:9, :308
+ *   BVH::IsIntersect (closest hit)     Src/Core/bvh.cu:253
+ *   Light::Visible (shadow predicate)  Src/Core/light.cu:5
+ *   Renderer::RenderLoop (frame loop)  Src/Core/renderer.cuh:1106
+ * The reference exposes these as in-process C++ classes and global
+ * singletons (renderParam, Src/Core/scene.h:46; cameraParam,
+ * Src/Core/camera.h:48); it has no FFI of its own.
+ */
+#ifndef CRT_H
+#define CRT_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum crt_status {
+    CRT_OK = 0,
+    CRT_ERR_INVALID = 1,   /* bad argument (null pointer, negative size, ...) */
+    CRT_ERR_IO = 2,        /* file could not be opened or read               */
+    CRT_ERR_PARSE = 3,     /* malformed JSON / OBJ / HDR                     */
+    CRT_ERR_CUDA = 4,      /* a CUDA runtime call failed                     */
+    CRT_ERR_OOM = 5,       /* device allocation failed                       */
+    CRT_ERR_CAPACITY = 6,  /* request exceeds a fixed capacity               */
+    CRT_ERR_TIMEOUT = 7    /* a bounded device-side wait gave up             */
+} crt_status;
+
+typedef struct crt_ctx crt_ctx;
+typedef struct crt_scene crt_scene;
+
+/* One ray: origin + tmin, direction + tmax (32 B, two float4).
+ * tmin only prunes BVH boxes and tmax is the initial closest distance, as in
+ * BVH::IsIntersect(ray, info, tMin, tMax) (Src/Core/bvh.cu:253,263,283-284);
+ * triangles accept 0 <= t <= 1e8 (Src/Core/bvh.cu:271 default arguments,
+ * Src/Core/triangle.cu:125). */
+typedef struct crt_ray {
+    float ox, oy, oz, tmin;
+    float dx, dy, dz, tmax;
+} crt_ray;
+
+/* Closest-hit record (16 B): distance, original primitive index (-1 = miss)
+ * and the barycentrics (b1, b2) of Src/Core/triangle.cu:116-118. */
+typedef struct crt_hit {
+    float t;
+    int32_t prim;
+    float u, v;
+} crt_hit;
+
+/* Inputs of Light::Visible (Src/Core/light.cu:5-27): the shading point and its
+ * geometric normal, the light sample point and its normal (48 B). */
+typedef struct crt_shadow_query {
+    float px, py, pz;
+    float nx, ny, nz;
+    float lx, ly, lz;
+    float lnx, lny, lnz;
+} crt_shadow_query;
+
+/* Scene summary returned by crt_scene_info. */
+typedef struct crt_scene_info_t {
+    int64_t num_triangles;
+    int64_t num_bvh_nodes;
+    int32_t bvh_depth;
+    int32_t num_meshes;
+    int32_t num_materials;
+    int32_t num_lights;
+    float bounds_min[3];
+    float bounds_max[3];
+    float build_ms;        /* device BVH build time (CUDA events) */
+    int32_t width, height, spp, max_bounces;
+    float rr, fovy;
+    int32_t denoise;
+    int32_t has_env;
+} crt_scene_info_t;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Creates a context bound to CUDA device `device` with its own stream.
+ * Replaces the implicit device/global state of the reference
+ * (Src/Utils/ui.cpp:164 cudaSetDevice(0); Src/Core/scene.h:46). */
+crt_status crt_create(int device, crt_ctx **out);
+void crt_destroy(crt_ctx *ctx);
+/* Message of the last failing call on this thread ("" if none). */
+const char *crt_last_error(void);
+/* Library version string. */
+const char *crt_version(void);
+
+/* ---- scenes ----------------------------------------------------------- */
+
+/* Geometry-only scene from a triangle soup (n_tris x 9 floats: v0,v1,v2),
+ * primitive index = position in the array. Builds the BVH on the device.
+ * Replaces BVH::BVH(Triangle*, int, 4, SAH) + CreateBVH
+ * (Src/Core/bvh.cu:9-32, :308-314; called from Src/Core/scene.cpp:115-127). */
+crt_status crt_scene_from_triangles(crt_ctx *ctx, const float *tri_verts,
+                                    int64_t n_tris, crt_scene **out);
+void crt_scene_free(crt_scene *scene);
+crt_status crt_scene_info(const crt_scene *scene, crt_scene_info_t *info);
+
+/* ---- ray queries ------------------------------------------------------ */
+
+/* Closest hit for n rays in host memory (BVH::IsIntersect, Src/Core/bvh.cu:253
+ * with Triangle::IsIntersect, Src/Core/triangle.cu:15). */
+crt_status crt_trace_closest(crt_scene *scene, const crt_ray *rays, int64_t n,
+                             crt_hit *hits);
+/* Same on device buffers, asynchronous on `stream` (cudaStream_t or NULL). */
+crt_status crt_trace_closest_device(crt_scene *scene, const crt_ray *d_rays,
+                                    int64_t n, crt_hit *d_hits, void *stream);
+
+/* Light::Visible predicate (Src/Core/light.cu:5-27) for n queries; writes
+ * occluded[i] = 1 when the reference would return false (not visible). */
+crt_status crt_trace_shadow(crt_scene *scene, const crt_shadow_query *q,
+                            int64_t n, uint8_t *occluded);
+crt_status crt_trace_shadow_device(crt_scene *scene, const crt_shadow_query *d_q,
+                                   int64_t n, uint8_t *d_occluded, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CRT_H */

@@ -1,0 +1,154 @@
+"""Oracle (test infrastructure only): ctypes access to
+  * liboracle.so          - the CPU restatement of the reference's render path
+                            (crt_oracle.c), and
+  * _ref/libcrtref.so     - the reference's own sources compiled as host C++
+                            (present when built where the reference tree is).
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
+legs use this package, as the checker; the product never imports it."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libcrtref.so")
+
+_VP = C.c_void_p
+
+
+def build() -> None:
+    r = subprocess.run(["make", "-C", HERE, "-j", str(os.cpu_count() or 1)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("building the oracle failed:\n" + r.stdout[-3000:] + r.stderr[-3000:])
+
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib() -> C.CDLL:
+    global _oracle
+    if _oracle is None:
+        L = C.CDLL(ORACLE_SO)
+        L.oracle_trace_brute.argtypes = [_VP, C.c_long, _VP, C.c_long, _VP, C.c_int]
+        L.oracle_trace_fp64.argtypes = [_VP, C.c_long, _VP, C.c_long, _VP, _VP, C.c_int]
+        L.oracle_visible.argtypes = [_VP, C.c_long, _VP, C.c_long, _VP, C.c_int]
+        L.oracle_tri_isect.argtypes = [_VP, _VP, _VP, C.c_float, _VP, _VP, _VP]
+        _oracle = L
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        L = C.CDLL(REF_SO)
+        L.ref_scene_from_triangles.restype = _VP
+        L.ref_scene_from_triangles.argtypes = [_VP, C.c_long]
+        L.ref_scene_free.argtypes = [_VP]
+        L.ref_bvh_stats.argtypes = [_VP, _VP, _VP]
+        L.ref_trace_closest.argtypes = [_VP, _VP, C.c_long, _VP, C.c_int]
+        L.ref_visible.argtypes = [_VP, _VP, C.c_long, _VP, C.c_int]
+        _ref = L
+    return _ref
+
+
+def _f32(a, cols):
+    return np.ascontiguousarray(a, dtype=np.float32).reshape(-1, cols)
+
+
+def trace_brute(tris, rays, nthreads: int = 0) -> np.ndarray:
+    t, r = _f32(tris, 9), _f32(rays, 8)
+    out = np.empty((r.shape[0], 4), dtype=np.float32)
+    oracle_lib().oracle_trace_brute(t.ctypes.data, t.shape[0], r.ctypes.data, r.shape[0], out.ctypes.data, nthreads)
+    return out
+
+
+def trace_fp64(tris, rays, nthreads: int = 0):
+    t, r = _f32(tris, 9), _f32(rays, 8)
+    out_t = np.empty(r.shape[0], dtype=np.float64)
+    out_p = np.empty(r.shape[0], dtype=np.int32)
+    oracle_lib().oracle_trace_fp64(t.ctypes.data, t.shape[0], r.ctypes.data, r.shape[0], out_t.ctypes.data,
+                                   out_p.ctypes.data, nthreads)
+    return out_t, out_p
+
+
+def visible(tris, queries, nthreads: int = 0) -> np.ndarray:
+    t, q = _f32(tris, 9), _f32(queries, 12)
+    out = np.empty(q.shape[0], dtype=np.uint8)
+    oracle_lib().oracle_visible(t.ctypes.data, t.shape[0], q.ctypes.data, q.shape[0], out.ctypes.data, nthreads)
+    return out
+
+
+def tri_isect(tri, o, d, closest=np.float32(1e8)):
+    v = _f32(tri, 9)
+    oo = np.ascontiguousarray(o, dtype=np.float32)
+    dd = np.ascontiguousarray(d, dtype=np.float32)
+    t, b1, b2 = C.c_float(), C.c_float(), C.c_float()
+    ok = oracle_lib().oracle_tri_isect(v.ctypes.data, oo.ctypes.data, dd.ctypes.data, C.c_float(closest),
+                                       C.byref(t), C.byref(b1), C.byref(b2))
+    return bool(ok), t.value, b1.value, b2.value
+
+
+class _quiet_stdout:
+    """Silences file descriptor 1 while the reference's code prints progress
+    (its BVH build and destructor write to stdout)."""
+
+    def __enter__(self):
+        import sys
+
+        sys.stdout.flush()
+        self._saved = os.dup(1)
+        self._null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self._null, 1)
+
+    def __exit__(self, *exc):
+        C.CDLL(None).fflush(None)
+        os.dup2(self._saved, 1)
+        os.close(self._saved)
+        os.close(self._null)
+
+
+class RefScene:
+    """The reference's own BVH (host-compiled) over a triangle soup."""
+
+    def __init__(self, tris):
+        self.tris = _f32(tris, 9)
+        with _quiet_stdout():
+            self._h = ref_lib().ref_scene_from_triangles(self.tris.ctypes.data, self.tris.shape[0])
+
+    def stats(self):
+        n, d = C.c_int(), C.c_int()
+        ref_lib().ref_bvh_stats(self._h, C.byref(n), C.byref(d))
+        return n.value, d.value
+
+    def trace_closest(self, rays, nthreads: int = 0) -> np.ndarray:
+        r = _f32(rays, 8)
+        out = np.empty((r.shape[0], 4), dtype=np.float32)
+        ref_lib().ref_trace_closest(self._h, r.ctypes.data, r.shape[0], out.ctypes.data, nthreads)
+        return out
+
+    def visible(self, queries, nthreads: int = 0) -> np.ndarray:
+        q = _f32(queries, 12)
+        out = np.empty(q.shape[0], dtype=np.uint8)
+        ref_lib().ref_visible(self._h, q.ctypes.data, q.shape[0], out.ctypes.data, nthreads)
+        return out
+
+    def close(self):
+        if self._h:
+            with _quiet_stdout():
+                ref_lib().ref_scene_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
