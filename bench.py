@@ -123,6 +123,45 @@ def reference_cpu(tris, rays, queries, threads):
     return (len(rays) + len(queries)) / dt / 1e6, dt
 
 
+def reference_cuda(tris, rays, qs, hits_mine, occ_mine, steps, stream):
+    """Times the reference's own traversal built for the GPU (oracle/_ref,
+    headless CUDA build) on the same device batch and checks its hit records
+    against ours. Returns a dict or None when that build is absent."""
+    import torch
+
+    import oracle
+
+    if not oracle.ref_cuda_available():
+        return None
+    ref = oracle.RefCudaScene(tris)
+    n = rays.shape[0]
+    out = torch.empty_like(hits_mine)
+    occ = torch.empty_like(occ_mine)
+    s = stream.cuda_stream
+    ref.trace(rays.data_ptr(), n, out.data_ptr(), s)
+    ref.visible(qs.data_ptr(), n, occ.data_ptr(), s)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    for _ in range(steps):
+        ref.trace(rays.data_ptr(), n, out.data_ptr(), s)
+    ev[1].record(stream)
+    for _ in range(steps):
+        ref.visible(qs.data_ptr(), n, occ.data_ptr(), s)
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    ext = ev[0].elapsed_time(ev[1]) / steps
+    sh = ev[1].elapsed_time(ev[2]) / steps
+    same_prim = (out[:, 1].view(torch.int32) == hits_mine[:, 1].view(torch.int32))
+    same_t = same_prim & (out[:, 0] == hits_mine[:, 0])
+    res = {"value": round(2 * n / ((ext + sh) * 1e-3) / 1e6, 2), "unit": "Mrays/s",
+           "extend_ms_per_launch": round(ext, 4), "shadow_ms_per_launch": round(sh, 4),
+           "hit_records_identical_frac": float(same_t.float().mean().item()),
+           "occluded_identical_frac": float((occ == occ_mine).float().mean().item()),
+           "build": "reference sources, nvcc -O3 -rdc -arch sm_100a, BVH built on the host"}
+    ref.close()
+    return res
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU implementation of the path
     (rank 0 only), on the same scene, metric and unit."""
@@ -165,15 +204,20 @@ def run_reference(args, rank, world):
 
 
 def main():
+    global N_RAYS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="crt", choices=["crt", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA traversal")
+    ap.add_argument("--rays", type=int, default=N_RAYS, help="rays (and shadow queries) per step per GPU")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, local_rank, world = dist_env()
+    N_RAYS = args.rays
 
     if args.impl == "reference":
         run_reference(args, rank, world)
@@ -200,7 +244,8 @@ def main():
     qs = torch.from_numpy(q_np).to(dev)
     hits = torch.empty((N_RAYS, 4), dtype=torch.float32, device=dev)
     occ = torch.empty((N_RAYS,), dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
 
     def step():
         scene.trace_closest(rays, hits)
@@ -236,6 +281,9 @@ def main():
         total_ms = float(t.item())
         dist.barrier()
     clocks = sampler.stop() if sampler else None
+    ref_cuda = None
+    if rank == 0 and not args.no_ref_cuda:
+        ref_cuda = reference_cuda(tris, rays, qs, hits, occ, max(1, min(args.steps, 3)), stream)
 
     # e2e through the host-buffer API: pinned host inputs, results back.
     pin_r = torch.from_numpy(rays_np).pin_memory()
@@ -243,16 +291,18 @@ def main():
     pin_h = torch.empty((N_RAYS, 4), dtype=torch.float32).pin_memory()
     pin_o = torch.empty((N_RAYS,), dtype=torch.uint8).pin_memory()
     rn, qn, hn, on = pin_r.numpy(), pin_q.numpy(), pin_h.numpy(), pin_o.numpy()
-    e2e_steps = max(2, min(args.steps, 5))
-    scene.trace_closest(rn, hn)
-    scene.trace_shadow(qn, on)
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    e2e_steps = 0 if args.no_e2e else max(2, min(args.steps, 5))
+    e2e_s = 1.0
+    if e2e_steps:
         scene.trace_closest(rn, hn)
         scene.trace_shadow(qn, on)
-    e2e_s = time.perf_counter() - t0
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            scene.trace_closest(rn, hn)
+            scene.trace_shadow(qn, on)
+        e2e_s = time.perf_counter() - t0
     if world > 1:
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -295,6 +345,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_val, 2), "unit": "Mrays/s",
                     "h2d_bytes_per_step": N_RAYS * (32 + 48), "d2h_bytes_per_step": N_RAYS * (16 + 1)},
+            "reference_cuda": ref_cuda,
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
         }

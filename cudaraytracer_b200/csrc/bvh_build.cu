@@ -454,7 +454,7 @@ struct SmallShared {
 };
 
 __global__ void __launch_bounds__(kBlock) k_small(const Task *tasks, int *idx, const float4 *plo, const float4 *phi,
-                                                  float4 *nodes, int *node_counter, int *max_depth) {
+                                                  float4 *nodes, int *node_counter, int *max_depth, int *error_flag) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SmallShared &S = *reinterpret_cast<SmallShared *>(smem_raw);
     const int tid = threadIdx.x;
@@ -548,10 +548,8 @@ __global__ void __launch_bounds__(kBlock) k_small(const Task *tasks, int *idx, c
                 int total;
                 int lrank = block_exclusive_scan(left ? 1 : 0, S.s_warp, total);
                 if (valid) {
-                    if (left)
-                        S.tmp[S.lbase + lrank] = p;
-                    else
-                        S.tmp[nleft + S.rbase + (e - base) - lrank] = p;
+                    int pos = left ? S.lbase + lrank : nleft + S.rbase + (e - base) - lrank;
+                    if (pos >= 0 && pos < t.count) S.tmp[pos] = p;
                 }
                 int nvalid = min((int)blockDim.x, t.count - base);
                 __syncthreads();
@@ -561,7 +559,10 @@ __global__ void __launch_bounds__(kBlock) k_small(const Task *tasks, int *idx, c
                 }
                 __syncthreads();
             }
-            for (int e = tid; e < t.count; e += blockDim.x) idx[t.start + e] = S.tmp[e];
+            if (tid == 0 && S.lbase != nleft) atomicExch(error_flag, 1);
+            __syncthreads();
+            if (*(volatile int *)error_flag == 0)
+                for (int e = tid; e < t.count; e += blockDim.x) idx[t.start + e] = S.tmp[e];
         } else {
             // Index median: exact bounds of both halves.
             const int nleft = S.nleft;
@@ -663,7 +664,7 @@ void build_bvh(const float *d_verts, int n, cudaStream_t stream, BvhBuffers &out
     CRT_CUDA(cudaEventRecord(e0, stream));
 
     DevBuf<float4> plo(n), phi(n);
-    DevBuf<int> idx(n), tmp(n), root_keys(12), counters(2);
+    DevBuf<int> idx(n), tmp(n), root_keys(12), counters(3);
     int max_nodes = std::max(1, n - 1);
     CRT_CUDA(cudaMalloc(&out.nodes, (size_t)max_nodes * 4 * sizeof(float4)));
     CRT_CUDA(cudaMalloc(&out.tris, (size_t)n * 3 * sizeof(float4)));
@@ -672,7 +673,7 @@ void build_bvh(const float *d_verts, int n, cudaStream_t stream, BvhBuffers &out
     int init_keys[12];
     for (int k = 0; k < 12; ++k) init_keys[k] = (k % 6) < 3 ? INT_MAX : INT_MIN;
     CRT_CUDA(cudaMemcpyAsync(root_keys.p, init_keys, sizeof(init_keys), cudaMemcpyHostToDevice, stream));
-    CRT_CUDA(cudaMemsetAsync(counters.p, 0, 2 * sizeof(int), stream));
+    CRT_CUDA(cudaMemsetAsync(counters.p, 0, 3 * sizeof(int), stream));
     int grid = std::min((n + kBlock - 1) / kBlock, 148 * 8);
     k_prim_bounds<<<grid, kBlock, 0, stream>>>(d_verts, n, plo.p, phi.p, idx.p, root_keys.p);
     CRT_CUDA(cudaGetLastError());
@@ -737,6 +738,9 @@ void build_bvh(const float *d_verts, int n, cudaStream_t stream, BvhBuffers &out
                 if (c == 0 || ctask[c] != ctask[c - 1]) run = 0;
                 cloff[c] = run;
                 run += cleft[c];
+                if (c == nc - 1 || ctask[c + 1] != ctask[c])
+                    CRT_CHECK(run == dec[ctask[c]].nleft, CRT_ERR_CUDA,
+                              "BVH build: partition count disagrees with the SAH bins");
             }
             CRT_CUDA(cudaMemcpyAsync(d_cloff.p, cloff.data(), nc * sizeof(int), cudaMemcpyHostToDevice, stream));
             k_scatter_large<<<nc, kBlock, 0, stream>>>(d_tasks.p, d_dec.p, d_ctask.p, d_cbegin.p, d_cloff.p, idx.p,
@@ -761,13 +765,15 @@ void build_bvh(const float *d_verts, int n, cudaStream_t stream, BvhBuffers &out
             size_t smem = sizeof(SmallShared);
             CRT_CUDA(cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_small<<<(int)small.size(), kBlock, smem, stream>>>(d_small.p, idx.p, plo.p, phi.p, out.nodes,
-                                                                counters.p, counters.p + 1);
+                                                                counters.p, counters.p + 1, counters.p + 2);
             CRT_CUDA(cudaGetLastError());
             CRT_CUDA(cudaStreamSynchronize(stream));
         }
-        int cnt[2];
+        int cnt[3];
         CRT_CUDA(cudaMemcpyAsync(cnt, counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
         CRT_CUDA(cudaStreamSynchronize(stream));
+        CRT_CHECK(cnt[2] == 0, CRT_ERR_CUDA, "BVH build: partition count disagrees with the SAH bins");
+        CRT_CHECK(cnt[0] <= max_nodes && cnt[1] < kStackSize - 2, CRT_ERR_CAPACITY, "BVH build: node or depth bound");
         out.num_nodes = cnt[0];
         out.depth = cnt[1];
     }

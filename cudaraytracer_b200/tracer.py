@@ -22,6 +22,17 @@ def _is_cuda_tensor(x) -> bool:
     return getattr(x, "is_cuda", False)
 
 
+def _torch_stream(device, stream=None) -> int:
+    """cudaStream_t of `stream` (or torch's current stream). Torch's default
+    stream has handle 0, which the C ABI reads as "the context's own stream",
+    so it is passed as cudaStreamLegacy (1) instead."""
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream(device).cuda_stream
+    s = int(getattr(s, "cuda_stream", s))
+    return s if s != 0 else 1
+
+
 class Context:
     """A crt_ctx bound to one CUDA device."""
 
@@ -95,7 +106,7 @@ class Scene:
             n = rays.shape[0]
             if hits is None:
                 hits = torch.empty((n, 4), dtype=torch.float32, device=rays.device)
-            s = stream if stream is not None else torch.cuda.current_stream(rays.device).cuda_stream
+            s = _torch_stream(rays.device, stream)
             _lib.call("crt_trace_closest_device", self._h, rays.data_ptr(), int(n), hits.data_ptr(), C.c_void_p(s))
             return hits
         r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
@@ -112,7 +123,7 @@ class Scene:
             n = queries.shape[0]
             if occluded is None:
                 occluded = torch.empty((n,), dtype=torch.uint8, device=queries.device)
-            s = stream if stream is not None else torch.cuda.current_stream(queries.device).cuda_stream
+            s = _torch_stream(queries.device, stream)
             _lib.call("crt_trace_shadow_device", self._h, queries.data_ptr(), int(n), occluded.data_ptr(),
                       C.c_void_p(s))
             return occluded

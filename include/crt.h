@@ -5,7 +5,9 @@
  * Every entry point returns a crt_status; no C++ exception crosses the ABI.
  * Host-buffer entry points copy inputs host->device and results back inside
  * the call; "_device" variants take device pointers and a CUDA stream
- * (passed as void*, NULL = the context's stream) and do not synchronise.
+ * (a cudaStream_t passed as void*; NULL selects the context's own stream,
+ * cudaStreamLegacy = (void*)1 the legacy default stream) and do not
+ * synchronise.
  *
  * Reference interfaces these replace (DarrenChen-CN/CudaRayTracer):
  *   Scene(const std::string&)          Src/Core/scene.cpp:50

@@ -16,6 +16,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libcrtref.so")
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libcrtref_cuda.so")
 
 _VP = C.c_void_p
 
@@ -145,6 +146,59 @@ class RefScene:
         if self._h:
             with _quiet_stdout():
                 ref_lib().ref_scene_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_refcuda = None
+
+
+def ref_cuda_available() -> bool:
+    return os.path.exists(REF_CUDA_SO)
+
+
+def ref_cuda_lib() -> C.CDLL:
+    global _refcuda
+    if _refcuda is None:
+        L = C.CDLL(REF_CUDA_SO)
+        L.refcuda_scene_from_triangles.restype = _VP
+        L.refcuda_scene_from_triangles.argtypes = [_VP, C.c_long]
+        L.refcuda_scene_free.argtypes = [_VP]
+        L.refcuda_trace.argtypes = [_VP, _VP, C.c_long, _VP, _VP]
+        L.refcuda_visible.argtypes = [_VP, _VP, C.c_long, _VP, _VP]
+        _refcuda = L
+    return _refcuda
+
+
+class RefCudaScene:
+    """The reference's own traversal compiled for the GPU (headless build):
+    host BVH build + CreateBVH upload, one thread per ray calling
+    BVH::IsIntersect / Light::Visible. Device pointers in, stream-ordered."""
+
+    def __init__(self, tris):
+        self.tris = _f32(tris, 9)
+        with _quiet_stdout():
+            self._h = ref_cuda_lib().refcuda_scene_from_triangles(self.tris.ctypes.data, self.tris.shape[0])
+
+    def trace(self, d_rays: int, n: int, d_out: int, stream: int = 0) -> None:
+        rc = ref_cuda_lib().refcuda_trace(self._h, d_rays, n, d_out, stream)
+        if rc:
+            raise RuntimeError(f"reference CUDA trace failed: cudaError {rc}")
+
+    def visible(self, d_q: int, n: int, d_occ: int, stream: int = 0) -> None:
+        rc = ref_cuda_lib().refcuda_visible(self._h, d_q, n, d_occ, stream)
+        if rc:
+            raise RuntimeError(f"reference CUDA visible failed: cudaError {rc}")
+
+    def close(self):
+        if self._h:
+            with _quiet_stdout():
+                ref_cuda_lib().refcuda_scene_free(self._h)
             self._h = None
 
     def __del__(self):

@@ -5,8 +5,6 @@
 // addressing (wrap / clamp, normalised or texel coordinates) and filtering
 // (nearest, or bilinear with 8-bit fractional weights; CUDA C Programming
 // Guide, "Texture Fetching"). Test infrastructure only.
-#define STB_IMAGE_IMPLEMENTATION
-#include "stb_image.h"
 #include <cstdlib>
 #include <cstring>
 #include <cmath>
