@@ -57,6 +57,37 @@ class SceneInfo(C.Structure):
     ]
 
 
+class RenderParams(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("spp", C.c_int32),
+        ("max_bounces", C.c_int32),
+        ("rr", C.c_float),
+        ("rr_start_bounce", C.c_int32),
+        ("seed", C.c_uint64),
+        ("spp_per_pass", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class Camera(C.Structure):
+    _fields_ = [
+        ("target", C.c_float * 3),
+        ("distance", C.c_float),
+        ("theta_deg", C.c_float),
+        ("phi_deg", C.c_float),
+        ("fovy_deg", C.c_float),
+        ("position", C.c_float * 3),
+        ("u", C.c_float * 3),
+        ("v", C.c_float * 3),
+        ("w", C.c_float * 3),
+        ("du", C.c_float * 3),
+        ("dv", C.c_float * 3),
+        ("left_down", C.c_float * 3),
+    ]
+
+
 def build(force: bool = False) -> None:
     """Compiles libcrt.so in-tree with nvcc for sm_100a (make in csrc/)."""
     csrc = os.path.join(_HERE, "csrc")
@@ -80,6 +111,15 @@ _SIGS = {
     "crt_scene_from_triangles": (C.c_int, [_VP, _VP, C.c_int64, C.POINTER(_VP)]),
     "crt_scene_free": (None, [_VP]),
     "crt_scene_info": (C.c_int, [_VP, C.POINTER(SceneInfo)]),
+    "crt_scene_load_json": (C.c_int, [_VP, C.c_char_p, C.POINTER(_VP)]),
+    "crt_scene_export_geometry": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "crt_scene_export_tables": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "crt_get_render_params": (C.c_int, [_VP, C.POINTER(RenderParams)]),
+    "crt_set_render_params": (C.c_int, [_VP, C.POINTER(RenderParams)]),
+    "crt_get_camera": (C.c_int, [_VP, C.POINTER(Camera)]),
+    "crt_set_camera_orbit": (C.c_int, [_VP, C.POINTER(Camera)]),
+    "crt_render": (C.c_int, [_VP, C.c_int32, _VP, _VP, _VP]),
+    "crt_render_device": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
     "crt_trace_closest": (C.c_int, [_VP, _VP, C.c_int64, _VP]),
     "crt_trace_closest_device": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
     "crt_trace_shadow": (C.c_int, [_VP, _VP, C.c_int64, _VP]),

@@ -27,6 +27,20 @@ Scene::~Scene() {
     if (d_verts) cudaFree(d_verts);
 }
 
+void Scene::fill_info(crt_scene_info_t &info) const {
+    info.num_meshes = (int32_t)host.meshes.size();
+    info.num_materials = (int32_t)host.materials.size();
+    info.num_lights = (int32_t)host.lights.size();
+    info.width = rp.width;
+    info.height = rp.height;
+    info.spp = rp.spp;
+    info.max_bounces = rp.max_bounces;
+    info.rr = rp.rr;
+    info.fovy = cam.fovy;
+    info.denoise = host.denoise ? 1 : 0;
+    info.has_env = host.env_light >= 0 ? 1 : 0;
+}
+
 }  // namespace crt
 
 using namespace crt;
@@ -174,6 +188,196 @@ crt_status crt_trace_shadow(crt_scene *scene, const crt_shadow_query *q, int64_t
             CRT_CUDA(cudaMemcpyAsync(occluded + off, base + in_b, m, cudaMemcpyDeviceToHost, s));
         }
         for (int k = 0; k < 2; ++k) CRT_CUDA(cudaStreamSynchronize(ctx->streams[k]));
+    });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+crt_status crt_scene_load_json(crt_ctx *ctx, const char *path, crt_scene **out) {
+    return guard([&] {
+        CRT_CHECK(ctx && path && out, CRT_ERR_INVALID, "crt_scene_load_json: null argument");
+        CRT_CUDA(cudaSetDevice(ctx->device));
+        auto *s = new crt_scene();
+        s->ctx = ctx;
+        try {
+            load_scene_json(path, s->host);
+            HostScene &h = s->host;
+            size_t n = h.prim_mesh.size();
+            CRT_CHECK(n < (size_t)(1 << 27) - 1, CRT_ERR_CAPACITY, "too many triangles");
+            CRT_CUDA(cudaMalloc(&s->d_verts, h.verts.size() * sizeof(float)));
+            CRT_CUDA(cudaMemcpy(s->d_verts, h.verts.data(), h.verts.size() * sizeof(float), cudaMemcpyHostToDevice));
+            build_bvh(s->d_verts, (int)n, ctx->stream, s->bvh);
+            upload_render_data(h, s->rd);
+            s->rp.width = h.width;
+            s->rp.height = h.height;
+            s->rp.spp = h.spp;
+            s->rp.max_bounces = h.max_bounces;
+            s->rp.rr = h.rr;
+            init_camera(s->cam, s->bvh.bounds_min, s->bvh.bounds_max, h.direction, h.fovy, h.width, h.height);
+            s->renderable = true;
+        } catch (...) {
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+crt_status crt_scene_export_geometry(const crt_scene *scene, float *verts, float *normals, float *uvs,
+                                     int32_t *prim_mesh) {
+    return guard([&] {
+        CRT_CHECK(scene && scene->renderable, CRT_ERR_INVALID, "crt_scene_export_geometry: not a loaded scene");
+        const HostScene &h = scene->host;
+        if (verts) std::memcpy(verts, h.verts.data(), h.verts.size() * sizeof(float));
+        if (normals) std::memcpy(normals, h.normals.data(), h.normals.size() * sizeof(float));
+        if (uvs) std::memcpy(uvs, h.uvs.data(), h.uvs.size() * sizeof(float));
+        if (prim_mesh) std::memcpy(prim_mesh, h.prim_mesh.data(), h.prim_mesh.size() * sizeof(int32_t));
+    });
+}
+
+crt_status crt_scene_export_tables(const crt_scene *scene, float *materials, float *meshes, float *lights) {
+    return guard([&] {
+        CRT_CHECK(scene && scene->renderable, CRT_ERR_INVALID, "crt_scene_export_tables: not a loaded scene");
+        const HostScene &h = scene->host;
+        if (materials)
+            for (size_t i = 0; i < h.materials.size(); ++i) {
+                const DMaterial &m = h.materials[i];
+                float *o = materials + 16 * i;
+                float v[16] = {(float)m.type, m.base[0], m.base[1], m.base[2], m.ke[0], m.ke[1], m.ke[2], m.roughness,
+                               m.metallic, m.transmission, m.scatter[0], m.scatter[1], m.scatter[2], m.ior,
+                               (float)m.tex, 0.f};
+                std::memcpy(o, v, sizeof(v));
+            }
+        if (meshes)
+            for (size_t i = 0; i < h.meshes.size(); ++i) {
+                const DMesh &m = h.meshes[i];
+                float v[8] = {(float)m.material, (float)m.light, (float)m.start, (float)m.count, m.area, 0, 0, 0};
+                std::memcpy(meshes + 8 * i, v, sizeof(v));
+            }
+        if (lights)
+            for (size_t i = 0; i < h.lights.size(); ++i) {
+                const DLight &l = h.lights[i];
+                float v[8] = {(float)l.type, (float)l.mesh, l.emission[0], l.emission[1], l.emission[2], 0, 0, 0};
+                std::memcpy(lights + 8 * i, v, sizeof(v));
+            }
+    });
+}
+
+crt_status crt_get_render_params(const crt_scene *scene, crt_render_params *p) {
+    return guard([&] {
+        CRT_CHECK(scene && p, CRT_ERR_INVALID, "crt_get_render_params: null argument");
+        std::memset(p, 0, sizeof(*p));
+        p->width = scene->rp.width;
+        p->height = scene->rp.height;
+        p->spp = scene->rp.spp;
+        p->max_bounces = scene->rp.max_bounces;
+        p->rr = scene->rp.rr;
+        p->rr_start_bounce = scene->rp.rr_start_bounce;
+        p->seed = scene->rp.seed;
+        p->spp_per_pass = scene->rp.spp_per_pass;
+    });
+}
+
+crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p) {
+    return guard([&] {
+        CRT_CHECK(scene && p && scene->renderable, CRT_ERR_INVALID, "crt_set_render_params: not a loaded scene");
+        CRT_CHECK(p->width > 0 && p->height > 0 && (int64_t)p->width * p->height < (1 << 30), CRT_ERR_INVALID,
+                  "crt_set_render_params: bad resolution");
+        CRT_CHECK(p->spp >= 0 && p->max_bounces >= 0 && p->spp_per_pass >= 0, CRT_ERR_INVALID,
+                  "crt_set_render_params: negative count");
+        bool resized = p->width != scene->rp.width || p->height != scene->rp.height;
+        scene->rp.width = p->width;
+        scene->rp.height = p->height;
+        scene->rp.spp = p->spp;
+        scene->rp.max_bounces = p->max_bounces;
+        scene->rp.rr = p->rr;
+        scene->rp.rr_start_bounce = p->rr_start_bounce;
+        scene->rp.seed = p->seed;
+        scene->rp.spp_per_pass = p->spp_per_pass;
+        if (resized) {
+            scene->cam.width = p->width;
+            scene->cam.height = p->height;
+            compute_camera(scene->cam);
+        }
+    });
+}
+
+crt_status crt_get_camera(const crt_scene *scene, crt_camera *c) {
+    return guard([&] {
+        CRT_CHECK(scene && c && scene->renderable, CRT_ERR_INVALID, "crt_get_camera: not a loaded scene");
+        const CameraState &s = scene->cam;
+        for (int k = 0; k < 3; ++k) {
+            c->target[k] = s.target[k];
+            c->position[k] = s.position[k];
+            c->u[k] = s.u[k];
+            c->v[k] = s.v[k];
+            c->w[k] = s.w[k];
+            c->du[k] = s.du[k];
+            c->dv[k] = s.dv[k];
+            c->left_down[k] = s.left_down[k];
+        }
+        c->distance = s.distance;
+        c->theta_deg = s.theta;
+        c->phi_deg = s.phi;
+        c->fovy_deg = s.fovy;
+    });
+}
+
+crt_status crt_set_camera_orbit(crt_scene *scene, const crt_camera *c) {
+    return guard([&] {
+        CRT_CHECK(scene && c && scene->renderable, CRT_ERR_INVALID, "crt_set_camera_orbit: not a loaded scene");
+        CameraState &s = scene->cam;
+        for (int k = 0; k < 3; ++k) s.target[k] = c->target[k];
+        s.distance = c->distance;
+        s.theta = c->theta_deg;
+        s.phi = c->phi_deg;
+        s.fovy = c->fovy_deg;
+        compute_camera(s);
+    });
+}
+
+crt_status crt_render_device(crt_scene *scene, int32_t first_sample, int32_t spp, float *d_direct, float *d_indirect,
+                             float *d_sumsq, void *stream) {
+    return guard([&] {
+        CRT_CHECK(scene && scene->renderable, CRT_ERR_INVALID, "crt_render_device: not a loaded scene");
+        CRT_CHECK(d_direct && d_indirect && spp >= 0 && first_sample >= 0, CRT_ERR_INVALID,
+                  "crt_render_device: bad argument");
+        CRT_CUDA(cudaSetDevice(scene->ctx->device));
+        cudaStream_t s = stream ? (cudaStream_t)stream : scene->ctx->stream;
+        Accum acc;
+        acc.direct = (float4 *)d_direct;
+        acc.indirect = (float4 *)d_indirect;
+        acc.sumsq = (float4 *)d_sumsq;
+        acc.pixels = (size_t)scene->rp.width * scene->rp.height;
+        if (spp > 0)
+            render_samples(make_view(scene->bvh, scene->rd), scene->cam, scene->rp, first_sample, spp, scene->wf, acc, s);
+    });
+}
+
+crt_status crt_render(crt_scene *scene, int32_t spp, float *direct, float *indirect, float *sumsq) {
+    return guard([&] {
+        CRT_CHECK(scene && scene->renderable, CRT_ERR_INVALID, "crt_render: not a loaded scene");
+        CRT_CHECK(spp >= 0, CRT_ERR_INVALID, "crt_render: negative spp");
+        CRT_CUDA(cudaSetDevice(scene->ctx->device));
+        cudaStream_t s = scene->ctx->stream;
+        size_t px = (size_t)scene->rp.width * scene->rp.height;
+        size_t bytes = px * sizeof(float4);
+        scene->accum.reserve(3 * bytes);
+        char *base = (char *)scene->accum.p;
+        CRT_CUDA(cudaMemsetAsync(base, 0, 3 * bytes, s));
+        Accum acc;
+        acc.direct = (float4 *)base;
+        acc.indirect = (float4 *)(base + bytes);
+        acc.sumsq = sumsq ? (float4 *)(base + 2 * bytes) : nullptr;
+        acc.pixels = px;
+        if (spp > 0)
+            render_samples(make_view(scene->bvh, scene->rd), scene->cam, scene->rp, 0, spp, scene->wf, acc, s);
+        if (direct) CRT_CUDA(cudaMemcpyAsync(direct, acc.direct, bytes, cudaMemcpyDeviceToHost, s));
+        if (indirect) CRT_CUDA(cudaMemcpyAsync(indirect, acc.indirect, bytes, cudaMemcpyDeviceToHost, s));
+        if (sumsq) CRT_CUDA(cudaMemcpyAsync(sumsq, acc.sumsq, bytes, cudaMemcpyDeviceToHost, s));
+        CRT_CUDA(cudaStreamSynchronize(s));
     });
 }
 

@@ -3,6 +3,9 @@
 #include "common.cuh"
 #include "bvh_build.h"
 #include "trace.cuh"
+#include "render.h"
+#include "scene_data.h"
+#include <memory>
 #include <new>
 #include <exception>
 
@@ -51,8 +54,16 @@ struct Scene {
     crt_ctx *ctx = nullptr;
     float *d_verts = nullptr;
     BvhBuffers bvh;
-    virtual ~Scene();
-    virtual void fill_info(crt_scene_info_t &) const {}
+    // render path (scenes loaded from JSON)
+    bool renderable = false;
+    HostScene host;
+    RenderData rd;
+    CameraState cam;
+    RenderParams rp;
+    Wavefront wf;
+    DeviceScratch accum;  // host-API render accumulators
+    ~Scene();
+    void fill_info(crt_scene_info_t &info) const;
 };
 }  // namespace crt
 

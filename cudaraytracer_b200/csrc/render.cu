@@ -1,0 +1,843 @@
+// Wavefront path tracer: raygen -> (extend -> shade -> shadow) x max_bounces.
+//
+// Replaces Renderer::RenderLoop's frame body (Src/Core/renderer.cuh:1144-1193):
+// GenerateRayKernel (:96-115), IntersectionKernel (:132-163), ShadingKernel /
+// PathTracing (:170-440) and the thrust StreamCompaction with two host syncs
+// per call (:1032-1049). Here:
+//  * path state is SoA (5 x float4 = 80 B per path) in two ping-pong queues;
+//  * extend writes a 16 B hit record per path; shade runs the reference's
+//    per-hit logic, defers the next-event-estimation visibility test to a
+//    record (64 B) for the shadow kernel, and pushes surviving paths to the
+//    other queue with warp-aggregated atomics (no scan, no host round trip);
+//  * queue lengths live on the device, kernels are launched with a fixed
+//    persistent grid that reads them, so a bounce needs no host
+//    synchronisation and the whole pass can be captured in a CUDA graph;
+//  * a path's radiance is added to the pixel (float4 atomics) only when the
+//    path terminates, so paths still alive after max_bounces are dropped,
+//    exactly as the reference drops them (renderer.cuh:1166-1193).
+// Rows are bottom-up (pixel j = 0 is the bottom row), as the reference's
+// accumulation buffers.
+#include "render.h"
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace crt {
+
+// ---------------------------------------------------------------------------
+// host: scene upload
+// ---------------------------------------------------------------------------
+RenderData::~RenderData() {
+    if (attr) cudaFree(attr);
+    if (meshes) cudaFree(meshes);
+    if (materials) cudaFree(materials);
+    if (lights) cudaFree(lights);
+    if (env_tex) cudaDestroyTextureObject(env_tex);
+    if (env_array) cudaFreeArray(env_array);
+    if (env_ucdf) cudaFree(env_ucdf);
+    if (env_vcdf) cudaFree(env_vcdf);
+    if (env_row_alias) cudaFree(env_row_alias);
+    if (env_col_alias) cudaFree(env_col_alias);
+}
+
+template <class T>
+static T *upload(const std::vector<T> &v) {
+    T *d = nullptr;
+    if (v.empty()) return nullptr;
+    CRT_CUDA(cudaMalloc(&d, v.size() * sizeof(T)));
+    CRT_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+}
+
+// Vose's alias method (deterministic worklist order) over weights w; the
+// sampled index has probability w[i] / sum(w).
+static void build_alias(const std::vector<double> &w, float2 *out) {
+    const int n = (int)w.size();
+    double sum = 0;
+    for (double x : w) sum += x;
+    std::vector<double> p(n);
+    for (int i = 0; i < n; ++i) p[i] = sum > 0 ? w[i] * n / sum : 1.0;
+    std::vector<int> small, large;
+    for (int i = 0; i < n; ++i) (p[i] < 1.0 ? small : large).push_back(i);
+    std::vector<float> prob(n, 1.f);
+    std::vector<int> alias(n);
+    for (int i = 0; i < n; ++i) alias[i] = i;
+    while (!small.empty() && !large.empty()) {
+        int s = small.back();
+        small.pop_back();
+        int l = large.back();
+        prob[s] = (float)p[s];
+        alias[s] = l;
+        p[l] = (p[l] + p[s]) - 1.0;
+        if (p[l] < 1.0) {
+            large.pop_back();
+            small.push_back(l);
+        }
+    }
+    for (int i : large) prob[i] = 1.f;
+    for (int i : small) prob[i] = 1.f;
+    for (int i = 0; i < n; ++i) {
+        int a = alias[i];
+        float fa;
+        std::memcpy(&fa, &a, 4);
+        out[i] = make_float2(prob[i], fa);
+    }
+}
+
+void upload_render_data(const HostScene &hs, RenderData &rd) {
+    const size_t n = hs.prim_mesh.size();
+    std::vector<float4> attr(n * 4);
+    for (size_t p = 0; p < n; ++p) {
+        const float *nn = &hs.normals[9 * p];
+        const float *uv = &hs.uvs[6 * p];
+        int m = hs.prim_mesh[p];
+        float mf;
+        std::memcpy(&mf, &m, 4);
+        attr[4 * p + 0] = make_float4(nn[0], nn[1], nn[2], uv[0]);
+        attr[4 * p + 1] = make_float4(nn[3], nn[4], nn[5], uv[1]);
+        attr[4 * p + 2] = make_float4(nn[6], nn[7], nn[8], uv[2]);
+        attr[4 * p + 3] = make_float4(uv[3], uv[4], uv[5], mf);
+    }
+    rd.attr = upload(attr);
+    rd.meshes = upload(hs.meshes);
+    rd.materials = upload(hs.materials);
+    rd.lights = upload(hs.lights);
+    rd.num_meshes = (int)hs.meshes.size();
+    rd.num_materials = (int)hs.materials.size();
+    rd.num_lights = (int)hs.lights.size();
+    rd.env_light = hs.env_light;
+    if (hs.env_light >= 0) {
+        const int W = hs.env_w, H = hs.env_h;
+        rd.env_w = W;
+        rd.env_h = H;
+        cudaChannelFormatDesc cd = cudaCreateChannelDesc<float4>();
+        CRT_CUDA(cudaMallocArray(&rd.env_array, &cd, W, H));
+        CRT_CUDA(cudaMemcpy2DToArray(rd.env_array, 0, 0, hs.env.data(), (size_t)W * 16, (size_t)W * 16, H,
+                                     cudaMemcpyHostToDevice));
+        cudaResourceDesc res;
+        std::memset(&res, 0, sizeof(res));
+        res.resType = cudaResourceTypeArray;
+        res.res.array.array = rd.env_array;
+        cudaTextureDesc td;
+        std::memset(&td, 0, sizeof(td));
+        td.addressMode[0] = cudaAddressModeWrap;   // as HDRTexture::Load (texture.cu:95-100)
+        td.addressMode[1] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 1;
+        CRT_CUDA(cudaCreateTextureObject(&rd.env_tex, &res, &td, nullptr));
+        // Importance-sampling CDFs of HDRTexture::Load (texture.cu:40-83), in
+        // the same float arithmetic and order.
+        std::vector<float> u((size_t)W * H), v(H);
+        for (int y = 0; y < H; ++y) {
+            float vsum = 0.0f;
+            for (int x = 0; x < W; ++x) {
+                size_t i = (size_t)y * W + x;
+                float r = hs.env[4 * i], g = hs.env[4 * i + 1], b = hs.env[4 * i + 2];
+                float lum = 0.2126f * r + 0.7152f * g + 0.0722f * b;
+                float theta = (float)((double)(((float)y + 0.5f) / (float)H) * kPiD);
+                lum *= sinf(theta);
+                vsum += lum;
+                u[i] = vsum;
+            }
+            v[y] = vsum;
+        }
+        for (int y = 0; y < H; ++y) {
+            float rs = v[y];
+            for (int x = 0; x < W; ++x) {
+                size_t i = (size_t)y * W + x;
+                u[i] = rs > 0.0f ? u[i] / rs : 0.0f;
+            }
+        }
+        for (int i = 1; i < H; ++i) v[i] += v[i - 1];
+        float tot = v[H - 1];
+        for (int i = 0; i < H; ++i) v[i] = tot > 0.0f ? v[i] / tot : 0.0f;
+        // Alias tables carrying the CDFs' discrete distribution.
+        std::vector<float2> ra(H), ca((size_t)W * H);
+        std::vector<double> w(H);
+        for (int y = 0; y < H; ++y) w[y] = y == 0 ? v[0] : (double)(v[y] - v[y - 1]);
+        build_alias(w, ra.data());
+        std::vector<double> wc(W);
+        for (int y = 0; y < H; ++y) {
+            const float *row = &u[(size_t)y * W];
+            for (int x = 0; x < W; ++x) wc[x] = x == 0 ? row[0] : (double)(row[x] - row[x - 1]);
+            build_alias(wc, &ca[(size_t)y * W]);
+        }
+        rd.env_ucdf = upload(u);
+        rd.env_vcdf = upload(v);
+        rd.env_row_alias = upload(ra);
+        rd.env_col_alias = upload(ca);
+    }
+}
+
+SceneView make_view(const BvhBuffers &bvh, const RenderData &rd) {
+    SceneView s;
+    std::memset(&s, 0, sizeof(s));
+    s.bvh = bvh.view();
+    s.slot_of_prim = bvh.slot_of_prim;
+    s.attr = rd.attr;
+    s.meshes = rd.meshes;
+    s.materials = rd.materials;
+    s.lights = rd.lights;
+    s.num_lights = rd.num_lights;
+    s.env_light = rd.env_light;
+    s.env.tex = rd.env_tex;
+    s.env.w = rd.env_w;
+    s.env.h = rd.env_h;
+    s.env.ucdf = rd.env_ucdf;
+    s.env.vcdf = rd.env_vcdf;
+    s.env.row_alias = rd.env_row_alias;
+    s.env.col_alias = rd.env_col_alias;
+    // Bounds3D::Center / DiagonalLength of the scene bounds (Src/Core/bounds.h:110-118).
+    float e[3];
+    for (int k = 0; k < 3; ++k) {
+        s.center[k] = (bvh.bounds_min[k] + bvh.bounds_max[k]) * 0.5f;
+        e[k] = bvh.bounds_max[k] - bvh.bounds_min[k];
+    }
+    s.diag = std::sqrt(e[0] * e[0] + (e[1] * e[1] + e[2] * e[2]));
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// host: camera
+// ---------------------------------------------------------------------------
+static float deg2rad(float a) { return (float)((double)(a / 180) * kPiD); }
+static float rad2deg(float r) { return (float)((double)r * 180 / kPiD); }
+
+void compute_camera(CameraState &c) {
+    float th = deg2rad(c.theta), ph = deg2rad(c.phi);
+    float x = c.distance * std::sin(th) * std::sin(ph);
+    float y = c.distance * std::cos(th);
+    float z = c.distance * std::sin(th) * std::cos(ph);
+    float off[3] = {x, y, z};
+    for (int k = 0; k < 3; ++k) {
+        c.position[k] = c.target[k] + off[k];
+        c.lookat[k] = c.target[k];
+    }
+    c.up[0] = 0.f; c.up[1] = 1.f; c.up[2] = 0.f;
+    auto nrm = [](float *v) {
+        float z = v[0] * v[0] + (v[1] * v[1] + v[2] * v[2]);
+        if (z > 0.f) {
+            float s = std::sqrt(z);
+            v[0] /= s; v[1] /= s; v[2] /= s;
+        }
+    };
+    auto crs = [](const float *a, const float *b, float *o) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    float lp[3];
+    for (int k = 0; k < 3; ++k) lp[k] = c.lookat[k] - c.position[k];
+    float wv[3] = {lp[0], lp[1], lp[2]};
+    nrm(wv);
+    for (int k = 0; k < 3; ++k) c.w[k] = -wv[k];
+    float upn[3] = {c.up[0], c.up[1], c.up[2]};
+    nrm(upn);
+    crs(upn, c.w, c.u);
+    nrm(c.u);
+    crs(c.w, c.u, c.v);
+    nrm(c.v);
+    c.focal = std::sqrt(lp[0] * lp[0] + (lp[1] * lp[1] + lp[2] * lp[2]));
+    c.ratio = 1.f * c.width / c.height;
+    float hh = 2 * c.focal * std::tan(deg2rad(c.fovy / 2));
+    float ww = hh * c.ratio;
+    for (int k = 0; k < 3; ++k) {
+        c.du[k] = ww * c.u[k] / c.width;
+        c.dv[k] = hh * c.v[k] / c.height;
+        c.left_down[k] = c.lookat[k] - c.width / 2 * c.du[k] - c.height / 2 * c.dv[k];
+    }
+}
+
+void init_camera(CameraState &c, const float bmin[3], const float bmax[3], const float dir[3], float fovy, int w,
+                 int h) {
+    float e[3];
+    for (int k = 0; k < 3; ++k) {
+        c.target[k] = (bmin[k] + bmax[k]) * 0.5f;
+        e[k] = bmax[k] - bmin[k];
+    }
+    float diag = std::sqrt(e[0] * e[0] + (e[1] * e[1] + e[2] * e[2]));
+    c.fovy = fovy;
+    c.width = w;
+    c.height = h;
+    c.distance = diag * 0.5f / std::sin(deg2rad(fovy) / 2.f) * 0.6f;
+    float d[3] = {dir[0], dir[1], dir[2]};
+    float z = d[0] * d[0] + (d[1] * d[1] + d[2] * d[2]);
+    if (z > 0.f) {
+        float s = std::sqrt(z);
+        for (int k = 0; k < 3; ++k) d[k] /= s;
+    }
+    float dn = std::sqrt(d[0] * d[0] + (d[1] * d[1] + d[2] * d[2]));
+    c.theta = rad2deg(std::acos(d[1] / dn));
+    c.phi = rad2deg(std::atan2(d[0], d[2]));
+    compute_camera(c);
+}
+
+// ---------------------------------------------------------------------------
+// wavefront buffers
+// ---------------------------------------------------------------------------
+void Wavefront::reserve(size_t paths) {
+    if (paths <= cap) return;
+    release();
+    for (int q = 0; q < 2; ++q)
+        for (int k = 0; k < 5; ++k) CRT_CUDA(cudaMalloc(&this->q[q][k], paths * sizeof(float4)));
+    CRT_CUDA(cudaMalloc(&hits, paths * sizeof(float4)));
+    for (int k = 0; k < 4; ++k) CRT_CUDA(cudaMalloc(&shadow[k], paths * sizeof(float4)));
+    for (int k = 0; k < 2; ++k) CRT_CUDA(cudaMalloc(&term[k], paths * sizeof(float4)));
+    CRT_CUDA(cudaMalloc(&counters, 8 * sizeof(int)));
+    CRT_CUDA(cudaMemset(counters, 0, 8 * sizeof(int)));
+    cap = paths;
+}
+
+void Wavefront::release() {
+    for (int q = 0; q < 2; ++q)
+        for (int k = 0; k < 5; ++k)
+            if (this->q[q][k]) cudaFree(this->q[q][k]), this->q[q][k] = nullptr;
+    if (hits) cudaFree(hits), hits = nullptr;
+    for (int k = 0; k < 4; ++k)
+        if (shadow[k]) cudaFree(shadow[k]), shadow[k] = nullptr;
+    for (int k = 0; k < 2; ++k)
+        if (term[k]) cudaFree(term[k]), term[k] = nullptr;
+    if (counters) cudaFree(counters), counters = nullptr;
+    cap = 0;
+}
+
+// ---------------------------------------------------------------------------
+// device: path state
+// ---------------------------------------------------------------------------
+constexpr uint32_t kFirst = 1u << 31, kSpec = 1u << 30, kPixelMask = (1u << 30) - 1;
+constexpr uint32_t kTermBit = 1u << 31, kDirectBit = 1u << 30, kIndexMask = (1u << 30) - 1;
+
+struct PathState {
+    V3 o, d, w, dc, ic;
+    float pdf;
+    uint32_t pixel;
+    bool first, spec;
+    Pcg32 rng;
+};
+
+struct QueueView {
+    float4 *p[5];
+};
+
+__device__ __forceinline__ PathState load_path(const QueueView &q, int i) {
+    float4 a = q.p[0][i], b = q.p[1][i], c = q.p[2][i], d = q.p[3][i], e = q.p[4][i];
+    PathState s;
+    s.o = V3{a.x, a.y, a.z};
+    s.pdf = a.w;
+    s.d = V3{b.x, b.y, b.z};
+    uint32_t meta = __float_as_uint(b.w);
+    s.pixel = meta & kPixelMask;
+    s.first = (meta & kFirst) != 0;
+    s.spec = (meta & kSpec) != 0;
+    s.w = V3{c.x, c.y, c.z};
+    s.dc = V3{c.w, d.x, d.y};
+    s.ic = V3{d.z, d.w, e.x};
+    s.rng.state = ((uint64_t)__float_as_uint(e.z) << 32) | __float_as_uint(e.y);
+    s.rng.inc = ((uint64_t)s.pixel << 1) | 1u;
+    return s;
+}
+
+__device__ __forceinline__ void store_path(const QueueView &q, int i, const PathState &s) {
+    uint32_t meta = s.pixel | (s.first ? kFirst : 0u) | (s.spec ? kSpec : 0u);
+    q.p[0][i] = make_float4(s.o.x, s.o.y, s.o.z, s.pdf);
+    q.p[1][i] = make_float4(s.d.x, s.d.y, s.d.z, __uint_as_float(meta));
+    q.p[2][i] = make_float4(s.w.x, s.w.y, s.w.z, s.dc.x);
+    q.p[3][i] = make_float4(s.dc.y, s.dc.z, s.ic.x, s.ic.y);
+    q.p[4][i] = make_float4(s.ic.z, __uint_as_float((uint32_t)s.rng.state), __uint_as_float((uint32_t)(s.rng.state >> 32)),
+                            0.f);
+}
+
+struct AccumView {
+    float4 *direct, *indirect, *sumsq;
+};
+
+// AccumulateColor (renderer.cuh:117-122) for a terminated path, plus the
+// per-pixel sum of squares of the sample value (for z-tests).
+__device__ __forceinline__ void accumulate(const AccumView &a, uint32_t pixel, V3 dc, V3 ic) {
+    atomicAdd(a.direct + pixel, make_float4(dc.x, dc.y, dc.z, 0.f));
+    atomicAdd(a.indirect + pixel, make_float4(ic.x, ic.y, ic.z, 0.f));
+    if (a.sumsq) {
+        float r = dc.x + ic.x, g = dc.y + ic.y, b = dc.z + ic.z;
+        atomicAdd(a.sumsq + pixel, make_float4(r * r, g * g, b * b, 1.f));
+    }
+}
+
+// Warp-aggregated slot allocation: one atomic per converged group of lanes.
+__device__ __forceinline__ int warp_alloc(int *counter, bool want) {
+    unsigned active = __activemask();
+    unsigned m = __ballot_sync(active, want);
+    if (m == 0) return -1;
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(active, base, leader);
+    return want ? base + __popc(m & ((1u << lane) - 1u)) : -1;
+}
+
+struct CamView {
+    float pos[3], ld[3], du[3], dv[3];
+    int w, h;
+};
+
+struct StepParams {
+    int bounce;
+    float rr;
+    int rr_start;
+    uint64_t seed;
+    int first_sample;
+    int pixels;
+};
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+// GenerateRayKernel + PinholeGeneratingRay (renderer.cuh:96-115,
+// camera.cu:27-35): jitter (u, v), pixel (i + u, j + v) from the bottom-left.
+__global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *counters) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) counters[0] = n;
+    if (i >= n) return;
+    uint32_t pixel = (uint32_t)(i % sp.pixels);
+    uint32_t sample = (uint32_t)(sp.first_sample + i / sp.pixels);
+    int px = (int)pixel % cam.w, py = (int)pixel / cam.w;
+    PathState s;
+    s.rng = pcg32_seed(sp.seed, pixel, sample);
+    float u0 = pcg32_uniform(s.rng), u1 = pcg32_uniform(s.rng);
+    V3 ld = ld3(cam.ld), du = ld3(cam.du), dv = ld3(cam.dv), pos = ld3(cam.pos);
+    V3 pp = (ld + (px + u0) * du) + (py + u1) * dv;
+    s.o = pos;
+    s.d = normalized(pp - pos);
+    s.w = V3{1.f, 1.f, 1.f};
+    s.dc = s.ic = V3{0.f, 0.f, 0.f};
+    s.pdf = 0.f;
+    s.pixel = pixel;
+    s.first = true;
+    s.spec = false;
+    store_path(q, i, s);
+}
+
+// Extend: closest hit of every live path (TraceRay, renderer.cuh:124-130:
+// tMin 0, closest starts at 1e8). Also clears the next bounce's counters.
+__global__ void __launch_bounds__(128) k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters,
+                                                int out_idx) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counters[out_idx] = 0;
+        counters[2] = 0;
+        counters[3] = 0;
+    }
+    const int n = *n_in;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 a = q.p[0][i], b = q.p[1][i];
+        Hit h = closest_hit<false>(bvh, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, 0.f, kTriTMax);
+        hits[i] = make_float4(h.t, __int_as_float(h.slot), h.b1, h.b2);
+    }
+}
+
+struct NeeRecord {
+    V3 hp, hn, lp, ln, C;
+    bool direct;
+    bool valid;
+};
+
+enum StepResult { kContinue = 0, kTerminate = 1 };
+
+// NEE toward one light: sample it, evaluate the contribution as if visible
+// and leave the visibility test (Light::Visible) to the shadow kernel.
+__device__ __forceinline__ bool nee_sample(const SceneView &s, Pcg32 &rng, int &lid, LightSample &ls, float &sel_pdf) {
+    if (s.num_lights == 0) return false;  // LightManager::SampleLight returns nullptr
+    lid = (int)(pcg32_uniform(rng) * s.num_lights);
+    if (lid == s.num_lights) lid = s.num_lights - 1;
+    sel_pdf = 1.0f / s.num_lights;
+    light_sample_point(s, s.lights[lid], rng, ls);
+    return true;
+}
+
+// ProbeOutgongingPoint (material.cu:405-441): two probe rays along -n and +n
+// through the displaced point, the nearer hit wins.
+__device__ __forceinline__ void sss_probe(const SceneView &s, V3 hitPoint, V3 normal, float distance, float angle,
+                                          V3 &outP, V3 &outN) {
+    V3 pn = normalized(normal), t, b;
+    create_onb(pn, t, b);
+    V3 off = distance * (cosf(angle) * t + sinf(angle) * b);
+    outP = hitPoint + off;
+    float ro = fmaxf(distance, 1e-3f);
+    float tmin = 1e-4f, tmax = fmaxf(distance * 2.f, 1e-2f);
+    V3 fo = outP + pn * ro, bo = outP - pn * ro;
+    Hit fh = closest_hit<false>(s.bvh, fo, -pn, tmin, tmax);
+    Hit bh = closest_hit<false>(s.bvh, bo, pn, tmin, tmax);
+    const Hit *use = nullptr;
+    if (fh.slot >= 0 && bh.slot >= 0)
+        use = fh.t <= bh.t ? &fh : &bh;
+    else if (fh.slot >= 0)
+        use = &fh;
+    else if (bh.slot >= 0)
+        use = &bh;
+    if (use) {
+        outP = hit_point(s.bvh, *use);
+        const float4 *tp = s.bvh.tris + 3 * (size_t)use->slot;
+        float4 a = __ldg(tp), bb = __ldg(tp + 1), c = __ldg(tp + 2);
+        V3 v0{a.x, a.y, a.z};
+        outN = vnormalized(vcross(vsub(V3{bb.x, bb.y, bb.z}, v0), vsub(V3{c.x, c.y, c.z}, v0)));
+    } else {
+        outP = hitPoint;
+        outN = pn;
+    }
+}
+
+// PathTracing (renderer.cuh:170-422) for one path at its closest hit.
+__device__ StepResult path_step(const SceneView &s, const StepParams &sp, PathState &ps, const Hit &h, NeeRecord &nee) {
+    nee.valid = false;
+    const bool rr_on = sp.bounce >= sp.rr_start;
+    // IntersectionInfo of Triangle::IsIntersect (triangle.cu:121-130)
+    const float4 *tp = s.bvh.tris + 3 * (size_t)h.slot;
+    float4 ta = __ldg(tp), tb = __ldg(tp + 1), tc = __ldg(tp + 2);
+    int prim = __float_as_int(ta.w);
+    V3 v0{ta.x, ta.y, ta.z}, v1{tb.x, tb.y, tb.z}, v2{tc.x, tc.y, tc.z};
+    V3 hitPoint = hit_point(s.bvh, h);
+    V3 infoNormal = vnormalized(vcross(vsub(v1, v0), vsub(v2, v0)));
+    const float4 *ap = s.attr + 4 * (size_t)prim;
+    float4 A0 = __ldg(ap), A1 = __ldg(ap + 1), A2 = __ldg(ap + 2), A3 = __ldg(ap + 3);
+    float b0 = rsub(rsub(1.f, h.b1), h.b2);
+    V3 sn = normalized((b0 * V3{A0.x, A0.y, A0.z} + h.b1 * V3{A1.x, A1.y, A1.z}) + h.b2 * V3{A2.x, A2.y, A2.z});
+    const DMesh &M = s.meshes[__float_as_int(A3.w)];
+    const DMaterial mat = s.materials[M.material];
+
+    V3 geomNormal = normalized(infoNormal);
+    V3 hitNormal = (double)sqnorm(sn) > kEpsD ? normalized(sn) : geomNormal;
+    if (dot(hitNormal, geomNormal) < 0.f) hitNormal = -hitNormal;
+    V3 wo = -ps.d;
+
+    if (mat.type == MAT_LIGHT) {  // renderer.cuh:192-216
+        V3 ke = ld3(mat.ke);
+        if (ps.first) {
+            ps.dc = ps.dc + ke;
+            ps.first = false;
+            return kTerminate;
+        } else if (ps.spec) {
+            ps.ic = ps.ic + mul(ps.w, ke);
+        } else {
+            float pdfLight = 0.f;  // a light material on a mesh that is not a light: no MIS
+            if (M.light >= 0) pdfLight = light_solid_angle_pdf(s, s.lights[M.light], ps.o, hitPoint, infoNormal);
+            float mw = mis_weight(ps.pdf, pdfLight);
+            ps.ic = ps.ic + mul(ps.w, ke) * mw;
+        }
+        return kTerminate;
+    }
+
+    if (mat.type == MAT_DIELECTRIC) {  // renderer.cuh:218-240
+        V3 dwi, dw;
+        float dpdf = 1.0f;
+        sample_dielectric(mat, wo, hitNormal, dwi, dpdf, dw, ps.rng);
+        ps.pdf = dpdf;
+        ps.o = hitPoint + dwi * 1e-4f;
+        ps.d = dwi;
+        ps.w = mul(ps.w, dw);
+        float p = pcg32_uniform(ps.rng);
+        if (rr_on && p > sp.rr) return kTerminate;
+        if (rr_on) ps.w = ps.w / sp.rr;
+        ps.first = false;
+        ps.spec = true;
+        return kContinue;
+    }
+
+    if (mat.type != MAT_SUBSURFACE) {  // renderer.cuh:242-289
+        int lid;
+        LightSample ls;
+        float sel;
+        if (nee_sample(s, ps.rng, lid, ls, sel)) {
+            const DLight &L = s.lights[lid];
+            V3 dirWi = normalized(ls.position - hitPoint);
+            float pdfLight = light_solid_angle_pdf(s, L, hitPoint, ls.position, ls.normal);
+            pdfLight *= sel;
+            float cosT = dot(hitNormal, dirWi);
+            V3 brdf = mat_eval(mat, wo, hitNormal, dirWi);
+            V3 dirL = (mul(light_emission(s, L, dirWi), brdf) * cosT) / pdfLight;
+            float pdfB = mat_pdf(mat, wo, hitNormal, dirWi);
+            float mw = mis_weight(pdfLight, pdfB);
+            nee.C = mw * mul(ps.w, dirL);
+            nee.hp = hitPoint;
+            nee.hn = infoNormal;
+            nee.lp = ls.position;
+            nee.ln = ls.normal;
+            nee.direct = ps.first;
+            nee.valid = nee.C.x != 0.f || nee.C.y != 0.f || nee.C.z != 0.f;
+        }
+        V3 iwi;
+        float ipdf;
+        mat_sample(mat, wo, hitNormal, iwi, ipdf, ps.rng);
+        V3 brdf = mat_eval(mat, wo, hitNormal, iwi);
+        ps.pdf = ipdf;
+        ps.o = hitPoint;
+        ps.d = iwi;
+        float c = dot(hitNormal, iwi);
+        if (!((double)ipdf < kEpsD || c < 0))
+            ps.w = (mul(ps.w, brdf) * c) / ipdf;
+        else
+            return kTerminate;
+    } else {  // subsurface, renderer.cuh:290-404
+        float FIn = fresnel_mat(mat, wo, hitNormal);
+        float reflectProb = clampf(0.02f, 0.98f, FIn);
+        float transmitProb = fmaxf(1.f - reflectProb, 1e-6f);
+        float ev = pcg32_uniform(ps.rng);
+        if (ev < reflectProb) {
+            V3 rd;
+            if (mat.roughness > 1e-3f) {
+                float r1 = pcg32_uniform(ps.rng), r2 = pcg32_uniform(ps.rng);
+                float a = fmaxf(mat.roughness * mat.roughness, 0.02f);
+                float phi = (float)(2.0 * kPiD * (double)r1);
+                float cosT = sqrtf((1.0f - r2) / (1.0f + (a * a - 1.0f) * r2));
+                float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));
+                V3 hw = local_to_world(V3{sinT * cosf(phi), sinT * sinf(phi), cosT}, hitNormal);
+                rd = normalized(reflect(-wo, hw));
+                if (dot(rd, hitNormal) <= 0.0f) rd = normalized(reflect(-wo, hitNormal));
+            } else {
+                rd = normalized(reflect(-wo, hitNormal));
+            }
+            ps.o = hitPoint + rd * 1e-4f;
+            ps.d = rd;
+            ps.w = mul(ps.w, V3{FIn, FIn, FIn}) / reflectProb;
+            ps.pdf = 1.0f;
+            float p = pcg32_uniform(ps.rng);
+            if (rr_on && p > sp.rr) return kTerminate;
+            if (rr_on) ps.w = ps.w / sp.rr;
+            ps.first = false;
+            ps.spec = true;
+            return kContinue;
+        }
+        // SampleSpatialDiffusionProfile (material.cu:343-368)
+        float distance;
+        int ch = (int)(pcg32_uniform(ps.rng) * 3);
+        ch = (int)clampf(0.f, 2.f, (float)ch);
+        float d = mat.scatter[ch];
+        if (d < 1e-6f) {
+            distance = 0.f;
+        } else {
+            float r1 = pcg32_uniform(ps.rng);
+            if (r1 < 0.5f) {
+                r1 = r1 * 2.f;
+                distance = -d * logf(1.f - r1);
+            } else {
+                r1 = (r1 - 0.5f) * 2.f;
+                distance = -3.f * d * logf(1.f - r1);
+            }
+        }
+        float angle = (float)((double)(pcg32_uniform(ps.rng) * 2.f) * kPiD);
+        V3 outP, outN;
+        sss_probe(s, hitPoint, geomNormal, distance, angle, outP, outN);
+        float sd = norm(outP - hitPoint);
+        float spatialPdf = sd < 1e-6f ? 0.f : burley_pdf(mat, sd);
+        if ((double)spatialPdf < kEpsD) return kTerminate;
+        V3 prof{0.f, 0.f, 0.f};
+        if (!(sd < 1e-6f)) prof = mul(albedo_of(mat), V3{burley(mat, sd, 0), burley(mat, sd, 1), burley(mat, sd, 2)}) / kPiF;
+        ps.w = mul(mul(ps.w, V3{1.f - FIn, 1.f - FIn, 1.f - FIn}), prof) / (transmitProb * spatialPdf);
+        int lid;
+        LightSample ls;
+        float sel;
+        if (nee_sample(s, ps.rng, lid, ls, sel)) {
+            const DLight &L = s.lights[lid];
+            V3 dirWi = normalized(ls.position - outP);
+            float ftout = 1 - fresnel_mat(mat, dirWi, outN);
+            float pdfLight = light_solid_angle_pdf(s, L, outP, ls.position, ls.normal);
+            pdfLight *= sel;
+            float cosT = dot(outN, dirWi);
+            if (cosT > 0.f && (double)pdfLight > kEpsD) {
+                V3 dirL = (mul(light_emission(s, L, dirWi), V3{1.f, 1.f, 1.f} / kPiF) * cosT) / pdfLight;
+                float pdfB = (float)((double)cosT / kPiD);
+                float mw = mis_weight(pdfLight, pdfB);
+                nee.C = (mw * mul(ps.w, dirL)) * ftout;
+                nee.hp = outP;
+                nee.hn = outN;
+                nee.lp = ls.position;
+                nee.ln = ls.normal;
+                nee.direct = ps.first;
+                nee.valid = nee.C.x != 0.f || nee.C.y != 0.f || nee.C.z != 0.f;
+            }
+        }
+        V3 odir;
+        float opdf;
+        sample_diffuse(outN, odir, opdf, ps.rng);
+        float cosOut = dot(outN, odir);
+        float ftout = 1 - fresnel_mat(mat, odir, outN);
+        if ((double)opdf < kEpsD || cosOut < 0.f) return kTerminate;
+        ps.o = outP + outN * 1e-4f;
+        ps.d = odir;
+        ps.w = ps.w * ftout;
+        ps.pdf = opdf;
+    }
+    // Russian roulette (renderer.cuh:407-420)
+    float p = pcg32_uniform(ps.rng);
+    if (rr_on && p > sp.rr) return kTerminate;
+    if (rr_on) ps.w = ps.w / sp.rr;
+    ps.first = false;
+    ps.spec = false;
+    return kContinue;
+}
+
+struct ShadowView {
+    float4 *r[4];
+};
+
+__global__ void __launch_bounds__(128) k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits,
+                                               const int *n_in, QueueView qout, int *counters, int out_idx,
+                                               ShadowView sh, float4 *term0, float4 *term1, AccumView acc) {
+    const int n = *n_in;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        PathState ps = load_path(qin, i);
+        float4 hr = hits[i];
+        Hit h;
+        h.t = hr.x;
+        h.slot = __float_as_int(hr.y);
+        h.b1 = hr.z;
+        h.b2 = hr.w;
+        NeeRecord nee;
+        nee.valid = false;
+        StepResult res;
+        if (h.slot < 0) {
+            // miss (IntersectionKernel, renderer.cuh:139-157): environment
+            // radiance weighted into direct (first bounce) or indirect.
+            if (s.env_light >= 0) {
+                V3 bg = env_emission(s.env, ps.d);
+                if (ps.first)
+                    ps.dc = ps.dc + mul(ps.w, bg);
+                else
+                    ps.ic = ps.ic + mul(ps.w, bg);
+            }
+            res = kTerminate;
+        } else {
+            res = path_step(s, sp, ps, h, nee);
+        }
+        bool cont = res == kContinue;
+        int slot = warp_alloc(&counters[out_idx], cont);
+        if (cont) store_path(qout, slot, ps);
+        bool need_term = !cont && nee.valid;
+        int tslot = warp_alloc(&counters[3], need_term);
+        if (need_term) {
+            term0[tslot] = make_float4(ps.dc.x, ps.dc.y, ps.dc.z, __uint_as_float(ps.pixel));
+            term1[tslot] = make_float4(ps.ic.x, ps.ic.y, ps.ic.z, 0.f);
+        } else if (!cont) {
+            accumulate(acc, ps.pixel, ps.dc, ps.ic);
+        }
+        int sslot = warp_alloc(&counters[2], nee.valid);
+        if (nee.valid) {
+            uint32_t target = cont ? (uint32_t)slot : (kTermBit | (uint32_t)tslot);
+            if (nee.direct) target |= kDirectBit;
+            sh.r[0][sslot] = make_float4(nee.hp.x, nee.hp.y, nee.hp.z, nee.hn.x);
+            sh.r[1][sslot] = make_float4(nee.hn.y, nee.hn.z, nee.lp.x, nee.lp.y);
+            sh.r[2][sslot] = make_float4(nee.lp.z, nee.ln.x, nee.ln.y, nee.ln.z);
+            sh.r[3][sslot] = make_float4(nee.C.x, nee.C.y, nee.C.z, __uint_as_float(target));
+        }
+    }
+}
+
+// Shadow: Light::Visible for each deferred NEE sample; a visible sample's
+// contribution joins its path's direct or indirect radiance; a path that
+// already terminated is then added to its pixel.
+__global__ void __launch_bounds__(128) k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueView qout,
+                                                float4 *term0, float4 *term1, AccumView acc) {
+    const int n = counters[2];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 a = sh.r[0][i], b = sh.r[1][i], c = sh.r[2][i], d = sh.r[3][i];
+        bool vis = visible(bvh, V3{a.x, a.y, a.z}, V3{a.w, b.x, b.y}, V3{b.z, b.w, c.x}, V3{c.y, c.z, c.w});
+        uint32_t target = __float_as_uint(d.w);
+        uint32_t idx = target & kIndexMask;
+        bool direct = (target & kDirectBit) != 0;
+        V3 C{d.x, d.y, d.z};
+        if (target & kTermBit) {
+            float4 t0 = term0[idx], t1 = term1[idx];
+            V3 dc{t0.x, t0.y, t0.z}, ic{t1.x, t1.y, t1.z};
+            if (vis) {
+                if (direct)
+                    dc = dc + C;
+                else
+                    ic = ic + C;
+            }
+            accumulate(acc, __float_as_uint(t0.w), dc, ic);
+        } else if (vis) {
+            if (direct) {
+                float4 p2 = qout.p[2][idx], p3 = qout.p[3][idx];
+                p2.w += C.x;
+                p3.x += C.y;
+                p3.y += C.z;
+                qout.p[2][idx] = p2;
+                qout.p[3][idx] = p3;
+            } else {
+                float4 p3 = qout.p[3][idx], p4 = qout.p[4][idx];
+                p3.z += C.x;
+                p3.w += C.y;
+                p4.x += C.z;
+                qout.p[3][idx] = p3;
+                qout.p[4][idx] = p4;
+            }
+        }
+    }
+}
+
+static int persistent_grid(const void *kernel, int block) {
+    static int sms = 0;
+    if (!sms) {
+        int dev;
+        CRT_CUDA(cudaGetDevice(&dev));
+        CRT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    int per = 0;
+    CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, block, 0));
+    return sms * std::max(1, per);
+}
+
+int render_samples(const SceneView &view, const CameraState &cam, const RenderParams &rp, int first_sample, int spp,
+                   Wavefront &wf, Accum &acc, cudaStream_t stream) {
+    const int pixels = cam.width * cam.height;
+    CRT_CHECK(pixels > 0 && pixels <= (int)kPixelMask, CRT_ERR_INVALID, "bad resolution");
+    int per_pass = rp.spp_per_pass > 0 ? rp.spp_per_pass : std::max(1, (int)((8u << 20) / (unsigned)pixels));
+    per_pass = std::min(per_pass, spp);
+    size_t need = (size_t)pixels * per_pass;
+    CRT_CHECK(need <= kIndexMask, CRT_ERR_CAPACITY, "wavefront larger than 2^30 paths");
+    wf.reserve(need);
+    CamView cv;
+    for (int k = 0; k < 3; ++k) {
+        cv.pos[k] = cam.position[k];
+        cv.ld[k] = cam.left_down[k];
+        cv.du[k] = cam.du[k];
+        cv.dv[k] = cam.dv[k];
+    }
+    cv.w = cam.width;
+    cv.h = cam.height;
+    AccumView av{acc.direct, acc.indirect, acc.sumsq};
+    QueueView q[2];
+    for (int j = 0; j < 2; ++j)
+        for (int k = 0; k < 5; ++k) q[j].p[k] = wf.q[j][k];
+    ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
+    const int g_ext = persistent_grid((const void *)k_extend, 128);
+    const int g_sh = persistent_grid((const void *)k_shade, 128);
+    const int g_sd = persistent_grid((const void *)k_shadow, 128);
+    int launches = 0;
+    for (int done = 0; done < spp; done += per_pass) {
+        int s_here = std::min(per_pass, spp - done);
+        int n = pixels * s_here;
+        StepParams sp;
+        sp.bounce = 0;
+        sp.rr = rp.rr;
+        sp.rr_start = rp.rr_start_bounce;
+        sp.seed = rp.seed;
+        sp.first_sample = first_sample + done;
+        sp.pixels = pixels;
+        k_raygen<<<(n + 255) / 256, 256, 0, stream>>>(cv, sp, n, q[0], wf.counters);
+        ++launches;
+        for (int b = 0; b < rp.max_bounces; ++b) {
+            int in = b & 1, out = 1 - in;
+            sp.bounce = b;
+            k_extend<<<g_ext, 128, 0, stream>>>(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out);
+            k_shade<<<g_sh, 128, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out], wf.counters, out, sh,
+                                              wf.term[0], wf.term[1], av);
+            k_shadow<<<g_sd, 128, 0, stream>>>(view.bvh, sh, wf.counters, q[out], wf.term[0], wf.term[1], av);
+            launches += 3;
+        }
+        CRT_CUDA(cudaGetLastError());
+    }
+    return launches;
+}
+
+}  // namespace crt

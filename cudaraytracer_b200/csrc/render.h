@@ -1,0 +1,65 @@
+// Wavefront renderer interface (render.cu).
+#pragma once
+#include "shade.cuh"
+#include "bvh_build.h"
+#include <vector>
+
+namespace crt {
+
+struct RenderParams {
+    int width = 0, height = 0;
+    int spp = 16;
+    int max_bounces = 5;
+    float rr = 0.8f;
+    int rr_start_bounce = 0;  // extension; 0 = reference (RR at every shading event)
+    uint64_t seed = 1;
+    int spp_per_pass = 0;     // samples per wavefront; 0 = automatic
+};
+
+// Device-resident render data of a scene (everything but the BVH).
+struct RenderData {
+    float4 *attr = nullptr;
+    DMesh *meshes = nullptr;
+    DMaterial *materials = nullptr;
+    DLight *lights = nullptr;
+    int num_meshes = 0, num_materials = 0, num_lights = 0, env_light = -1;
+    cudaArray_t env_array = nullptr;
+    cudaTextureObject_t env_tex = 0;
+    float *env_ucdf = nullptr, *env_vcdf = nullptr;
+    float2 *env_row_alias = nullptr, *env_col_alias = nullptr;
+    int env_w = 0, env_h = 0;
+    ~RenderData();
+};
+
+// Path-state buffers of one wavefront, reused across renders.
+struct Wavefront {
+    size_t cap = 0;
+    float4 *q[2][5] = {};      // two path queues, 5 x float4 per path
+    float4 *hits = nullptr;    // (t, slot, b1, b2)
+    float4 *shadow[4] = {};    // shadow-test records
+    float4 *term[2] = {};      // terminated paths waiting for their shadow test
+    int *counters = nullptr;   // [in0, in1, shadow, term] per bounce parity
+    void reserve(size_t paths);
+    void release();
+    ~Wavefront() { release(); }
+};
+
+// Accumulators (float4 per pixel, rows bottom-up as the reference's).
+struct Accum {
+    float4 *direct = nullptr, *indirect = nullptr, *sumsq = nullptr;
+    size_t pixels = 0;
+};
+
+void upload_render_data(const HostScene &hs, RenderData &rd);
+SceneView make_view(const BvhBuffers &bvh, const RenderData &rd);
+// ComputeCameraParam (Src/Core/camera.h:58-84) from the orbit parameters.
+void compute_camera(CameraState &c);
+// InitCameraParam (Src/Core/scene.cpp:646-667): orbit from scene bounds.
+void init_camera(CameraState &c, const float bmin[3], const float bmax[3], const float dir[3], float fovy, int w,
+                 int h);
+// Renders `spp` samples into acc (added to its contents) on `stream`.
+// Returns the number of kernel launches issued.
+int render_samples(const SceneView &view, const CameraState &cam, const RenderParams &rp, int first_sample, int spp,
+                   Wavefront &wf, Accum &acc, cudaStream_t stream);
+
+}  // namespace crt

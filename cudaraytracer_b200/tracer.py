@@ -5,6 +5,10 @@
                        Src/Core/bvh.cu:9,308).
 * Scene.trace_closest  - BVH::IsIntersect (Src/Core/bvh.cu:253).
 * Scene.trace_shadow   - Light::Visible (Src/Core/light.cu:5).
+* Scene.load           - Scene::Scene(jsonPath) (Src/Core/scene.cpp:50).
+* Scene.render         - the non-denoised progressive frame loop of
+                         Renderer::RenderLoop (Src/Core/renderer.cuh:1144-1193)
+                         returning the float accumulators.
 
 Arguments may be numpy arrays (host path: the library copies in and out,
 pipelined in chunks) or CUDA torch tensors (device path, no copies).
@@ -71,9 +75,80 @@ class Scene:
         _lib.call("crt_scene_from_triangles", ctx.handle, t.ctypes.data, int(t.shape[0]), C.byref(h))
         return cls(ctx, h)
 
+    @classmethod
+    def load(cls, ctx: Context, path: str) -> "Scene":
+        """Loads a scene JSON (reference schema) with its OBJ / HDR assets."""
+        h = C.c_void_p()
+        _lib.call("crt_scene_load_json", ctx.handle, str(path).encode(), C.byref(h))
+        return cls(ctx, h)
+
     @property
     def handle(self):
         return self._h
+
+    # -- render path ---------------------------------------------------------
+
+    def render_params(self) -> dict:
+        p = _lib.RenderParams()
+        _lib.call("crt_get_render_params", self._h, C.byref(p))
+        return {k: getattr(p, k) for k, _ in p._fields_ if k != "reserved"}
+
+    def set_render_params(self, **kw) -> None:
+        p = _lib.RenderParams()
+        _lib.call("crt_get_render_params", self._h, C.byref(p))
+        for k, v in kw.items():
+            if not hasattr(p, k):
+                raise KeyError(k)
+            setattr(p, k, v)
+        _lib.call("crt_set_render_params", self._h, C.byref(p))
+
+    def camera(self) -> dict:
+        c = _lib.Camera()
+        _lib.call("crt_get_camera", self._h, C.byref(c))
+        return {k: (list(getattr(c, k)) if hasattr(getattr(c, k), "__len__") else getattr(c, k)) for k, _ in c._fields_}
+
+    def set_camera_orbit(self, target, distance, theta_deg, phi_deg, fovy_deg) -> None:
+        c = _lib.Camera()
+        for k in range(3):
+            c.target[k] = target[k]
+        c.distance, c.theta_deg, c.phi_deg, c.fovy_deg = distance, theta_deg, phi_deg, fovy_deg
+        _lib.call("crt_set_camera_orbit", self._h, C.byref(c))
+
+    def render(self, spp: int, with_sumsq: bool = False):
+        """Renders spp samples per pixel from a cleared frame. Returns float32
+        (H, W, 4) sums over samples (rows bottom-up): direct, indirect and,
+        if requested, the per-pixel sum of squared sample values."""
+        rp = self.render_params()
+        h, w = rp["height"], rp["width"]
+        d = np.empty((h, w, 4), np.float32)
+        i = np.empty((h, w, 4), np.float32)
+        q = np.empty((h, w, 4), np.float32) if with_sumsq else None
+        _lib.call("crt_render", self._h, int(spp), d.ctypes.data, i.ctypes.data, q.ctypes.data if q is not None else None)
+        return (d, i, q) if with_sumsq else (d, i)
+
+    def render_device(self, direct, indirect, spp: int, first_sample: int = 0, sumsq=None, stream=None):
+        """Adds samples [first_sample, first_sample + spp) into CUDA float32
+        tensors of shape (H, W, 4) (asynchronous on the current stream)."""
+        s = _torch_stream(direct.device, stream)
+        _lib.call("crt_render_device", self._h, int(first_sample), int(spp), direct.data_ptr(), indirect.data_ptr(),
+                  sumsq.data_ptr() if sumsq is not None else None, C.c_void_p(s))
+
+    def export_geometry(self):
+        n = self.info()["num_triangles"]
+        v = np.empty((n, 9), np.float32)
+        nn = np.empty((n, 9), np.float32)
+        uv = np.empty((n, 6), np.float32)
+        pm = np.empty((n,), np.int32)
+        _lib.call("crt_scene_export_geometry", self._h, v.ctypes.data, nn.ctypes.data, uv.ctypes.data, pm.ctypes.data)
+        return v, nn, uv, pm
+
+    def export_tables(self):
+        inf = self.info()
+        m = np.empty((inf["num_materials"], 16), np.float32)
+        me = np.empty((inf["num_meshes"], 8), np.float32)
+        li = np.empty((inf["num_lights"], 8), np.float32)
+        _lib.call("crt_scene_export_tables", self._h, m.ctypes.data, me.ctypes.data, li.ctypes.data)
+        return m, me, li
 
     def info(self) -> dict:
         si = _lib.SceneInfo()

@@ -110,6 +110,68 @@ crt_status crt_scene_from_triangles(crt_ctx *ctx, const float *tri_verts,
 void crt_scene_free(crt_scene *scene);
 crt_status crt_scene_info(const crt_scene *scene, crt_scene_info_t *info);
 
+/* Loads a scene JSON with the reference's schema and semantics (camera,
+ * materials, objects as OBJ files, area and environment lights) and builds
+ * its BVH on the device. Replaces Scene::Scene(path) (Src/Core/scene.cpp:50)
+ * with ParseSceneFile (:129), BuildBVH (:115), InitCameraParam (:646). */
+crt_status crt_scene_load_json(crt_ctx *ctx, const char *path, crt_scene **out);
+
+/* Loaded geometry in scene order (arrays sized by crt_scene_info):
+ * verts n x 9, normals n x 9 (per vertex), uvs n x 6, prim_mesh n. Any
+ * pointer may be NULL. Mirrors Scene's host triangle arrays
+ * (Src/Core/scene.cpp:508-536). */
+crt_status crt_scene_export_geometry(const crt_scene *scene, float *verts, float *normals, float *uvs,
+                                     int32_t *prim_mesh);
+/* Material / mesh / light tables: materials n x 16 floats (type, base[3],
+ * ke[3], roughness, metallic, transmission, scatter[3], ior, tex, 0),
+ * meshes n x 8 (material, light, start, count, area, 0, 0, 0), lights
+ * n x 8 (type, mesh, emission[3], 0, 0, 0); integers stored as float values. */
+crt_status crt_scene_export_tables(const crt_scene *scene, float *materials, float *meshes, float *lights);
+
+/* ---- rendering -------------------------------------------------------- */
+
+/* Render parameters; defaults come from the scene JSON camera block
+ * (Src/Core/scene.cpp:187-252) and CameraParam (Src/Core/camera.h:40-44). */
+typedef struct crt_render_params {
+    int32_t width, height;    /* resolution */
+    int32_t spp;              /* samples per pixel of one crt_render call */
+    int32_t max_bounces;      /* extend/shade iterations (renderer.cuh:1166) */
+    float rr;                 /* Russian-roulette continuation probability */
+    int32_t rr_start_bounce;  /* extension: first bounce that applies RR; 0 = reference */
+    uint64_t seed;            /* PCG32 seed of the per-path streams */
+    int32_t spp_per_pass;     /* samples per wavefront; 0 = automatic */
+    int32_t reserved;
+} crt_render_params;
+
+crt_status crt_get_render_params(const crt_scene *scene, crt_render_params *p);
+crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p);
+
+/* Orbit camera (CameraParam, Src/Core/camera.h:11-46). Setting recomputes
+ * the pinhole basis as Camera::ComputeCameraParam (camera.h:58-84). */
+typedef struct crt_camera {
+    float target[3];
+    float distance, theta_deg, phi_deg, fovy_deg;
+    float position[3], u[3], v[3], w[3];  /* derived, ignored on set */
+    float du[3], dv[3], left_down[3];     /* derived: pixel steps, corner */
+} crt_camera;
+
+crt_status crt_get_camera(const crt_scene *scene, crt_camera *cam);
+crt_status crt_set_camera_orbit(crt_scene *scene, const crt_camera *cam);
+
+/* Renders spp samples per pixel from a cleared frame and copies the float
+ * accumulators to host buffers of width*height*4 floats: sums over samples
+ * of the direct and indirect radiance (rgb + 0) and, optionally, the sum of
+ * squares of each sample's total radiance (rgb + sample count). Rows are
+ * bottom-up, as the reference's direct/indirect lighting buffers
+ * (Src/Core/renderer.cuh:56-59, 117-122); divide by spp for the image.
+ * Replaces the non-denoised progressive loop of Renderer::RenderLoop
+ * (Src/Core/renderer.cuh:1144-1193). Any output pointer may be NULL. */
+crt_status crt_render(crt_scene *scene, int32_t spp, float *direct, float *indirect, float *sumsq);
+/* Adds samples [first_sample, first_sample + spp) into device accumulators
+ * (float4 per pixel; sumsq may be NULL) on `stream`, asynchronously. */
+crt_status crt_render_device(crt_scene *scene, int32_t first_sample, int32_t spp, float *d_direct,
+                             float *d_indirect, float *d_sumsq, void *stream);
+
 /* ---- ray queries ------------------------------------------------------ */
 
 /* Closest hit for n rays in host memory (BVH::IsIntersect, Src/Core/bvh.cu:253

@@ -31,6 +31,74 @@ _oracle = None
 _ref = None
 
 
+class _OracleSceneC(C.Structure):
+    _fields_ = [
+        ("verts", _VP), ("normals", _VP), ("uvs", _VP), ("prim_mesh", _VP), ("ntris", C.c_long),
+        ("meshes", _VP), ("materials", _VP), ("lights", _VP),
+        ("nmeshes", C.c_int), ("nmaterials", C.c_int), ("nlights", C.c_int),
+        ("env_light", C.c_int), ("env", _VP), ("env_w", C.c_int), ("env_h", C.c_int),
+        ("cam_pos", C.c_float * 3), ("cam_ld", C.c_float * 3), ("cam_du", C.c_float * 3), ("cam_dv", C.c_float * 3),
+        ("width", C.c_int), ("height", C.c_int), ("max_bounces", C.c_int), ("rr", C.c_float),
+        ("rr_start", C.c_int), ("seed", C.c_ulonglong),
+    ]
+
+
+def render(scene, camera, spp: int, first_sample: int = 0, seed: int = 1, max_bounces=None, rr=None,
+           rr_start: int = 0, width=None, height=None, nthreads: int = 0):
+    """Oracle path tracer over an oracle.scene.OracleScene with camera
+    vectors {position, left_down, du, dv}; returns (direct, indirect, sumsq)
+    float32 arrays of shape (H, W, 4), sums over samples, bottom-up rows."""
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data
+
+    w = int(width or scene.width)
+    h = int(height or scene.height)
+    o = _OracleSceneC()
+    o.verts = arr(scene.verts, np.float32)
+    o.normals = arr(scene.normals, np.float32)
+    o.uvs = arr(scene.uvs, np.float32)
+    o.prim_mesh = arr(scene.prim_mesh, np.int32)
+    o.ntris = len(scene.prim_mesh)
+    o.meshes = arr(scene.meshes, np.float32)
+    o.materials = arr(scene.materials, np.float32)
+    o.lights = arr(scene.lights, np.float32)
+    o.nmeshes, o.nmaterials, o.nlights = len(scene.meshes), len(scene.materials), len(scene.lights)
+    o.env_light = scene.env_light
+    if scene.env_light >= 0:
+        o.env = arr(scene.env, np.float32)
+        o.env_h, o.env_w = scene.env.shape[0], scene.env.shape[1]
+    for k in range(3):
+        o.cam_pos[k] = camera["position"][k]
+        o.cam_ld[k] = camera["left_down"][k]
+        o.cam_du[k] = camera["du"][k]
+        o.cam_dv[k] = camera["dv"][k]
+    o.width, o.height = w, h
+    o.max_bounces = int(scene.max_bounces if max_bounces is None else max_bounces)
+    o.rr = float(scene.rr if rr is None else rr)
+    o.rr_start = rr_start
+    o.seed = seed
+    d = np.zeros((h, w, 4), np.float32)
+    i = np.zeros((h, w, 4), np.float32)
+    q = np.zeros((h, w, 4), np.float32)
+    oracle_lib().oracle_render(C.byref(o), first_sample, spp, d.ctypes.data, i.ctypes.data, q.ctypes.data, nthreads)
+    return d, i, q
+
+
+def env_tables(env):
+    e = np.ascontiguousarray(env, dtype=np.float32)
+    h, w = e.shape[:2]
+    u = np.zeros(w * h, np.float32)
+    v = np.zeros(h, np.float32)
+    ra = np.zeros(2 * h, np.float32)
+    ca = np.zeros(2 * w * h, np.float32)
+    oracle_lib().oracle_env_tables(e.ctypes.data, w, h, u.ctypes.data, v.ctypes.data, ra.ctypes.data, ca.ctypes.data)
+    return u, v, ra, ca
+
+
 def oracle_lib() -> C.CDLL:
     global _oracle
     if _oracle is None:
@@ -39,6 +107,8 @@ def oracle_lib() -> C.CDLL:
         L.oracle_trace_fp64.argtypes = [_VP, C.c_long, _VP, C.c_long, _VP, _VP, C.c_int]
         L.oracle_visible.argtypes = [_VP, C.c_long, _VP, C.c_long, _VP, C.c_int]
         L.oracle_tri_isect.argtypes = [_VP, _VP, _VP, C.c_float, _VP, _VP, _VP]
+        L.oracle_render.argtypes = [C.POINTER(_OracleSceneC), C.c_int, C.c_int, _VP, _VP, _VP, C.c_int]
+        L.oracle_env_tables.argtypes = [_VP, C.c_int, C.c_int, _VP, _VP, _VP, _VP]
         _oracle = L
     return _oracle
 

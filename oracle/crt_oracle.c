@@ -66,7 +66,9 @@ int oracle_tri_isect(const float *v, const float *o_, const float *d_, float clo
  * triangle, ties resolved to the lowest index (first visited). The box tMin
  * of BVH::IsIntersect (Src/Core/bvh.cu:283-284) only prunes boxes and has no
  * brute-force counterpart; closest starts at tMax (:263). */
-static int closest_brute(const float *verts, long ntris, v3 o, v3 d, float tmax, float *t, float *b1, float *b2) {
+int oracle_closest_brute(const float *verts, long ntris, const float *o_, const float *d_, float tmax, float *t,
+                         float *b1, float *b2) {
+    v3 o = ld3(o_), d = ld3(d_);
     int prim = -1;
     float best = tmax, tb1 = 0.f, tb2 = 0.f;
     float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
@@ -99,7 +101,7 @@ static void trace_brute_body(long i, void *c_) {
     job_ctx *c = (job_ctx *)c_;
     const float *r = c->in + 8 * i;
     float t, b1, b2;
-    int prim = closest_brute(c->verts, c->ntris, ld3(r), ld3(r + 4), r[7], &t, &b1, &b2);
+    int prim = oracle_closest_brute(c->verts, c->ntris, r, r + 4, r[7], &t, &b1, &b2);
     float *o = c->out + 4 * i;
     o[0] = t;
     memcpy(&o[1], &prim, 4);
@@ -166,7 +168,7 @@ void oracle_trace_fp64(const float *verts, long ntris, const float *rays, long n
  * 1e-2 along the ray; occluded iff the closest hit is more than 0.1 from the
  * shading point and its light distance differs from the sample distance by
  * more than 0.1 (float distances compared with the double 0.1). */
-static int visible_one(const float *verts, long ntris, const float *a) {
+int oracle_visible_one(const float *verts, long ntris, const float *a) {
     v3 h = add(ld3(a), scale(ld3(a + 3), 1e-4f));
     v3 l = add(ld3(a + 6), scale(ld3(a + 9), 1e-4f));
     v3 diff = sub(h, l);
@@ -174,7 +176,8 @@ static int visible_one(const float *verts, long ntris, const float *a) {
     v3 dir = normalized(diff);
     v3 o = add(l, scale(dir, 1e-2f));
     float t, b1, b2;
-    int prim = closest_brute(verts, ntris, o, dir, 1e8f, &t, &b1, &b2);
+    float oo[3] = {o.x, o.y, o.z}, dd[3] = {dir.x, dir.y, dir.z};
+    int prim = oracle_closest_brute(verts, ntris, oo, dd, 1e8f, &t, &b1, &b2);
     if (prim < 0) return 1;
     const float *v = verts + 9 * prim;
     float b0 = (1.f - b1) - b2;
@@ -186,7 +189,7 @@ static int visible_one(const float *verts, long ntris, const float *a) {
 
 static void visible_body(long i, void *c_) {
     job_ctx *c = (job_ctx *)c_;
-    c->out_u8[i] = visible_one(c->verts, c->ntris, c->in + 12 * i) ? 0 : 1;
+    c->out_u8[i] = oracle_visible_one(c->verts, c->ntris, c->in + 12 * i) ? 0 : 1;
 }
 
 void oracle_visible(const float *verts, long ntris, const float *q, long n, uint8_t *occluded, int nthreads) {
