@@ -120,6 +120,7 @@ _SIGS = {
     "crt_set_camera_orbit": (C.c_int, [_VP, C.POINTER(Camera)]),
     "crt_render": (C.c_int, [_VP, C.c_int32, _VP, _VP, _VP]),
     "crt_render_device": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
+    "crt_render_device_noalloc": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
     "crt_trace_closest": (C.c_int, [_VP, _VP, C.c_int64, _VP]),
     "crt_trace_closest_device": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
     "crt_trace_shadow": (C.c_int, [_VP, _VP, C.c_int64, _VP]),

@@ -17,7 +17,7 @@
 //    exactly as the reference drops them (renderer.cuh:1166-1193).
 // Rows are bottom-up (pixel j = 0 is the bottom row), as the reference's
 // accumulation buffers.
-#include "render.h"
+#include "render_kernels.cuh"
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -305,8 +305,6 @@ void Wavefront::release() {
 // ---------------------------------------------------------------------------
 // device: path state
 // ---------------------------------------------------------------------------
-constexpr uint32_t kFirst = 1u << 31, kSpec = 1u << 30, kPixelMask = (1u << 30) - 1;
-constexpr uint32_t kTermBit = 1u << 31, kDirectBit = 1u << 30, kIndexMask = (1u << 30) - 1;
 
 struct PathState {
     V3 o, d, w, dc, ic;
@@ -316,9 +314,6 @@ struct PathState {
     Pcg32 rng;
 };
 
-struct QueueView {
-    float4 *p[5];
-};
 
 __device__ __forceinline__ PathState load_path(const QueueView &q, int i) {
     float4 a = q.p[0][i], b = q.p[1][i], c = q.p[2][i], d = q.p[3][i], e = q.p[4][i];
@@ -348,9 +343,6 @@ __device__ __forceinline__ void store_path(const QueueView &q, int i, const Path
                             0.f);
 }
 
-struct AccumView {
-    float4 *direct, *indirect, *sumsq;
-};
 
 // AccumulateColor (renderer.cuh:117-122) for a terminated path, plus the
 // per-pixel sum of squares of the sample value (for z-tests).
@@ -376,19 +368,7 @@ __device__ __forceinline__ int warp_alloc(int *counter, bool want) {
     return want ? base + __popc(m & ((1u << lane) - 1u)) : -1;
 }
 
-struct CamView {
-    float pos[3], ld[3], du[3], dv[3];
-    int w, h;
-};
 
-struct StepParams {
-    int bounce;
-    float rr;
-    int rr_start;
-    uint64_t seed;
-    int first_sample;
-    int pixels;
-};
 
 // ---------------------------------------------------------------------------
 // kernels
@@ -676,9 +656,6 @@ __device__ StepResult path_step(const SceneView &s, const StepParams &sp, PathSt
     return kContinue;
 }
 
-struct ShadowView {
-    float4 *r[4];
-};
 
 __global__ void __launch_bounds__(128) k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits,
                                                const int *n_in, QueueView qout, int *counters, int out_idx,
@@ -775,7 +752,7 @@ __global__ void __launch_bounds__(128) k_shadow(BvhView bvh, ShadowView sh, cons
     }
 }
 
-static int persistent_grid(const void *kernel, int block) {
+int persistent_grid(const void *kernel, int block) {
     static int sms = 0;
     if (!sms) {
         int dev;

@@ -1,0 +1,54 @@
+// Kernel-level interface of the wavefront renderer: path-state encoding,
+// kernel parameter blocks and the stage kernels (defined in render.cu).
+#pragma once
+#include "render.h"
+
+namespace crt {
+
+// Path metadata word: pixel index in bits 0-29, flags in 30-31.
+constexpr uint32_t kFirst = 1u << 31, kSpec = 1u << 30, kPixelMask = (1u << 30) - 1;
+constexpr uint32_t kTermBit = 1u << 31, kDirectBit = 1u << 30, kIndexMask = (1u << 30) - 1;
+
+// Path queue: five float4 planes per path (SoA).
+struct QueueView {
+    float4 *p[5];
+};
+
+// Pixel accumulators (float4 per pixel).
+struct AccumView {
+    float4 *direct, *indirect, *sumsq;
+};
+
+// Pinhole camera vectors used by raygen.
+struct CamView {
+    float pos[3], ld[3], du[3], dv[3];
+    int w, h;
+};
+
+// Per-launch constants of a bounce.
+struct StepParams {
+    int bounce;
+    float rr;
+    int rr_start;
+    uint64_t seed;
+    int first_sample;
+    int pixels;
+};
+
+// Deferred next-event-estimation visibility records (four float4 planes).
+struct ShadowView {
+    float4 *r[4];
+};
+
+__global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *counters);
+__global__ void k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters, int out_idx);
+__global__ void k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits, const int *n_in, QueueView qout,
+                        int *counters, int out_idx, ShadowView sh, float4 *term0, float4 *term1, AccumView acc);
+__global__ void k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueView qout, float4 *term0,
+                         float4 *term1, AccumView acc);
+
+// Blocks per grid for a persistent launch of `kernel` (all SMs at full
+// occupancy).
+int persistent_grid(const void *kernel, int block);
+
+}  // namespace crt

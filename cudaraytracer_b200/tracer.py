@@ -133,6 +133,14 @@ class Scene:
         _lib.call("crt_render_device", self._h, int(first_sample), int(spp), direct.data_ptr(), indirect.data_ptr(),
                   sumsq.data_ptr() if sumsq is not None else None, C.c_void_p(s))
 
+    def render_device_noalloc(self, direct, indirect, spp: int, first_sample: int = 0, sumsq=None, stream=None):
+        """render_device without device allocation: the library's fixed
+        scratch holds the path queues (at most 65,536 pixels; calls must not
+        overlap on the GPU). For hosts that forbid allocation during a frame."""
+        s = _torch_stream(direct.device, stream)
+        _lib.call("crt_render_device_noalloc", self._h, int(first_sample), int(spp), direct.data_ptr(),
+                  indirect.data_ptr(), sumsq.data_ptr() if sumsq is not None else None, C.c_void_p(s))
+
     def export_geometry(self):
         n = self.info()["num_triangles"]
         v = np.empty((n, 9), np.float32)

@@ -172,6 +172,20 @@ crt_status crt_render(crt_scene *scene, int32_t spp, float *direct, float *indir
 crt_status crt_render_device(crt_scene *scene, int32_t first_sample, int32_t spp, float *d_direct,
                              float *d_indirect, float *d_sumsq, void *stream);
 
+/* Same as crt_render_device but allocates no device memory: the path queues
+ * live in a fixed scratch area inside the library's device image (17.8 MB
+ * per GPU that loads the library, held until exit), for hosts that own the
+ * GPU memory pool and forbid foreign cudaMalloc/cudaFree during a frame
+ * (engines, viewport plugins, real-time services). At most 65,536 paths per
+ * wavefront: images with more than 65,536 pixels return CRT_ERR_CAPACITY.
+ * The first call on a device looks up the scratch address and must come
+ * before any stream capture on that device. All calls share the scratch,
+ * so calls whose GPU work overlaps race; the caller must order them.
+ * No counterpart in the reference (its renderer allocates its buffers in
+ * Renderer::CudaInit). */
+crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_sample, int32_t spp, float *d_direct,
+                                     float *d_indirect, float *d_sumsq, void *stream);
+
 /* ---- ray queries ------------------------------------------------------ */
 
 /* Closest hit for n rays in host memory (BVH::IsIntersect, Src/Core/bvh.cu:253
