@@ -302,7 +302,7 @@ def env_map(width=2048, height=1024, seed=7, sun_peak=5000.0, sun_sigma=0.03):
 
 
 def icosphere_field(n_spheres=64, level=5, seed=1, width=1920, height=1080, spp=64, max_bounces=16, rr=0.8,
-                    env_size=(2048, 1024), with_env=True) -> SceneSpec:
+                    env_size=(2048, 1024), with_env=True, sun_peak=5000.0, sun_sigma=0.03) -> SceneSpec:
     rng = np.random.default_rng(seed)
     uv, uf = icosphere(level)
     meshes, materials = [], []
@@ -340,7 +340,7 @@ def icosphere_field(n_spheres=64, level=5, seed=1, width=1920, height=1080, spp=
     }
     lights, env = [], None
     if with_env:
-        env = env_map(*env_size, seed=seed + 6)
+        env = env_map(*env_size, seed=seed + 6, sun_peak=sun_peak, sun_sigma=sun_sigma)
         lights = [{"type": "env"}]
     return SceneSpec(meshes, materials, lights, camera, env=env)
 

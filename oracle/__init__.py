@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libcrtref.so")
 REF_CUDA_SO = os.path.join(HERE, "_ref", "libcrtref_cuda.so")
+REF_RENDER_SO = os.path.join(HERE, "_ref", "libcrtref_render.so")
 
 _VP = C.c_void_p
 
@@ -276,3 +277,55 @@ class RefCudaScene:
             self.close()
         except Exception:
             pass
+
+
+_refrender = None
+
+
+def ref_render_available() -> bool:
+    return os.path.exists(REF_RENDER_SO)
+
+
+def ref_render_lib() -> C.CDLL:
+    global _refrender
+    if _refrender is None:
+        L = C.CDLL(REF_RENDER_SO)
+        L.refr_load.restype = _VP
+        L.refr_load.argtypes = [C.c_char_p]
+        L.refr_info.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float), _VP]
+        L.refr_render.argtypes = [_VP, C.c_int, C.c_int, _VP, _VP, _VP, C.POINTER(C.c_float)]
+        _refrender = L
+    return _refrender
+
+
+class RefRenderer:
+    """The reference's own renderer, built headless for the GPU: its scene
+    loader (Scene::Scene) and the non-denoised RenderLoop frame body, one
+    sample per pixel per frame with its curand sampler (seed 1234). One
+    scene per process (the reference keeps its scene in global state)."""
+
+    def __init__(self, json_path: str):
+        with _quiet_stdout():
+            self._h = ref_render_lib().refr_load(str(json_path).encode())
+        if not self._h:
+            raise RuntimeError(f"reference failed to load {json_path}")
+        w, h, mb, rr = C.c_int(), C.c_int(), C.c_int(), C.c_float()
+        cam = (C.c_float * 12)()
+        ref_render_lib().refr_info(C.byref(w), C.byref(h), C.byref(mb), C.byref(rr), cam)
+        self.width, self.height, self.max_bounces, self.rr = w.value, h.value, mb.value, rr.value
+        c = list(cam)
+        self.camera = {"position": c[0:3], "left_down": c[3:6], "du": c[6:9], "dv": c[9:12]}
+
+    def render(self, spp: int, with_sumsq: bool = True, max_bounces: int = 0):
+        """Returns (direct, indirect, sumsq or None, ms): float32 (H, W, 4)
+        sums over spp frames, rows bottom-up; ms = GPU time of the frames."""
+        d = np.zeros((self.height, self.width, 4), np.float32)
+        i = np.zeros_like(d)
+        q = np.zeros_like(d) if with_sumsq else None
+        ms = C.c_float()
+        with _quiet_stdout():
+            rc = ref_render_lib().refr_render(self._h, spp, max_bounces, d.ctypes.data, i.ctypes.data,
+                                              q.ctypes.data if q is not None else None, C.byref(ms))
+        if rc:
+            raise RuntimeError(f"reference render failed: cudaError {rc}")
+        return d, i, q, ms.value

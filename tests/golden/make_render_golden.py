@@ -1,0 +1,54 @@
+"""Generates tests/golden/render_ref_*.npz: converged images rendered by the
+reference's own renderer (oracle/_ref/libcrtref_render.so, a headless CUDA
+build of its Scene loader and RenderLoop frame body). Needs a GPU and the
+prebuilt oracle/_ref libraries; writes to the directory given (default
+tests/golden). Each scene renders in a fresh process because the reference
+keeps its scene in process-global state.
+
+    python tests/golden/make_render_golden.py [outdir]
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+# name -> (scene factory kwargs, spp)
+SCENES = {
+    "cornell": ("cornell_box", dict(width=128, height=128, max_bounces=8), 4096),
+    "icospheres": ("icosphere_field", dict(n_spheres=8, level=2, width=64, height=64, env_size=(256, 128),
+                                           max_bounces=6, sun_peak=40.0, sun_sigma=0.1), 16384),
+}
+
+
+def render_one(name: str, outdir: str) -> None:
+    import oracle
+    from cudaraytracer_b200 import scenes
+
+    fn, kw, spp = SCENES[name]
+    spec = getattr(scenes, fn)(**kw)
+    with tempfile.TemporaryDirectory() as td:
+        path = spec.write(td, name)
+        rr = oracle.RefRenderer(path)
+        d, i, q, ms = rr.render(spp, with_sumsq=True)
+    np.savez_compressed(os.path.join(outdir, f"render_ref_{name}.npz"), direct=d, indirect=i, sumsq=q,
+                        spp=np.int64(spp), gpu_ms=np.float64(ms), camera=np.asarray(
+                            rr.camera["position"] + rr.camera["left_down"] + rr.camera["du"] + rr.camera["dv"],
+                            np.float32))
+    print(f"{name}: {spp} spp in {ms:.1f} ms")
+
+
+if __name__ == "__main__":
+    if len(sys.argv) > 2 and sys.argv[1] == "--one":
+        render_one(sys.argv[2], sys.argv[3])
+    else:
+        out = sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__))
+        os.makedirs(out, exist_ok=True)
+        for name in SCENES:
+            subprocess.run([sys.executable, os.path.abspath(__file__), "--one", name, out], check=True)
