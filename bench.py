@@ -171,6 +171,58 @@ def reference_cuda(tris, rays, qs, hits_mine, occ_mine, steps, stream):
     return res
 
 
+def render_leg(ctx, steps, stream, with_reference=True):
+    """Full wavefront render of the traversal scene at 1920x1080 (depth 16,
+    2048x1024 sky+sun environment map, the four materials), 4 samples per
+    pixel per step, and the same through the reference's own renderer built
+    headless (oracle/_ref). Returns a dict (samples/s and spp/s)."""
+    import tempfile
+
+    import torch
+
+    from cudaraytracer_b200 import Scene, scenes
+
+    td = tempfile.mkdtemp(prefix="crt_bench_")
+    path = scenes.icosphere_field().write(td, "icospheres")
+    sc = Scene.load(ctx, path)
+    rp = sc.render_params()
+    W, H = rp["width"], rp["height"]
+    step_spp = 4
+    dev = torch.device("cuda", ctx.device)
+    d = torch.zeros((H, W, 4), device=dev)
+    i = torch.zeros((H, W, 4), device=dev)
+    sc.render_device(d, i, step_spp, first_sample=0, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(steps):
+        sc.render_device(d, i, step_spp, first_sample=step_spp * (k + 1), stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    spp_total = steps * step_spp
+    out = {"scene": "icosphere field 1920x1080, depth 16, env 2048x1024", "spp_per_step": step_spp,
+           "spp_per_s": round(spp_total / (ms * 1e-3), 2),
+           "msamples_per_s": round(W * H * spp_total / (ms * 1e-3) / 1e6, 2),
+           "ms_per_spp": round(ms / spp_total, 3)}
+    t0 = time.perf_counter()
+    sc.render(step_spp)
+    out["e2e_ms_per_spp_host_api"] = round((time.perf_counter() - t0) * 1e3 / step_spp, 3)
+    if with_reference:
+        import oracle
+
+        if oracle.ref_render_available():
+            ref = oracle.RefRenderer(path)
+            ref.render(1, with_sumsq=False)
+            frames = 2
+            _, _, _, rms = ref.render(frames, with_sumsq=False)
+            out["reference_cuda"] = {"msamples_per_s": round(W * H * frames / (rms * 1e-3) / 1e6, 3),
+                                     "ms_per_spp": round(rms / frames, 2),
+                                     "build": "reference renderer.cuh + Scene, nvcc -O3 -rdc sm_100a, headless"}
+    sc.close()
+    return out
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU implementation of the path
     (rank 0 only), on the same scene, metric and unit."""
@@ -222,6 +274,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA traversal")
+    ap.add_argument("--no-render", action="store_true", help="skip the full-frame render leg")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays (and shadow queries) per step per GPU")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -293,6 +346,9 @@ def main():
     ref_cuda = None
     if rank == 0 and not args.no_ref_cuda:
         ref_cuda = reference_cuda(tris, rays, qs, hits, occ, max(1, min(args.steps, 3)), stream)
+    render = None
+    if rank == 0 and not args.no_render:
+        render = render_leg(ctx, max(2, min(args.steps, 8)), stream, with_reference=not args.no_ref_cuda)
 
     # e2e through the host-buffer API: pinned host inputs, results back.
     pin_r = torch.from_numpy(rays_np).pin_memory()
@@ -361,6 +417,7 @@ def main():
             "e2e": {"value": round(e2e_val, 2), "unit": "Mrays/s",
                     "h2d_bytes_per_step": N_RAYS * (32 + 48), "d2h_bytes_per_step": N_RAYS * (16 + 1)},
             "reference_cuda": ref_cuda,
+            "render": render,
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
         }
