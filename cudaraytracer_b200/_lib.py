@@ -88,6 +88,22 @@ class Camera(C.Structure):
     ]
 
 
+class GBuffer(C.Structure):
+    _fields_ = [("pos_tri", C.c_void_p), ("normal_mat", C.c_void_p), ("bary_mesh", C.c_void_p),
+                ("motion_depth", C.c_void_p)]
+
+
+class DenoiseParams(C.Structure):
+    _fields_ = [
+        ("max_history_length", C.c_int32),
+        ("sigma_light", C.c_float),
+        ("sigma_normal", C.c_float),
+        ("sigma_depth", C.c_float),
+        ("reprojection_depth_factor", C.c_float),
+        ("atrous_iterations", C.c_int32),
+    ]
+
+
 def build(force: bool = False) -> None:
     """Compiles libcrt.so in-tree with nvcc for sm_100a (make in csrc/)."""
     csrc = os.path.join(_HERE, "csrc")
@@ -121,6 +137,14 @@ _SIGS = {
     "crt_render": (C.c_int, [_VP, C.c_int32, _VP, _VP, _VP]),
     "crt_render_device": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
     "crt_render_device_noalloc": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
+    "crt_denoise_params_default": (C.c_int, [C.POINTER(DenoiseParams)]),
+    "crt_gbuffer_from_primary": (C.c_int, [_VP, C.POINTER(Camera), C.POINTER(GBuffer), _VP]),
+    "crt_svgf_create": (C.c_int, [_VP, C.c_int32, C.c_int32, C.POINTER(_VP)]),
+    "crt_svgf_free": (None, [_VP]),
+    "crt_svgf_reset": (C.c_int, [_VP]),
+    "crt_svgf_frame": (C.c_int, [_VP, C.POINTER(DenoiseParams), C.POINTER(GBuffer), C.POINTER(GBuffer), _VP, _VP,
+                                 _VP, _VP, _VP]),
+    "crt_render_svgf_frame": (C.c_int, [_VP, _VP, C.POINTER(DenoiseParams), C.c_int32, _VP, _VP, _VP]),
     "crt_trace_closest": (C.c_int, [_VP, _VP, C.c_int64, _VP]),
     "crt_trace_closest_device": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
     "crt_trace_shadow": (C.c_int, [_VP, _VP, C.c_int64, _VP]),

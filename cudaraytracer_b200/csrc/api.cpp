@@ -382,3 +382,164 @@ crt_status crt_render(crt_scene *scene, int32_t spp, float *direct, float *indir
 }
 
 }  // extern "C"
+
+crt_svgf::~crt_svgf() {
+    for (int k = 0; k < 2; ++k)
+        for (void *p : {(void *)gb[k].pos_tri, (void *)gb[k].normal_mat, (void *)gb[k].bary_mesh,
+                        (void *)gb[k].motion_depth})
+            if (p) cudaFree(p);
+    if (noisy_d) cudaFree(noisy_d);
+    if (noisy_i) cudaFree(noisy_i);
+}
+
+static crt::DenoiseParams to_params(const crt_denoise_params *p) {
+    crt::DenoiseParams d;
+    if (p) {
+        d.max_history_length = p->max_history_length;
+        d.sigma_light = p->sigma_light;
+        d.sigma_normal = p->sigma_normal;
+        d.sigma_depth = p->sigma_depth;
+        d.reprojection_depth_factor = p->reprojection_depth_factor;
+        d.atrous_iterations = p->atrous_iterations;
+    }
+    return d;
+}
+
+static crt::GBufferPlanes to_planes(const crt_gbuffer *g) {
+    crt::GBufferPlanes o;
+    o.pos_tri = (float4 *)g->pos_tri;
+    o.normal_mat = (ushort4 *)g->normal_mat;
+    o.bary_mesh = (ushort4 *)g->bary_mesh;
+    o.motion_depth = (float4 *)g->motion_depth;
+    return o;
+}
+
+static crt::CameraState camera_from(const crt::CameraState &base, const crt_camera *c) {
+    crt::CameraState s = base;
+    for (int k = 0; k < 3; ++k) s.target[k] = c->target[k];
+    s.distance = c->distance;
+    s.theta = c->theta_deg;
+    s.phi = c->phi_deg;
+    s.fovy = c->fovy_deg;
+    crt::compute_camera(s);
+    return s;
+}
+
+extern "C" {
+
+crt_status crt_denoise_params_default(crt_denoise_params *p) {
+    return guard([&] {
+        CRT_CHECK(p, CRT_ERR_INVALID, "crt_denoise_params_default: null");
+        crt::DenoiseParams d;
+        p->max_history_length = d.max_history_length;
+        p->sigma_light = d.sigma_light;
+        p->sigma_normal = d.sigma_normal;
+        p->sigma_depth = d.sigma_depth;
+        p->reprojection_depth_factor = d.reprojection_depth_factor;
+        p->atrous_iterations = d.atrous_iterations;
+    });
+}
+
+crt_status crt_gbuffer_from_primary(crt_scene *scene, const crt_camera *prev, const crt_gbuffer *out, void *stream) {
+    return guard([&] {
+        CRT_CHECK(scene && scene->renderable && out && out->pos_tri && out->normal_mat && out->bary_mesh &&
+                      out->motion_depth,
+                  CRT_ERR_INVALID, "crt_gbuffer_from_primary: bad argument");
+        CRT_CUDA(cudaSetDevice(scene->ctx->device));
+        cudaStream_t s = stream ? (cudaStream_t)stream : scene->ctx->stream;
+        crt::CameraState pc = prev ? camera_from(scene->cam, prev) : scene->cam;
+        gbuffer_from_primary(make_view(scene->bvh, scene->rd), scene->cam, pc, scene->bvh.bounds_min,
+                             scene->bvh.bounds_max, to_planes(out), s);
+    });
+}
+
+crt_status crt_svgf_create(crt_ctx *ctx, int32_t width, int32_t height, crt_svgf **out) {
+    return guard([&] {
+        CRT_CHECK(ctx && out && width > 0 && height > 0, CRT_ERR_INVALID, "crt_svgf_create: bad argument");
+        CRT_CUDA(cudaSetDevice(ctx->device));
+        auto *v = new crt_svgf();
+        v->ctx = ctx;
+        try {
+            v->st.allocate(width, height);
+        } catch (...) {
+            delete v;
+            throw;
+        }
+        *out = v;
+    });
+}
+
+void crt_svgf_free(crt_svgf *s) {
+    if (!s) return;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    delete s;
+}
+
+crt_status crt_svgf_reset(crt_svgf *s) {
+    return guard([&] {
+        CRT_CHECK(s, CRT_ERR_INVALID, "crt_svgf_reset: null");
+        CRT_CUDA(cudaSetDevice(s->ctx->device));
+        CRT_CUDA(cudaDeviceSynchronize());
+        s->st.reset_sync();
+        s->have_prev_cam = false;
+    });
+}
+
+crt_status crt_svgf_frame(crt_svgf *s, const crt_denoise_params *p, const crt_gbuffer *cur, const crt_gbuffer *prev,
+                          const float *noisy_direct, const float *noisy_indirect, float *out_direct,
+                          float *out_indirect, void *stream) {
+    return guard([&] {
+        CRT_CHECK(s && cur && prev && noisy_direct && noisy_indirect && out_direct && out_indirect, CRT_ERR_INVALID,
+                  "crt_svgf_frame: null argument");
+        CRT_CUDA(cudaSetDevice(s->ctx->device));
+        cudaStream_t st = stream ? (cudaStream_t)stream : s->ctx->stream;
+        svgf_frame(s->st, to_params(p), to_planes(cur), to_planes(prev), (const float4 *)noisy_direct,
+                   (const float4 *)noisy_indirect, (float4 *)out_direct, (float4 *)out_indirect, st);
+    });
+}
+
+crt_status crt_render_svgf_frame(crt_scene *scene, crt_svgf *s, const crt_denoise_params *p, int32_t frame_index,
+                                 float *out_direct, float *out_indirect, void *stream) {
+    return guard([&] {
+        CRT_CHECK(scene && scene->renderable && s && out_direct && out_indirect && frame_index >= 0, CRT_ERR_INVALID,
+                  "crt_render_svgf_frame: bad argument");
+        CRT_CHECK(s->st.W == scene->rp.width && s->st.H == scene->rp.height, CRT_ERR_INVALID,
+                  "crt_render_svgf_frame: SVGF state size differs from the render resolution");
+        CRT_CUDA(cudaSetDevice(scene->ctx->device));
+        cudaStream_t st = stream ? (cudaStream_t)stream : scene->ctx->stream;
+        size_t n = (size_t)s->st.W * s->st.H;
+        if (!s->noisy_d) {
+            CRT_CUDA(cudaMalloc(&s->noisy_d, n * sizeof(float4)));
+            CRT_CUDA(cudaMalloc(&s->noisy_i, n * sizeof(float4)));
+            for (int k = 0; k < 2; ++k) {
+                CRT_CUDA(cudaMalloc(&s->gb[k].pos_tri, n * sizeof(float4)));
+                CRT_CUDA(cudaMalloc(&s->gb[k].normal_mat, n * sizeof(ushort4)));
+                CRT_CUDA(cudaMalloc(&s->gb[k].bary_mesh, n * sizeof(ushort4)));
+                CRT_CUDA(cudaMalloc(&s->gb[k].motion_depth, n * sizeof(float4)));
+                CRT_CUDA(cudaMemsetAsync(s->gb[k].pos_tri, 0, n * sizeof(float4), st));
+                CRT_CUDA(cudaMemsetAsync(s->gb[k].normal_mat, 0, n * sizeof(ushort4), st));
+                CRT_CUDA(cudaMemsetAsync(s->gb[k].bary_mesh, 0, n * sizeof(ushort4), st));
+                CRT_CUDA(cudaMemsetAsync(s->gb[k].motion_depth, 0, n * sizeof(float4), st));
+            }
+        }
+        // framebufferReset: each denoised frame starts from cleared buffers
+        CRT_CUDA(cudaMemsetAsync(s->noisy_d, 0, n * sizeof(float4), st));
+        CRT_CUDA(cudaMemsetAsync(s->noisy_i, 0, n * sizeof(float4), st));
+        Accum acc;
+        acc.direct = s->noisy_d;
+        acc.indirect = s->noisy_i;
+        acc.pixels = n;
+        render_samples(make_view(scene->bvh, scene->rd), scene->cam, scene->rp, frame_index, 1, scene->wf, acc, st);
+        const crt::CameraState &pc = s->have_prev_cam ? s->prev_cam : scene->cam;
+        gbuffer_from_primary(make_view(scene->bvh, scene->rd), scene->cam, pc, scene->bvh.bounds_min,
+                             scene->bvh.bounds_max, s->gb[s->gi], st);
+        svgf_frame(s->st, to_params(p), s->gb[s->gi], s->gb[1 - s->gi], s->noisy_d, s->noisy_i, (float4 *)out_direct,
+                   (float4 *)out_indirect, st);
+        s->gi = 1 - s->gi;
+        s->prev_cam = scene->cam;
+        s->have_prev_cam = true;
+    });
+}
+
+}  // extern "C"

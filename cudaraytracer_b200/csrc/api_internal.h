@@ -5,6 +5,7 @@
 #include "trace.cuh"
 #include "render.h"
 #include "scene_data.h"
+#include "svgf.h"
 #include <memory>
 #include <new>
 #include <exception>
@@ -68,3 +69,15 @@ struct Scene {
 }  // namespace crt
 
 struct crt_scene : crt::Scene {};
+
+struct crt_svgf {
+    crt_ctx *ctx = nullptr;
+    crt::SvgfState st;
+    // owned buffers for crt_render_svgf_frame: two G-buffers, noisy planes
+    crt::GBufferPlanes gb[2];
+    float4 *noisy_d = nullptr, *noisy_i = nullptr;
+    int gi = 0;               // G-buffer of the current frame
+    bool have_prev_cam = false;
+    crt::CameraState prev_cam;
+    ~crt_svgf();
+};

@@ -49,6 +49,9 @@ struct Hit {
 // rounded (the reference divides 1.f by a double and rounds to float, which
 // is the same value), strict t < closest so ties keep the first triangle
 // visited. Returns true and updates `hit` when accepted.
+// kCull = false accepts both facings (det != 0), as a rasteriser without
+// face culling sees the nearest surface (used for the G-buffer only).
+template <bool kCull = true>
 __device__ __forceinline__ bool intersect_triangle(V3 o, V3 d, float4 a, float4 b, float4 c,
                                                    int slot, Hit &hit) {
     V3 v0 = v3(a.x, a.y, a.z);
@@ -58,7 +61,7 @@ __device__ __forceinline__ bool intersect_triangle(V3 o, V3 d, float4 a, float4 
     V3 s1 = vcross(d, e2);
     V3 s2 = vcross(s, e1);
     float det = vdot(e1, s1);
-    if (det == 0.f || det < 0.f) return false;
+    if (kCull ? (det == 0.f || det < 0.f) : det == 0.f) return false;
     float inv = rrcp(det);
     float t = rmul(inv, vdot(s2, e2));
     if (t >= hit.t) return false;
@@ -94,7 +97,7 @@ __device__ __forceinline__ bool slab(float lox, float hix, float loy, float hiy,
 // accepted on [0, 1e8] with closest initialised to tmax. When t_exit > 0 the
 // traversal stops at the first accepted hit with t < t_exit (used by the
 // shadow predicate, whose answer is fixed once such a hit exists).
-template <bool kEarlyExit>
+template <bool kEarlyExit, bool kCull = true>
 __device__ __forceinline__ Hit closest_hit(const BvhView &bvh, V3 o, V3 d, float tmin, float tmax,
                                            float t_exit = 0.f) {
     Hit hit;
@@ -136,7 +139,7 @@ __device__ __forceinline__ Hit closest_hit(const BvhView &bvh, V3 o, V3 d, float
             int slot = first + k;
             const float4 *tp = bvh.tris + 3 * (size_t)slot;
             float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
-            bool acc = intersect_triangle(o, d, a, b, c, slot, hit);
+            bool acc = intersect_triangle<kCull>(o, d, a, b, c, slot, hit);
             if (kEarlyExit && acc && hit.t < t_exit) return hit;
         }
         link = stack[--sp];

@@ -1,0 +1,631 @@
+// SVGF denoiser and its primary-hit G-buffer.
+//
+// G-buffer: the reference rasterises one with OpenGL (RenderGBuffer,
+// Src/Core/renderer.cuh:1446-1503; Shader/gbuffer.vs, gbuffer.fs). Here a
+// primary ray through each pixel centre finds the nearest surface (no face
+// culling, as the raster pass culls none) and writes the same four planes
+// with the same encodings:
+//   pos_tri      float4  world position, triangle index within its mesh
+//   normal_mat   ushort4 uint((n * 0.5 + 0.5) * 65535) of the interpolated
+//                        vertex normal, material id
+//   bary_mesh    ushort4 uint(barycentrics * 65535), mesh id + 1
+//   motion_depth float4  NDC(current) - NDC(previous camera), linear view
+//                        depth, fwidth(depth) from 2x2 quad differences
+// Background pixels are all zero (the raster pass's clear values).
+//
+// SVGF: TemporalDenoising (renderer.cuh:524-677), ComputeVarianceKernel
+// (:689-805) and AtrousKernel (:807-954) restated pixel for pixel, driven in
+// the order of RenderLoop's denoise block (:1208-1258): temporal reprojection
+// into the current buffers, history copy, 7x7 variance estimate, then
+// atrous_iterations a-trous passes at steps 1, 2, 4, ... (skipped on the
+// first frame).
+#include "svgf.h"
+#include "shade.cuh"
+#include <cstring>
+
+namespace crt {
+
+// ---------------------------------------------------------------------------
+// G-buffer
+// ---------------------------------------------------------------------------
+struct Mat4 {
+    float m[16];  // row-major
+};
+
+// Perspective (Src/Utils/mathutil.cu:163-172).
+static Mat4 perspective(float fovy, float aspect, float n, float f) {
+    Mat4 r;
+    std::memset(&r, 0, sizeof(r));
+    float ff = 1.0f / std::tan((float)((double)(fovy / 180) * kPiD) / 2.0f);
+    r.m[0] = ff / aspect;
+    r.m[5] = ff;
+    r.m[10] = (f + n) / (n - f);
+    r.m[11] = (2 * f * n) / (n - f);
+    r.m[14] = -1.0f;
+    return r;
+}
+
+// LookAt (Src/Utils/mathutil.cu:175-193).
+static Mat4 look_at(const float *eye, const float *center, const float *up) {
+    auto nrm = [](float *v) {
+        float z = v[0] * v[0] + (v[1] * v[1] + v[2] * v[2]);
+        if (z > 0) {
+            float s = std::sqrt(z);
+            v[0] /= s; v[1] /= s; v[2] /= s;
+        }
+    };
+    auto crs = [](const float *a, const float *b, float *o) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    auto dt = [](const float *a, const float *b) { return a[0] * b[0] + (a[1] * b[1] + a[2] * b[2]); };
+    float f[3] = {center[0] - eye[0], center[1] - eye[1], center[2] - eye[2]}, s[3], u[3];
+    nrm(f);
+    crs(f, up, s);
+    nrm(s);
+    crs(s, f, u);
+    Mat4 r;
+    std::memset(&r, 0, sizeof(r));
+    r.m[0] = s[0]; r.m[1] = s[1]; r.m[2] = s[2]; r.m[3] = -dt(s, eye);
+    r.m[4] = u[0]; r.m[5] = u[1]; r.m[6] = u[2]; r.m[7] = -dt(u, eye);
+    r.m[8] = -f[0]; r.m[9] = -f[1]; r.m[10] = -f[2]; r.m[11] = dt(f, eye);
+    r.m[15] = 1.f;
+    return r;
+}
+
+static Mat4 mul(const Mat4 &a, const Mat4 &b) {
+    Mat4 r;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            float s = 0.f;
+            for (int k = 0; k < 4; ++k) s += a.m[4 * i + k] * b.m[4 * k + j];
+            r.m[4 * i + j] = s;
+        }
+    return r;
+}
+
+struct GbufCam {
+    float pos[3], ld[3], du[3], dv[3];
+    float view[16];
+    float vp[16], prev_vp[16];
+};
+
+__device__ __forceinline__ float4 xform(const float *M, V3 p) {
+    return make_float4(M[0] * p.x + M[1] * p.y + M[2] * p.z + M[3], M[4] * p.x + M[5] * p.y + M[6] * p.z + M[7],
+                       M[8] * p.x + M[9] * p.y + M[10] * p.z + M[11], M[12] * p.x + M[13] * p.y + M[14] * p.z + M[15]);
+}
+
+__global__ void k_gbuffer(SceneView s, GbufCam cam, int W, int H, float4 *pos_tri, ushort4 *normal_mat,
+                          ushort4 *bary_mesh, float4 *motion_depth) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= W || j >= H) return;
+    int pix = j * W + i;
+    V3 ld = ld3(cam.ld), du = ld3(cam.du), dv = ld3(cam.dv), pos = ld3(cam.pos);
+    V3 pp = (ld + (i + 0.5f) * du) + (j + 0.5f) * dv;
+    V3 d = normalized(pp - pos);
+    Hit h = closest_hit<false, false>(s.bvh, pos, d, 0.f, kTriTMax);
+    if (h.slot < 0) {
+        pos_tri[pix] = make_float4(0.f, 0.f, 0.f, 0.f);
+        normal_mat[pix] = make_ushort4(0, 0, 0, 0);
+        bary_mesh[pix] = make_ushort4(0, 0, 0, 0);
+        motion_depth[pix] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    int prim = tri_prim(s.bvh, h.slot);
+    V3 p = hit_point(s.bvh, h);
+    const float4 *ap = s.attr + 4 * (size_t)prim;
+    float4 A0 = __ldg(ap), A1 = __ldg(ap + 1), A2 = __ldg(ap + 2), A3 = __ldg(ap + 3);
+    float b0 = 1.f - h.b1 - h.b2;
+    V3 n = normalized((b0 * V3{A0.x, A0.y, A0.z} + h.b1 * V3{A1.x, A1.y, A1.z}) + h.b2 * V3{A2.x, A2.y, A2.z});
+    int mesh = __float_as_int(A3.w);
+    const DMesh &M = s.meshes[mesh];
+    auto enc = [](float x) -> unsigned short {
+        float v = x * 65535.0f;
+        return (unsigned short)(v <= 0.f ? 0.f : (v >= 65535.f ? 65535.f : v));
+    };
+    pos_tri[pix] = make_float4(p.x, p.y, p.z, (float)(prim - M.start));
+    normal_mat[pix] = make_ushort4(enc(n.x * 0.5f + 0.5f), enc(n.y * 0.5f + 0.5f), enc(n.z * 0.5f + 0.5f),
+                                   (unsigned short)M.material);
+    bary_mesh[pix] = make_ushort4(enc(b0), enc(h.b1), enc(h.b2), (unsigned short)(mesh + 1));
+    float4 c = xform(cam.vp, p), q = xform(cam.prev_vp, p);
+    float4 e = xform(cam.view, p);
+    motion_depth[pix] = make_float4(c.x / c.w - q.x / q.w, c.y / c.w - q.y / q.w, -e.z, 0.f);
+}
+
+// fwidth(depth) = |dFdx| + |dFdy| with the derivative taken within each 2x2
+// pixel quad, as a fragment shader computes it.
+__global__ void k_gbuffer_dz(int W, int H, const float4 *pos_tri_unused, float4 *motion_depth) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= W || j >= H) return;
+    int pix = j * W + i;
+    float4 md = motion_depth[pix];
+    if (md.z == 0.f) return;
+    int ix = i ^ 1, jy = j ^ 1;
+    float dx = 0.f, dy = 0.f;
+    if (ix < W) {
+        float z = motion_depth[j * W + ix].z;
+        if (z != 0.f) dx = (i & 1) ? md.z - z : z - md.z;
+    }
+    if (jy < H) {
+        float z = motion_depth[jy * W + i].z;
+        if (z != 0.f) dy = (j & 1) ? md.z - z : z - md.z;
+    }
+    motion_depth[pix].w = fabsf(dx) + fabsf(dy);
+}
+
+void gbuffer_from_primary(const SceneView &view, const CameraState &cur, const CameraState &prev, const float bmin[3],
+                          const float bmax[3], const GBufferPlanes &g, cudaStream_t stream) {
+    GbufCam gc;
+    for (int k = 0; k < 3; ++k) {
+        gc.pos[k] = cur.position[k];
+        gc.ld[k] = cur.left_down[k];
+        gc.du[k] = cur.du[k];
+        gc.dv[k] = cur.dv[k];
+    }
+    // Near 0.1, far = diagonal + |camera - centre| (renderer.cuh:1469-1471).
+    float c[3], e[3], dc[3];
+    for (int k = 0; k < 3; ++k) {
+        c[k] = (bmin[k] + bmax[k]) * 0.5f;
+        e[k] = bmax[k] - bmin[k];
+        dc[k] = cur.position[k] - c[k];
+    }
+    float far = std::sqrt(e[0] * e[0] + (e[1] * e[1] + e[2] * e[2])) +
+                std::sqrt(dc[0] * dc[0] + (dc[1] * dc[1] + dc[2] * dc[2]));
+    Mat4 P = perspective(cur.fovy, cur.ratio, 0.1f, far);
+    Mat4 V = look_at(cur.position, cur.lookat, cur.up);
+    Mat4 Vp = look_at(prev.position, prev.lookat, prev.up);
+    Mat4 VP = mul(P, V), PVP = mul(perspective(prev.fovy, prev.ratio, 0.1f, far), Vp);
+    std::memcpy(gc.view, V.m, sizeof(gc.view));
+    std::memcpy(gc.vp, VP.m, sizeof(gc.vp));
+    std::memcpy(gc.prev_vp, PVP.m, sizeof(gc.prev_vp));
+    dim3 b(16, 16), gr((cur.width + 15) / 16, (cur.height + 15) / 16);
+    k_gbuffer<<<gr, b, 0, stream>>>(view, gc, cur.width, cur.height, g.pos_tri, g.normal_mat, g.bary_mesh,
+                                    g.motion_depth);
+    k_gbuffer_dz<<<gr, b, 0, stream>>>(cur.width, cur.height, g.pos_tri, g.motion_depth);
+    CRT_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// SVGF
+// ---------------------------------------------------------------------------
+struct GB {
+    const float4 *pos_tri;
+    const ushort4 *normal_mat;
+    const ushort4 *bary_mesh;
+    const float4 *motion_depth;
+};
+
+__device__ __forceinline__ V3 decode_normal(ushort4 n) {
+    return normalized(V3{n.x / 65535.0f * 2.f - 1.f, n.y / 65535.0f * 2.f - 1.f, n.z / 65535.0f * 2.f - 1.f});
+}
+__device__ __forceinline__ V3 rgb(const float4 *b, int i) {
+    float4 v = b[i];
+    return V3{v.x, v.y, v.z};
+}
+
+// IsValidTemporalReprojectionTap (renderer.cuh:460-497).
+__device__ __forceinline__ bool valid_tap(int tx, int ty, int W, int H, int mesh, int mat, int tri, V3 n, float depth,
+                                          float dz, float pixdist, const GB &last, float reproj) {
+    if (tx < 0 || tx >= W || ty < 0 || ty >= H) return false;
+    int k = ty * W + tx;
+    float4 lp = last.pos_tri[k];
+    ushort4 lb = last.bary_mesh[k], ln = last.normal_mat[k];
+    float4 lm = last.motion_depth[k];
+    float dotn = dot(n, decode_normal(ln));
+    float dd = fabsf(depth - lm.z);
+    float thr = fmaxf(dz, lm.w) * (pixdist + 1.f) + reproj * fmaxf(depth, lm.z);
+    return mesh == (int)lb.w && mat == (int)ln.w && tri == (int)lp.w && dotn >= 0.9f && dd <= thr;
+}
+
+struct TemporalArgs {
+    int W, H, max_hist;
+    float reproj;
+    float4 *cur_d, *cur_i;                // current noisy -> blended (in place)
+    const float4 *hist_d, *hist_i;        // last frame's temporal history
+    float2 *mom_d, *mom_i;                // moments written this frame
+    const float2 *lmom_d, *lmom_i;        // last frame's moments
+    int *hlen;                            // history length written
+    const int *lhlen;
+    bool first;
+};
+
+// TemporalDenoising (renderer.cuh:524-677).
+__global__ void k_svgf_temporal(TemporalArgs a, GB cur, GB last) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.W || y >= a.H) return;
+    int idx = y * a.W + x;
+    V3 cd = rgb(a.cur_d, idx), ci = rgb(a.cur_i, idx);
+    if (a.first) {
+        float dl = luminance(cd), il = luminance(ci);
+        a.mom_d[idx] = make_float2(dl, dl * dl);
+        a.mom_i[idx] = make_float2(il, il * il);
+        a.cur_d[idx].w = 1.f;
+        a.cur_i[idx].w = 1.f;
+        a.hlen[idx] = 1;
+        return;
+    }
+    float4 pt = cur.pos_tri[idx];
+    ushort4 bm = cur.bary_mesh[idx], nm = cur.normal_mat[idx];
+    float4 md = cur.motion_depth[idx];
+    int mat = nm.w, mesh = bm.w, tri = (int)pt.w;
+    V3 n = decode_normal(nm);
+    float depth = md.z, dz = md.w;
+    float mvx = md.x * a.W * 0.5f, mvy = md.y * a.H * 0.5f;
+    float pixdist = sqrtf(mvx * mvx + mvy * mvy);
+    // GetLastFramePos (renderer.cuh:446-455)
+    float px = ((float)x + 0.5f) - mvx, py = ((float)y + 0.5f) - mvy;
+    bool inside = px >= 0.5f && px < a.W - 0.5f && py >= 0.5f && py < a.H - 0.5f;
+    bool valid = false;
+    V3 rd{0.f, 0.f, 0.f}, ri{0.f, 0.f, 0.f};
+    float2 rmd = make_float2(0.f, 0.f), rmi = make_float2(0.f, 0.f);
+    float rh = 0.f;
+    auto tap = [&](float w, int k) {
+        rd = rd + rgb(a.hist_d, k) * w;
+        ri = ri + rgb(a.hist_i, k) * w;
+        rmd.x += a.lmom_d[k].x * w;
+        rmd.y += a.lmom_d[k].y * w;
+        rmi.x += a.lmom_i[k].x * w;
+        rmi.y += a.lmom_i[k].y * w;
+        rh += (float)a.lhlen[k] * w;
+    };
+    if (inside) {
+        float fx = px - 0.5f, fy = py - 0.5f;
+        int bx = (int)floorf(fx), by = (int)floorf(fy);
+        float frx = fx - (float)bx, fry = fy - (float)by;
+        float tw = 0.f;
+        bool all = true;
+        for (int oy = 0; oy <= 1; oy++)
+            for (int ox = 0; ox <= 1; ox++) {
+                int tx = bx + ox, ty = by + oy;
+                if (!valid_tap(tx, ty, a.W, a.H, mesh, mat, tri, n, depth, dz, pixdist, last, a.reproj)) {
+                    all = false;
+                    continue;
+                }
+                float w = (ox == 0 ? (1.f - frx) : frx) * (oy == 0 ? (1.f - fry) : fry);
+                tap(w, ty * a.W + tx);
+                tw += w;
+            }
+        if (all && tw > 1e-6f) {
+            float inv = 1.f / tw;
+            rd = rd * inv;
+            ri = ri * inv;
+            rmd.x *= inv; rmd.y *= inv;
+            rmi.x *= inv; rmi.y *= inv;
+            rh *= inv;
+            valid = true;
+        } else {
+            rd = ri = V3{0.f, 0.f, 0.f};
+            rmd = rmi = make_float2(0.f, 0.f);
+            rh = 0.f;
+            tw = 0.f;
+            const float kw[2] = {0.5f, 0.25f};
+            int cx = max(0, min(a.W - 1, (int)floorf(px))), cy = max(0, min(a.H - 1, (int)floorf(py)));
+            for (int oy = -1; oy <= 1; oy++)
+                for (int ox = -1; ox <= 1; ox++) {
+                    int tx = cx + ox, ty = cy + oy;
+                    if (!valid_tap(tx, ty, a.W, a.H, mesh, mat, tri, n, depth, dz, pixdist, last, a.reproj)) continue;
+                    float w = kw[abs(ox)] * kw[abs(oy)];
+                    tap(w, ty * a.W + tx);
+                    tw += w;
+                }
+            if (tw > 1e-6f) {
+                float inv = 1.f / tw;
+                rd = rd * inv;
+                ri = ri * inv;
+                rmd.x *= inv; rmd.y *= inv;
+                rmi.x *= inv; rmi.y *= inv;
+                rh *= inv;
+                valid = true;
+            }
+        }
+    }
+    int hl = 1;
+    if (valid) hl = min(max(1, (int)floorf(rh + 0.5f)) + 1, a.max_hist);
+    float alpha = valid ? 1.f / hl : 1.0f;
+    float dl = luminance(cd), il = luminance(ci);
+    float4 od, oi;
+    od.x = alpha * cd.x + (1 - alpha) * rd.x;
+    od.y = alpha * cd.y + (1 - alpha) * rd.y;
+    od.z = alpha * cd.z + (1 - alpha) * rd.z;
+    oi.x = alpha * ci.x + (1 - alpha) * ri.x;
+    oi.y = alpha * ci.y + (1 - alpha) * ri.y;
+    oi.z = alpha * ci.z + (1 - alpha) * ri.z;
+    float2 lmd = valid ? rmd : make_float2(0.f, 0.f), lmi = valid ? rmi : make_float2(0.f, 0.f);
+    float2 mdd, mii;
+    mdd.x = alpha * dl + (1 - alpha) * lmd.x;
+    mdd.y = alpha * dl * dl + (1 - alpha) * lmd.y;
+    mii.x = alpha * il + (1 - alpha) * lmi.x;
+    mii.y = alpha * il * il + (1 - alpha) * lmi.y;
+    a.mom_d[idx] = mdd;
+    a.mom_i[idx] = mii;
+    if (valid) {
+        od.w = mdd.y - mdd.x * mdd.x;
+        oi.w = mii.y - mii.x * mii.x;
+        a.hlen[idx] = hl;
+    } else {
+        od.w = 1.f;
+        oi.w = 1.f;
+        a.hlen[idx] = 1;
+    }
+    a.cur_d[idx] = od;
+    a.cur_i[idx] = oi;
+}
+
+struct VarianceArgs {
+    int W, H, half;
+    float sigma_depth, sigma_normal, sigma_light;
+    const float4 *in_d, *in_i;
+    float4 *out_d, *out_i;
+    const float2 *mom_d, *mom_i;
+    const int *hlen;
+};
+
+// ComputeVarianceKernel (renderer.cuh:689-805).
+__global__ void k_svgf_variance(VarianceArgs a, GB g) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.W || y >= a.H) return;
+    int idx = y * a.W + x;
+    int h = a.hlen[idx];
+    if (h >= 4) {
+        a.out_d[idx] = a.in_d[idx];
+        a.out_i[idx] = a.in_i[idx];
+        return;
+    }
+    V3 cd = rgb(a.in_d, idx), ci = rgb(a.in_i, idx);
+    float cdl = luminance(cd), cil = luminance(ci);
+    float4 md = g.motion_depth[idx];
+    float cdepth = md.z, dz = fmaxf(md.w, 1e-4f);
+    ushort4 nm = g.normal_mat[idx], bm = g.bary_mesh[idx];
+    int cmat = nm.w, cmesh = bm.w;
+    V3 cn = decode_normal(nm);
+    V3 fd{0.f, 0.f, 0.f}, fi{0.f, 0.f, 0.f};
+    float fmd0 = 0.f, fmd1 = 0.f, fmi0 = 0.f, fmi1 = 0.f, twd = 0.f, twi = 0.f;
+    float sd = a.sigma_depth * fmaxf(dz, 1e-4f);
+    for (int kj = -a.half; kj <= a.half; kj++)
+        for (int ki = -a.half; ki <= a.half; ki++) {
+            int ni = x + ki, nj = y + kj;
+            if (!(ni >= 0 && ni < a.W && nj >= 0 && nj < a.H)) continue;
+            int nidx = nj * a.W + ni;
+            V3 nd = rgb(a.in_d, nidx), nid = rgb(a.in_i, nidx);
+            float nz = g.motion_depth[nidx].z;
+            ushort4 nnm = g.normal_mat[nidx], nbm = g.bary_mesh[nidx];
+            if (cmat != (int)nnm.w || cmesh != (int)nbm.w) continue;
+            V3 nn = decode_normal(nnm);
+            float ndl = luminance(nd), nil = luminance(nid);
+            float2 mdn = a.mom_d[nidx], min_ = a.mom_i[nidx];
+            float dist = sqrtf(float(ki * ki + kj * kj));
+            float wz = -fabsf(cdepth - nz) / (sd * dist + 1e-4f);
+            float wn = powf(fmaxf(0.f, dot(cn, nn)), a.sigma_normal);
+            float dref = fmaxf(fmaxf(cdl, ndl), 1e-4f);
+            float wdl = -fabsf(cdl - ndl) / (a.sigma_light / sqrtf(dref));
+            float wil = -fabsf(cil - nil) / (a.sigma_light / sqrtf(cil));
+            float dw = expf(wz + wdl) * wn, iw = expf(wz + wil) * wn;
+            fd = fd + nd * dw;
+            fi = fi + nid * iw;
+            fmd0 += mdn.x * dw;
+            fmd1 += mdn.y * dw;
+            fmi0 += min_.x * iw;
+            fmi1 += min_.y * iw;
+            twd += dw;
+            twi += iw;
+        }
+    twd = fmaxf(twd, 1e-6f);
+    twi = fmaxf(twi, 1e-6f);
+    fmd0 /= twd; fmd1 /= twd;
+    fmi0 /= twi; fmi1 /= twi;
+    fd = fd / twd;
+    fi = fi / twi;
+    float vd = fmaxf(0.f, fmd1 - fmd0 * fmd0), vi = fmaxf(0.f, fmi1 - fmi0 * fmi0);
+    vd *= 4.f / h;
+    vi *= 4.f / h;
+    a.out_d[idx] = make_float4(fd.x, fd.y, fd.z, vd);
+    a.out_i[idx] = make_float4(fi.x, fi.y, fi.z, vi);
+}
+
+struct AtrousArgs {
+    int W, H, step;
+    float sigma_depth, sigma_normal, sigma_light;
+    const float4 *in_d, *in_i;
+    float4 *out_d, *out_i;
+    const int *hlen;
+};
+
+// AtrousKernel (renderer.cuh:807-954).
+__global__ void k_svgf_atrous(AtrousArgs a, GB g) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.W || y >= a.H) return;
+    int idx = y * a.W + x;
+    int ch = max(a.hlen[idx], 1);
+    V3 cd = rgb(a.in_d, idx), ci = rgb(a.in_i, idx);
+    float cdl = luminance(cd), cil = luminance(ci);
+    float4 md = g.motion_depth[idx];
+    float cdepth = md.z, dz = fmaxf(md.w, 1e-4f);
+    ushort4 nm = g.normal_mat[idx], bm = g.bary_mesh[idx];
+    int cmat = nm.w, cmesh = bm.w;
+    V3 cn = decode_normal(nm);
+    const float vk[2] = {0.5f, 0.25f};
+    float fvd = 0.f, fvi = 0.f, fvw = 0.f;
+    for (int vj = -1; vj <= 1; vj++)
+        for (int vi = -1; vi <= 1; vi++) {
+            int sx = x + vi, sy = y + vj;
+            if (sx < 0 || sx >= a.W || sy < 0 || sy >= a.H) continue;
+            int k = sy * a.W + sx;
+            float w = vk[abs(vi)] * vk[abs(vj)];
+            fvd += w * fmaxf(0.0f, a.in_d[k].w);
+            fvi += w * fmaxf(0.0f, a.in_i[k].w);
+            fvw += w;
+        }
+    fvw = fmaxf(fvw, 1e-6f);
+    fvd /= fvw;
+    fvi /= fvw;
+    float sdd = sqrtf(fvd) + 1e-3f, sdi = sqrtf(fvi) + 1e-3f;
+    V3 fd{0.f, 0.f, 0.f}, fi{0.f, 0.f, 0.f};
+    float twd = 0.f, twi = 0.f, vard = 0.f, vari = 0.f;
+    float boot = fminf(1.f, fmaxf(0.f, (4.f - (float)ch) / 3.f));
+    float sdep = fmaxf(a.sigma_depth, 1e-3f) * fmaxf(dz, 1e-4f) * (1.f + 2.5f * boot);
+    float sld = a.sigma_light * (1.f + 2.0f * boot);
+    float sli = a.sigma_light * (1.f + 1.5f * boot);
+    float sn = fmaxf(8.f, a.sigma_normal * (1.f - 0.85f * boot));
+    const float kw[3] = {3.f / 8.f, 1.f / 4.f, 1.f / 16.f};
+    for (int kj = -2; kj <= 2; kj++)
+        for (int ki = -2; ki <= 2; ki++) {
+            int ni = x + ki * a.step, nj = y + kj * a.step;
+            if (!(ni >= 0 && ni < a.W && nj >= 0 && nj < a.H)) continue;
+            int nidx = nj * a.W + ni;
+            int nh = max(a.hlen[nidx], 1);
+            float nz = g.motion_depth[nidx].z;
+            ushort4 nnm = g.normal_mat[nidx], nbm = g.bary_mesh[nidx];
+            if (cmat != (int)nnm.w || cmesh != (int)nbm.w) continue;
+            V3 nn = decode_normal(nnm);
+            float4 nd4 = a.in_d[nidx], ni4 = a.in_i[nidx];
+            V3 nd{nd4.x, nd4.y, nd4.z}, nic{ni4.x, ni4.y, ni4.z};
+            float nvd = fmaxf(0.0f, nd4.w), nvi = fmaxf(0.0f, ni4.w);
+            float dist = sqrtf(float(ki * ki + kj * kj)) * a.step;
+            float wz = -fabsf(cdepth - nz) / (sdep * dist + 1e-6f);
+            float wn = powf(fmaxf(0.f, dot(cn, nn)), sn);
+            float ndl = luminance(nd), nil = luminance(nic);
+            float dref = fmaxf(fmaxf(cdl, ndl), 1e-4f), iref = fmaxf(cil, 1e-4f);
+            float wdl = -fabsf(cdl - ndl) / (sld * sdd / sqrtf(dref));
+            float wil = -fabsf(cil - nil) / (sli * sdi / sqrtf(iref));
+            float hc = boot > 0.f ? (0.5f + 0.5f * fminf((float)nh / 4.f, 1.f)) : 1.f;
+            float kwt = kw[abs(ki)] * kw[abs(kj)];
+            float dw = expf(wz + wdl) * wn * kwt * hc, iw = expf(wz + wil) * wn * kwt * hc;
+            fd = fd + dw * nd;
+            fi = fi + iw * nic;
+            twd += dw;
+            twi += iw;
+            vard += dw * dw * nvd;
+            vari += iw * iw * nvi;
+        }
+    if (twd > 1e-6f)
+        a.out_d[idx] = make_float4(fd.x / twd, fd.y / twd, fd.z / twd, vard / (twd * twd));
+    else
+        a.out_d[idx] = make_float4(cd.x, cd.y, cd.z, 1.f);
+    if (twi > 1e-6f)
+        a.out_i[idx] = make_float4(fi.x / twi, fi.y / twi, fi.z / twi, vari / (twi * twi));
+    else
+        a.out_i[idx] = make_float4(ci.x, ci.y, ci.z, 1.f);
+}
+
+// ---------------------------------------------------------------------------
+// host: state and frame
+// ---------------------------------------------------------------------------
+void SvgfState::allocate(int w, int h) {
+    release();
+    W = w;
+    H = h;
+    size_t n = (size_t)w * h;
+    for (int k = 0; k < 2; ++k) {
+        CRT_CUDA(cudaMalloc(&buf_d[k], n * sizeof(float4)));
+        CRT_CUDA(cudaMalloc(&buf_i[k], n * sizeof(float4)));
+        CRT_CUDA(cudaMalloc(&hist_d[k], n * sizeof(float4)));
+        CRT_CUDA(cudaMalloc(&hist_i[k], n * sizeof(float4)));
+        CRT_CUDA(cudaMalloc(&mom_d[k], n * sizeof(float2)));
+        CRT_CUDA(cudaMalloc(&mom_i[k], n * sizeof(float2)));
+        CRT_CUDA(cudaMalloc(&hlen[k], n * sizeof(int)));
+    }
+    reset_sync();
+}
+
+void SvgfState::reset_sync() {
+    size_t n = (size_t)W * H;
+    for (int k = 0; k < 2; ++k) {
+        CRT_CUDA(cudaMemset(hist_d[k], 0, n * sizeof(float4)));
+        CRT_CUDA(cudaMemset(hist_i[k], 0, n * sizeof(float4)));
+        CRT_CUDA(cudaMemset(mom_d[k], 0, n * sizeof(float2)));
+        CRT_CUDA(cudaMemset(mom_i[k], 0, n * sizeof(float2)));
+        CRT_CUDA(cudaMemset(hlen[k], 0, n * sizeof(int)));
+    }
+    t = 0;
+    first = true;
+}
+
+void SvgfState::release() {
+    for (int k = 0; k < 2; ++k) {
+        for (void **p : {(void **)&buf_d[k], (void **)&buf_i[k], (void **)&hist_d[k], (void **)&hist_i[k],
+                         (void **)&mom_d[k], (void **)&mom_i[k], (void **)&hlen[k]})
+            if (*p) {
+                cudaFree(*p);
+                *p = nullptr;
+            }
+    }
+}
+
+int svgf_frame(SvgfState &st, const DenoiseParams &p, const GBufferPlanes &cur, const GBufferPlanes &last,
+               const float4 *noisy_d, const float4 *noisy_i, float4 *out_d, float4 *out_i, cudaStream_t s) {
+    const int W = st.W, H = st.H;
+    const size_t bytes = (size_t)W * H * sizeof(float4);
+    dim3 b(16, 16), g((W + 15) / 16, (H + 15) / 16);
+    GB gc{cur.pos_tri, cur.normal_mat, cur.bary_mesh, cur.motion_depth};
+    GB gl{last.pos_tri, last.normal_mat, last.bary_mesh, last.motion_depth};
+    int c = 0;  // index of the buffer holding the current result
+    CRT_CUDA(cudaMemcpyAsync(st.buf_d[c], noisy_d, bytes, cudaMemcpyDeviceToDevice, s));
+    CRT_CUDA(cudaMemcpyAsync(st.buf_i[c], noisy_i, bytes, cudaMemcpyDeviceToDevice, s));
+    const int t = st.t;
+    TemporalArgs ta;
+    ta.W = W;
+    ta.H = H;
+    ta.max_hist = p.max_history_length;
+    ta.reproj = p.reprojection_depth_factor;
+    ta.cur_d = st.buf_d[c];
+    ta.cur_i = st.buf_i[c];
+    ta.hist_d = st.hist_d[1 - t];
+    ta.hist_i = st.hist_i[1 - t];
+    ta.mom_d = st.mom_d[t];
+    ta.mom_i = st.mom_i[t];
+    ta.lmom_d = st.mom_d[1 - t];
+    ta.lmom_i = st.mom_i[1 - t];
+    ta.hlen = st.hlen[t];
+    ta.lhlen = st.hlen[1 - t];
+    ta.first = st.first;
+    k_svgf_temporal<<<g, b, 0, s>>>(ta, gc, gl);
+    int launches = 1;
+    CRT_CUDA(cudaMemcpyAsync(st.hist_d[t], st.buf_d[c], bytes, cudaMemcpyDeviceToDevice, s));
+    CRT_CUDA(cudaMemcpyAsync(st.hist_i[t], st.buf_i[c], bytes, cudaMemcpyDeviceToDevice, s));
+    VarianceArgs va;
+    va.W = W;
+    va.H = H;
+    va.half = 7 / 2;
+    va.sigma_depth = p.sigma_depth;
+    va.sigma_normal = p.sigma_normal;
+    va.sigma_light = p.sigma_light;
+    va.in_d = st.buf_d[c];
+    va.in_i = st.buf_i[c];
+    va.out_d = st.buf_d[1 - c];
+    va.out_i = st.buf_i[1 - c];
+    va.mom_d = st.mom_d[t];
+    va.mom_i = st.mom_i[t];
+    va.hlen = st.hlen[t];
+    k_svgf_variance<<<g, b, 0, s>>>(va, gc);
+    ++launches;
+    c = 1 - c;
+    if (!st.first) {
+        int passes = p.atrous_iterations < 1 ? 1 : (p.atrous_iterations > 8 ? 8 : p.atrous_iterations);
+        for (int i = 0; i < passes; ++i) {
+            AtrousArgs aa;
+            aa.W = W;
+            aa.H = H;
+            aa.step = 1 << i;
+            aa.sigma_depth = p.sigma_depth;
+            aa.sigma_normal = p.sigma_normal;
+            aa.sigma_light = p.sigma_light;
+            aa.in_d = st.buf_d[c];
+            aa.in_i = st.buf_i[c];
+            aa.out_d = st.buf_d[1 - c];
+            aa.out_i = st.buf_i[1 - c];
+            aa.hlen = st.hlen[t];
+            k_svgf_atrous<<<g, b, 0, s>>>(aa, gc);
+            ++launches;
+            c = 1 - c;
+        }
+    }
+    CRT_CUDA(cudaGetLastError());
+    CRT_CUDA(cudaMemcpyAsync(out_d, st.buf_d[c], bytes, cudaMemcpyDeviceToDevice, s));
+    CRT_CUDA(cudaMemcpyAsync(out_i, st.buf_i[c], bytes, cudaMemcpyDeviceToDevice, s));
+    st.t = 1 - t;
+    st.first = false;
+    return launches;
+}
+
+}  // namespace crt

@@ -141,6 +141,43 @@ class Scene:
         _lib.call("crt_render_device_noalloc", self._h, int(first_sample), int(spp), direct.data_ptr(),
                   indirect.data_ptr(), sumsq.data_ptr() if sumsq is not None else None, C.c_void_p(s))
 
+    def gbuffer(self, prev_camera: dict | None = None, stream=None):
+        """Primary-hit G-buffer of the current camera (motion against
+        prev_camera, a dict as returned by camera()). Returns a dict of CUDA
+        tensors: pos_tri (H,W,4) f32, normal_mat (H,W,4) i16 bits of uint16,
+        bary_mesh (H,W,4) same, motion_depth (H,W,4) f32."""
+        import torch
+
+        rp = self.render_params()
+        h, w = rp["height"], rp["width"]
+        dev = torch.device("cuda", self.ctx.device)
+        g = {"pos_tri": torch.zeros((h, w, 4), dtype=torch.float32, device=dev),
+             "normal_mat": torch.zeros((h, w, 4), dtype=torch.int16, device=dev),
+             "bary_mesh": torch.zeros((h, w, 4), dtype=torch.int16, device=dev),
+             "motion_depth": torch.zeros((h, w, 4), dtype=torch.float32, device=dev)}
+        gb = _gbuffer_struct(g)
+        cam = None
+        if prev_camera is not None:
+            cam = _lib.Camera()
+            for k in range(3):
+                cam.target[k] = prev_camera["target"][k]
+            cam.distance = prev_camera["distance"]
+            cam.theta_deg, cam.phi_deg, cam.fovy_deg = prev_camera["theta_deg"], prev_camera["phi_deg"], \
+                prev_camera["fovy_deg"]
+        s = _torch_stream(dev, stream)
+        _lib.call("crt_gbuffer_from_primary", self._h, C.byref(cam) if cam is not None else None, C.byref(gb),
+                  C.c_void_p(s))
+        return g
+
+    def render_svgf_frame(self, svgf: "Svgf", frame_index: int, out_direct, out_indirect, params=None,
+                          stream=None) -> None:
+        """The reference's denoised frame: 1 spp + G-buffer + SVGF into CUDA
+        float32 tensors (H, W, 4) (rgb, variance)."""
+        s = _torch_stream(out_direct.device, stream)
+        p = params if params is not None else default_denoise_params()
+        _lib.call("crt_render_svgf_frame", self._h, svgf.handle, C.byref(p), int(frame_index), out_direct.data_ptr(),
+                  out_indirect.data_ptr(), C.c_void_p(s))
+
     def export_geometry(self):
         n = self.info()["num_triangles"]
         v = np.empty((n, 9), np.float32)
@@ -219,3 +256,58 @@ class Scene:
 def hit_prims(hits: np.ndarray) -> np.ndarray:
     """Primitive ids (int32) stored in column 1 of a hit array."""
     return np.ascontiguousarray(hits[:, 1]).view(np.int32)
+
+
+def _gbuffer_struct(g: dict):
+    gb = _lib.GBuffer()
+    gb.pos_tri = g["pos_tri"].data_ptr()
+    gb.normal_mat = g["normal_mat"].data_ptr()
+    gb.bary_mesh = g["bary_mesh"].data_ptr()
+    gb.motion_depth = g["motion_depth"].data_ptr()
+    return gb
+
+
+def default_denoise_params() -> "_lib.DenoiseParams":
+    """DenoiseParam defaults (Src/Utils/ui.h:14-25)."""
+    p = _lib.DenoiseParams()
+    _lib.call("crt_denoise_params_default", C.byref(p))
+    return p
+
+
+class Svgf:
+    """SVGF state (temporal history, moments, history lengths) for one image
+    size: TemporalDenoising + ComputeVarianceKernel + AtrousKernel of the
+    reference, over device buffers."""
+
+    def __init__(self, ctx: Context, width: int, height: int):
+        self.ctx = ctx
+        self.width, self.height = width, height
+        self._h = C.c_void_p()
+        _lib.call("crt_svgf_create", ctx.handle, int(width), int(height), C.byref(self._h))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def reset(self) -> None:
+        _lib.call("crt_svgf_reset", self._h)
+
+    def frame(self, cur_gbuffer: dict, prev_gbuffer: dict, noisy_direct, noisy_indirect, out_direct, out_indirect,
+              params=None, stream=None) -> None:
+        """One SVGF frame over CUDA float32 (H, W, 4) tensors."""
+        s = _torch_stream(noisy_direct.device, stream)
+        p = params if params is not None else default_denoise_params()
+        cur, prev = _gbuffer_struct(cur_gbuffer), _gbuffer_struct(prev_gbuffer)
+        _lib.call("crt_svgf_frame", self._h, C.byref(p), C.byref(cur), C.byref(prev), noisy_direct.data_ptr(),
+                  noisy_indirect.data_ptr(), out_direct.data_ptr(), out_indirect.data_ptr(), C.c_void_p(s))
+
+    def close(self):
+        if self._h:
+            _lib.lib().crt_svgf_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -186,6 +186,67 @@ crt_status crt_render_device(crt_scene *scene, int32_t first_sample, int32_t spp
 crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_sample, int32_t spp, float *d_direct,
                                      float *d_indirect, float *d_sumsq, void *stream);
 
+/* ---- SVGF denoising ---------------------------------------------------- */
+
+/* G-buffer planes in device memory, width*height entries each, rows
+ * bottom-up, with the encodings of the reference's raster G-buffer
+ * (Shader/gbuffer.fs:16-38; Src/Core/renderer.cuh:32-54):
+ *   pos_tri      4 floats  world position, triangle index within its mesh
+ *   normal_mat   4 uint16  uint((n*0.5+0.5)*65535) of the interpolated normal, material id
+ *   bary_mesh    4 uint16  uint(barycentrics*65535), mesh id + 1
+ *   motion_depth 4 floats  NDC motion (current - previous camera), linear depth, fwidth(depth)
+ * Background pixels are all zero. */
+typedef struct crt_gbuffer {
+    float *pos_tri;
+    uint16_t *normal_mat;
+    uint16_t *bary_mesh;
+    float *motion_depth;
+} crt_gbuffer;
+
+/* DenoiseParam (Src/Utils/ui.h:14-25). */
+typedef struct crt_denoise_params {
+    int32_t max_history_length; /* 24 */
+    float sigma_light;          /* 8 */
+    float sigma_normal;         /* 256 */
+    float sigma_depth;          /* 1 */
+    float reprojection_depth_factor; /* 0.1 */
+    int32_t atrous_iterations;  /* 5 */
+} crt_denoise_params;
+
+typedef struct crt_svgf crt_svgf;
+
+crt_status crt_denoise_params_default(crt_denoise_params *p);
+
+/* G-buffer of the scene's current camera from primary rays through pixel
+ * centres (nearest surface of either facing, as the reference's raster pass
+ * without culling); motion vectors against `prev` (NULL = the current
+ * camera, i.e. no motion). Replaces RenderGBuffer (renderer.cuh:1446-1503). */
+crt_status crt_gbuffer_from_primary(crt_scene *scene, const crt_camera *prev, const crt_gbuffer *out,
+                                    void *stream);
+
+/* SVGF state (temporal history, moments, history lengths) for a w x h image. */
+crt_status crt_svgf_create(crt_ctx *ctx, int32_t width, int32_t height, crt_svgf **out);
+void crt_svgf_free(crt_svgf *s);
+/* Clears the history; the next frame is a first frame. */
+crt_status crt_svgf_reset(crt_svgf *s);
+
+/* One SVGF frame over device buffers (float4 per pixel, rgb used): temporal
+ * reprojection against the history (TemporalDenoising, renderer.cuh:524),
+ * 7x7 variance estimate while history < 4 (ComputeVarianceKernel, :689) and
+ * atrous_iterations a-trous passes at steps 1, 2, 4, ... (AtrousKernel, :807;
+ * none on the first frame), in the order of RenderLoop's denoise block
+ * (:1208-1258). Outputs are float4 (rgb, variance). */
+crt_status crt_svgf_frame(crt_svgf *s, const crt_denoise_params *p, const crt_gbuffer *cur, const crt_gbuffer *prev,
+                          const float *noisy_direct, const float *noisy_indirect, float *out_direct,
+                          float *out_indirect, void *stream);
+
+/* The reference's denoised frame (renderParam.denoise, renderer.cuh:1144-1304):
+ * renders 1 sample per pixel (sample index = frame_index), builds the
+ * G-buffer against the camera of the previous frame of this state, runs
+ * SVGF and writes the denoised direct/indirect float4 planes (device). */
+crt_status crt_render_svgf_frame(crt_scene *scene, crt_svgf *s, const crt_denoise_params *p, int32_t frame_index,
+                                 float *out_direct, float *out_indirect, void *stream);
+
 /* ---- ray queries ------------------------------------------------------ */
 
 /* Closest hit for n rays in host memory (BVH::IsIntersect, Src/Core/bvh.cu:253

@@ -294,6 +294,8 @@ def ref_render_lib() -> C.CDLL:
         L.refr_load.argtypes = [C.c_char_p]
         L.refr_info.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float), _VP]
         L.refr_render.argtypes = [_VP, C.c_int, C.c_int, _VP, _VP, _VP, C.POINTER(C.c_float)]
+        L.refr_svgf.argtypes = [C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP, _VP, C.c_int, C.c_float,
+                                C.c_float, C.c_float, C.c_float, C.c_int, _VP, _VP]
         _refrender = L
     return _refrender
 
@@ -329,3 +331,25 @@ class RefRenderer:
         if rc:
             raise RuntimeError(f"reference render failed: cudaError {rc}")
         return d, i, q, ms.value
+
+
+def ref_svgf(noisy_d, noisy_i, pos_tri, normal_mat, bary_mesh, motion_depth, max_history=24, sigma_light=8.0,
+             sigma_normal=256.0, sigma_depth=1.0, reproj=0.1, atrous=5):
+    """The reference's SVGF kernels (headless CUDA build) over a frame
+    sequence: arrays of shape (F, H, W, 4) (normal_mat / bary_mesh uint16).
+    Returns (out_direct, out_indirect), float32 (F, H, W, 4)."""
+    nd = np.ascontiguousarray(noisy_d, np.float32)
+    ni = np.ascontiguousarray(noisy_i, np.float32)
+    gp = np.ascontiguousarray(pos_tri, np.float32)
+    gn = np.ascontiguousarray(normal_mat, np.uint16)
+    gb = np.ascontiguousarray(bary_mesh, np.uint16)
+    gm = np.ascontiguousarray(motion_depth, np.float32)
+    f, h, w, _ = nd.shape
+    od = np.zeros_like(nd)
+    oi = np.zeros_like(ni)
+    rc = ref_render_lib().refr_svgf(w, h, f, nd.ctypes.data, ni.ctypes.data, gp.ctypes.data, gn.ctypes.data,
+                                    gb.ctypes.data, gm.ctypes.data, max_history, sigma_light, sigma_normal,
+                                    sigma_depth, reproj, atrous, od.ctypes.data, oi.ctypes.data)
+    if rc:
+        raise RuntimeError(f"reference SVGF failed: cudaError {rc}")
+    return od, oi

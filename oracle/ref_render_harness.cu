@@ -146,3 +146,129 @@ int refr_render(void *h, int spp, int max_bounces, float *out_direct, float *out
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The reference's SVGF kernels on caller-provided inputs: the denoise block of
+// RenderLoop (renderer.cuh:1207-1258, with the index flips of :1299-1304) for
+// `frames` consecutive frames. Inputs per frame (host, w*h*4 each): noisy
+// direct/indirect (rgb), G-buffer planes with the raster encodings. Outputs
+// per frame: the final direct/indirect buffers (rgb + variance).
+// ---------------------------------------------------------------------------
+namespace {
+cudaArray_t make_array(cudaChannelFormatDesc d, int w, int h) {
+    cudaArray_t a;
+    cudaMallocArray(&a, &d, w, h);
+    return a;
+}
+}  // namespace
+
+extern "C" int refr_svgf(int w, int h, int frames, const float *noisy_d, const float *noisy_i, const float *gb_pos,
+                         const unsigned short *gb_nm, const unsigned short *gb_bm, const float *gb_md,
+                         int max_history, float sigma_light, float sigma_normal, float sigma_depth, float reproj,
+                         int atrous, float *out_d, float *out_i) {
+    const int n = w * h;
+    renderParam.width = w;
+    renderParam.height = h;
+    DenoiseParam dp;
+    dp.maxHistoryLength = max_history;
+    dp.sigmaLight = sigma_light;
+    dp.sigmaNormal = sigma_normal;
+    dp.sigmaDepth = sigma_depth;
+    dp.reprojectionDepthFactor = reproj;
+    dp.atrousIterations = atrous;
+    dp.currentTemporalBufferIndex = 0;
+    for (int i = 0; i < 2; i++) {
+        cudaMalloc(&dp.directMoments[i], sizeof(float2) * n);
+        cudaMalloc(&dp.indirectMoments[i], sizeof(float2) * n);
+        cudaMalloc(&dp.historyLength[i], sizeof(int) * n);
+        cudaMemset(dp.directMoments[i], 0, sizeof(float2) * n);
+        cudaMemset(dp.indirectMoments[i], 0, sizeof(float2) * n);
+        cudaMemset(dp.historyLength[i], 0, sizeof(int) * n);
+    }
+    RenderBuffer rbs[2], hist[2];
+    for (int i = 0; i < 2; i++) {
+        cudaMalloc(&rbs[i].directLightingBuffer, sizeof(float) * 4 * n);
+        cudaMalloc(&rbs[i].indirectLightingBuffer, sizeof(float) * 4 * n);
+        cudaMalloc(&hist[i].directLightingBuffer, sizeof(float) * 4 * n);
+        cudaMalloc(&hist[i].indirectLightingBuffer, sizeof(float) * 4 * n);
+        cudaMemset(hist[i].directLightingBuffer, 0, sizeof(float) * 4 * n);
+        cudaMemset(hist[i].indirectLightingBuffer, 0, sizeof(float) * 4 * n);
+    }
+    GBuffer gbs[2];
+    cudaArray_t arrs[2][4];
+    for (int i = 0; i < 2; i++) {
+        arrs[i][0] = make_array(cudaCreateChannelDesc<float4>(), w, h);
+        arrs[i][1] = make_array(cudaCreateChannelDesc<ushort4>(), w, h);
+        arrs[i][2] = make_array(cudaCreateChannelDesc<ushort4>(), w, h);
+        arrs[i][3] = make_array(cudaCreateChannelDesc<float4>(), w, h);
+        for (int k = 0; k < 4; k++) {
+            cudaArray_t a = arrs[i][k];
+            cudaTextureObject_t t = CreateTextureObject(a, cudaAddressModeClamp, cudaFilterModePoint,
+                                                        cudaReadModeElementType);
+            if (k == 0) gbs[i].cudaTexObjPositionTriID = t;
+            if (k == 1) gbs[i].cudaTexObjNormalMatID = t;
+            if (k == 2) gbs[i].cudaTexObjBaryMeshID = t;
+            if (k == 3) gbs[i].cudaTexObjMotionDepth = t;
+        }
+        gbs[i].width = w;
+        gbs[i].height = h;
+    }
+    int cur = 0, gi = 0;
+    bool firstFrame = true;
+    dim3 grid((w + denoiseBlockSize.x - 1) / denoiseBlockSize.x, (h + denoiseBlockSize.y - 1) / denoiseBlockSize.y);
+    for (int f = 0; f < frames; ++f) {
+        size_t off = (size_t)f * n * 4;
+        cudaMemcpy2DToArray(arrs[gi][0], 0, 0, gb_pos + off, w * 16, w * 16, h, cudaMemcpyHostToDevice);
+        cudaMemcpy2DToArray(arrs[gi][1], 0, 0, gb_nm + off, w * 8, w * 8, h, cudaMemcpyHostToDevice);
+        cudaMemcpy2DToArray(arrs[gi][2], 0, 0, gb_bm + off, w * 8, w * 8, h, cudaMemcpyHostToDevice);
+        cudaMemcpy2DToArray(arrs[gi][3], 0, 0, gb_md + off, w * 16, w * 16, h, cudaMemcpyHostToDevice);
+        RenderBuffer renderBuffer = rbs[cur];
+        cudaMemcpy(renderBuffer.directLightingBuffer, noisy_d + off, sizeof(float) * 4 * n, cudaMemcpyHostToDevice);
+        cudaMemcpy(renderBuffer.indirectLightingBuffer, noisy_i + off, sizeof(float) * 4 * n, cudaMemcpyHostToDevice);
+        int t = dp.currentTemporalBufferIndex;
+        RenderBuffer histCur = hist[t], histLast = hist[1 - t];
+        GBuffer gBuffer = gbs[gi], lastGBuffer = gbs[1 - gi];
+        TemporalDenoiseKernel<<<grid, denoiseBlockSize>>>(dp, cameraParam, renderParam, renderBuffer, histLast, gBuffer,
+                                                          lastGBuffer, firstFrame);
+        cudaDeviceSynchronize();
+        cudaMemcpy(histCur.directLightingBuffer, renderBuffer.directLightingBuffer, sizeof(float) * 4 * n,
+                   cudaMemcpyDeviceToDevice);
+        cudaMemcpy(histCur.indirectLightingBuffer, renderBuffer.indirectLightingBuffer, sizeof(float) * 4 * n,
+                   cudaMemcpyDeviceToDevice);
+        ComputeVarianceKernel<<<grid, denoiseBlockSize>>>(dp, renderParam, rbs[cur], rbs[1 - cur], gBuffer, 7);
+        cudaDeviceSynchronize();
+        cur = 1 - cur;
+        if (!firstFrame) {
+            int passes = max(1, min(8, dp.atrousIterations));
+            for (int i = 0; i < passes; i++) {
+                AtrousKernel<<<grid, denoiseBlockSize>>>(dp, cameraParam, renderParam, rbs[cur], rbs[1 - cur], gBuffer,
+                                                         1 << i);
+                cudaDeviceSynchronize();
+                cur = 1 - cur;
+            }
+        }
+        cudaMemcpy(out_d + off, rbs[cur].directLightingBuffer, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost);
+        cudaMemcpy(out_i + off, rbs[cur].indirectLightingBuffer, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost);
+        // end of frame (renderer.cuh:1299-1304)
+        cur = 1 - cur;
+        gi = 1 - gi;
+        dp.currentTemporalBufferIndex = 1 - dp.currentTemporalBufferIndex;
+        firstFrame = false;
+    }
+    int err = (int)cudaGetLastError();
+    for (int i = 0; i < 2; i++) {
+        cudaFree(dp.directMoments[i]);
+        cudaFree(dp.indirectMoments[i]);
+        cudaFree(dp.historyLength[i]);
+        cudaFree(rbs[i].directLightingBuffer);
+        cudaFree(rbs[i].indirectLightingBuffer);
+        cudaFree(hist[i].directLightingBuffer);
+        cudaFree(hist[i].indirectLightingBuffer);
+        cudaDestroyTextureObject(gbs[i].cudaTexObjPositionTriID);
+        cudaDestroyTextureObject(gbs[i].cudaTexObjNormalMatID);
+        cudaDestroyTextureObject(gbs[i].cudaTexObjBaryMeshID);
+        cudaDestroyTextureObject(gbs[i].cudaTexObjMotionDepth);
+        for (int k = 0; k < 4; k++) cudaFreeArray(arrs[i][k]);
+    }
+    return err;
+}
