@@ -223,6 +223,52 @@ def render_leg(ctx, steps, stream, with_reference=True):
     return out
 
 
+def batch_leg(ctx, stream):
+    """Batched persistent wavefront (survey config C3): 64 orbit views of
+    the Cornell box (radius 3, elevation U[-30, 30] deg, seeded), 512x512,
+    16 spp, depth 12, all views in shared wavefronts with a CUDA graph per
+    pass and an autotuned wavefront size, against 64 sequential single-view
+    renders of the same cameras."""
+    import tempfile
+
+    import torch
+
+    from cudaraytracer_b200 import Scene, scenes
+    from cudaraytracer_b200.autotune import autotune_paths_per_pass, orbit_views
+
+    td = tempfile.mkdtemp(prefix="crt_batch_")
+    sc = Scene.load(ctx, scenes.cornell_box(width=512, height=512, spp=16, max_bounces=12).write(td, "cb"))
+    views = orbit_views(sc, 64, radius=3.0, max_elev_deg=30.0, seed=1)
+    spp = 16
+    tune = autotune_paths_per_pass(sc, views, probe_spp=1,
+                                   candidates=(2 << 20, 4 << 20, 8 << 20, 16 << 20))
+    rp = sc.render_params()
+    shape = (len(views), rp["height"], rp["width"], 4)
+    d = torch.zeros(shape, device="cuda")
+    i = torch.zeros(shape, device="cuda")
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record(stream)
+    sc.render_views(views, d, i, spp, stream=stream.cuda_stream)
+    e[1].record(stream)
+    sd = torch.zeros(shape[1:], device="cuda")
+    si = torch.zeros(shape[1:], device="cuda")
+    torch.cuda.synchronize()
+    e[2].record(stream)
+    for v in views:
+        sc.set_camera_orbit(v["target"], v["distance"], v["theta_deg"], v["phi_deg"], v["fovy_deg"])
+        sc.render_device(sd, si, spp, stream=stream.cuda_stream)
+    e[3].record(stream)
+    torch.cuda.synchronize()
+    bms, sms = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
+    samples = len(views) * rp["width"] * rp["height"] * spp
+    sc.close()
+    return {"workload": "64 views x 512x512 x 16 spp, Cornell box, depth 12", "batched_ms": round(bms, 2),
+            "sequential_ms": round(sms, 2), "speedup": round(sms / bms, 3),
+            "batched_msamples_per_s": round(samples / (bms * 1e-3) / 1e6, 1),
+            "sequential_msamples_per_s": round(samples / (sms * 1e-3) / 1e6, 1),
+            "paths_per_pass": tune["paths_per_pass"], "autotune_ms": tune.get("timings_ms")}
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU implementation of the path
     (rank 0 only), on the same scene, metric and unit."""
@@ -275,6 +321,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA traversal")
     ap.add_argument("--no-render", action="store_true", help="skip the full-frame render leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view leg")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays (and shadow queries) per step per GPU")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -349,6 +396,9 @@ def main():
     render = None
     if rank == 0 and not args.no_render:
         render = render_leg(ctx, max(2, min(args.steps, 8)), stream, with_reference=not args.no_ref_cuda)
+    batch = None
+    if rank == 0 and not args.no_batch:
+        batch = batch_leg(ctx, stream)
 
     # e2e through the host-buffer API: pinned host inputs, results back.
     pin_r = torch.from_numpy(rays_np).pin_memory()
@@ -418,6 +468,7 @@ def main():
                     "h2d_bytes_per_step": N_RAYS * (32 + 48), "d2h_bytes_per_step": N_RAYS * (16 + 1)},
             "reference_cuda": ref_cuda,
             "render": render,
+            "batch": batch,
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
         }

@@ -67,7 +67,7 @@ class RenderParams(C.Structure):
         ("rr_start_bounce", C.c_int32),
         ("seed", C.c_uint64),
         ("spp_per_pass", C.c_int32),
-        ("reserved", C.c_int32),
+        ("paths_per_pass", C.c_int32),
     ]
 
 
@@ -137,6 +137,7 @@ _SIGS = {
     "crt_render": (C.c_int, [_VP, C.c_int32, _VP, _VP, _VP]),
     "crt_render_device": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
     "crt_render_device_noalloc": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
+    "crt_render_views": (C.c_int, [_VP, C.c_int32, _VP, C.c_int32, C.c_int32, _VP, _VP, _VP, C.c_int32, _VP]),
     "crt_denoise_params_default": (C.c_int, [C.POINTER(DenoiseParams)]),
     "crt_gbuffer_from_primary": (C.c_int, [_VP, C.POINTER(Camera), C.POINTER(GBuffer), _VP]),
     "crt_svgf_create": (C.c_int, [_VP, C.c_int32, C.c_int32, C.POINTER(_VP)]),

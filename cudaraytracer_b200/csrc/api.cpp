@@ -23,8 +23,21 @@ DeviceScratch::~DeviceScratch() {
 }
 
 Scene::~Scene() {
+    if (scratch_done) {
+        cudaEventSynchronize(scratch_done);
+        cudaEventDestroy(scratch_done);
+    }
     free_bvh(bvh);
     if (d_verts) cudaFree(d_verts);
+}
+
+void Scene::acquire_scratch(cudaStream_t s) {
+    if (scratch_done) CRT_CUDA(cudaStreamWaitEvent(s, scratch_done, 0));
+}
+
+void Scene::release_scratch(cudaStream_t s) {
+    if (!scratch_done) CRT_CUDA(cudaEventCreateWithFlags(&scratch_done, cudaEventDisableTiming));
+    CRT_CUDA(cudaEventRecord(scratch_done, s));
 }
 
 void Scene::fill_info(crt_scene_info_t &info) const {
@@ -277,6 +290,7 @@ crt_status crt_get_render_params(const crt_scene *scene, crt_render_params *p) {
         p->rr_start_bounce = scene->rp.rr_start_bounce;
         p->seed = scene->rp.seed;
         p->spp_per_pass = scene->rp.spp_per_pass;
+        p->paths_per_pass = scene->rp.paths_per_pass;
     });
 }
 
@@ -285,8 +299,8 @@ crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p) {
         CRT_CHECK(scene && p && scene->renderable, CRT_ERR_INVALID, "crt_set_render_params: not a loaded scene");
         CRT_CHECK(p->width > 0 && p->height > 0 && (int64_t)p->width * p->height < (1 << 30), CRT_ERR_INVALID,
                   "crt_set_render_params: bad resolution");
-        CRT_CHECK(p->spp >= 0 && p->max_bounces >= 0 && p->spp_per_pass >= 0, CRT_ERR_INVALID,
-                  "crt_set_render_params: negative count");
+        CRT_CHECK(p->spp >= 0 && p->max_bounces >= 0 && p->spp_per_pass >= 0 && p->paths_per_pass >= 0,
+                  CRT_ERR_INVALID, "crt_set_render_params: negative count");
         bool resized = p->width != scene->rp.width || p->height != scene->rp.height;
         scene->rp.width = p->width;
         scene->rp.height = p->height;
@@ -296,6 +310,7 @@ crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p) {
         scene->rp.rr_start_bounce = p->rr_start_bounce;
         scene->rp.seed = p->seed;
         scene->rp.spp_per_pass = p->spp_per_pass;
+        scene->rp.paths_per_pass = p->paths_per_pass;
         if (resized) {
             scene->cam.width = p->width;
             scene->cam.height = p->height;
@@ -351,8 +366,10 @@ crt_status crt_render_device(crt_scene *scene, int32_t first_sample, int32_t spp
         acc.indirect = (float4 *)d_indirect;
         acc.sumsq = (float4 *)d_sumsq;
         acc.pixels = (size_t)scene->rp.width * scene->rp.height;
+        scene->acquire_scratch(s);
         if (spp > 0)
             render_samples(make_view(scene->bvh, scene->rd), scene->cam, scene->rp, first_sample, spp, scene->wf, acc, s);
+        scene->release_scratch(s);
     });
 }
 
@@ -364,6 +381,8 @@ crt_status crt_render(crt_scene *scene, int32_t spp, float *direct, float *indir
         cudaStream_t s = scene->ctx->stream;
         size_t px = (size_t)scene->rp.width * scene->rp.height;
         size_t bytes = px * sizeof(float4);
+        scene->acquire_scratch(s);
+        CRT_CUDA(cudaStreamSynchronize(s));  // the accumulators may be reallocated below
         scene->accum.reserve(3 * bytes);
         char *base = (char *)scene->accum.p;
         CRT_CUDA(cudaMemsetAsync(base, 0, 3 * bytes, s));
@@ -377,6 +396,7 @@ crt_status crt_render(crt_scene *scene, int32_t spp, float *direct, float *indir
         if (direct) CRT_CUDA(cudaMemcpyAsync(direct, acc.direct, bytes, cudaMemcpyDeviceToHost, s));
         if (indirect) CRT_CUDA(cudaMemcpyAsync(indirect, acc.indirect, bytes, cudaMemcpyDeviceToHost, s));
         if (sumsq) CRT_CUDA(cudaMemcpyAsync(sumsq, acc.sumsq, bytes, cudaMemcpyDeviceToHost, s));
+        scene->release_scratch(s);
         CRT_CUDA(cudaStreamSynchronize(s));
     });
 }
@@ -523,6 +543,7 @@ crt_status crt_render_svgf_frame(crt_scene *scene, crt_svgf *s, const crt_denois
                 CRT_CUDA(cudaMemsetAsync(s->gb[k].motion_depth, 0, n * sizeof(float4), st));
             }
         }
+        scene->acquire_scratch(st);
         // framebufferReset: each denoised frame starts from cleared buffers
         CRT_CUDA(cudaMemsetAsync(s->noisy_d, 0, n * sizeof(float4), st));
         CRT_CUDA(cudaMemsetAsync(s->noisy_i, 0, n * sizeof(float4), st));
@@ -536,6 +557,7 @@ crt_status crt_render_svgf_frame(crt_scene *scene, crt_svgf *s, const crt_denois
                              scene->bvh.bounds_max, s->gb[s->gi], st);
         svgf_frame(s->st, to_params(p), s->gb[s->gi], s->gb[1 - s->gi], s->noisy_d, s->noisy_i, (float4 *)out_direct,
                    (float4 *)out_indirect, st);
+        scene->release_scratch(st);
         s->gi = 1 - s->gi;
         s->prev_cam = scene->cam;
         s->have_prev_cam = true;

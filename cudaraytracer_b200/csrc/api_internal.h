@@ -7,6 +7,7 @@
 #include "scene_data.h"
 #include "svgf.h"
 #include <memory>
+#include <vector>
 #include <new>
 #include <exception>
 
@@ -63,12 +64,25 @@ struct Scene {
     RenderParams rp;
     Wavefront wf;
     DeviceScratch accum;  // host-API render accumulators
+    DeviceScratch batch_scratch;  // multi-view cameras + pass state
+    // Every call that uses the wavefront/accumulator scratch waits for the
+    // previous such call's work (whatever stream it ran on) and records its
+    // own completion here, so calls on different streams cannot overlap on
+    // the shared buffers.
+    cudaEvent_t scratch_done = nullptr;
+    void acquire_scratch(cudaStream_t s);
+    void release_scratch(cudaStream_t s);
     ~Scene();
     void fill_info(crt_scene_info_t &info) const;
 };
 }  // namespace crt
 
 struct crt_scene : crt::Scene {};
+
+namespace crt {
+int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_sample, int spp, const Accum &acc,
+                 bool use_graph, cudaStream_t stream);
+}
 
 struct crt_svgf {
     crt_ctx *ctx = nullptr;

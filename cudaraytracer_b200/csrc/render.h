@@ -14,6 +14,7 @@ struct RenderParams {
     int rr_start_bounce = 0;  // extension; 0 = reference (RR at every shading event)
     uint64_t seed = 1;
     int spp_per_pass = 0;     // samples per wavefront; 0 = automatic
+    int paths_per_pass = 0;   // paths per wavefront of multi-view batches; 0 = 8M
 };
 
 // Device-resident render data of a scene (everything but the BVH).

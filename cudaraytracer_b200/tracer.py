@@ -91,7 +91,7 @@ class Scene:
     def render_params(self) -> dict:
         p = _lib.RenderParams()
         _lib.call("crt_get_render_params", self._h, C.byref(p))
-        return {k: getattr(p, k) for k, _ in p._fields_ if k != "reserved"}
+        return {k: getattr(p, k) for k, _ in p._fields_}
 
     def set_render_params(self, **kw) -> None:
         p = _lib.RenderParams()
@@ -177,6 +177,23 @@ class Scene:
         p = params if params is not None else default_denoise_params()
         _lib.call("crt_render_svgf_frame", self._h, svgf.handle, C.byref(p), int(frame_index), out_direct.data_ptr(),
                   out_indirect.data_ptr(), C.c_void_p(s))
+
+    def render_views(self, cameras, direct, indirect, spp: int, first_sample: int = 0, sumsq=None,
+                     use_graph: bool = True, stream=None) -> None:
+        """Batched rendering of several orbit cameras (dicts with target,
+        distance, theta_deg, phi_deg, fovy_deg) into view-major CUDA float32
+        tensors of shape (n_views, H, W, 4)."""
+        n = len(cameras)
+        arr = (_lib.Camera * n)()
+        for i, c in enumerate(cameras):
+            for k in range(3):
+                arr[i].target[k] = c["target"][k]
+            arr[i].distance = c["distance"]
+            arr[i].theta_deg, arr[i].phi_deg, arr[i].fovy_deg = c["theta_deg"], c["phi_deg"], c["fovy_deg"]
+        s = _torch_stream(direct.device, stream)
+        _lib.call("crt_render_views", self._h, n, arr, int(first_sample), int(spp), direct.data_ptr(),
+                  indirect.data_ptr(), sumsq.data_ptr() if sumsq is not None else None, 1 if use_graph else 0,
+                  C.c_void_p(s))
 
     def export_geometry(self):
         n = self.info()["num_triangles"]

@@ -139,8 +139,8 @@ typedef struct crt_render_params {
     float rr;                 /* Russian-roulette continuation probability */
     int32_t rr_start_bounce;  /* extension: first bounce that applies RR; 0 = reference */
     uint64_t seed;            /* PCG32 seed of the per-path streams */
-    int32_t spp_per_pass;     /* samples per wavefront; 0 = automatic */
-    int32_t reserved;
+    int32_t spp_per_pass;     /* samples per wavefront of crt_render*; 0 = automatic */
+    int32_t paths_per_pass;   /* paths per wavefront of crt_render_views; 0 = 8M */
 } crt_render_params;
 
 crt_status crt_get_render_params(const crt_scene *scene, crt_render_params *p);
@@ -185,6 +185,18 @@ crt_status crt_render_device(crt_scene *scene, int32_t first_sample, int32_t spp
  * Renderer::CudaInit). */
 crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_sample, int32_t spp, float *d_direct,
                                      float *d_indirect, float *d_sumsq, void *stream);
+
+/* Batched multi-view rendering (no reference counterpart: the reference
+ * renders one view, one sample per pixel per frame). Renders samples
+ * [first_sample, first_sample + spp) of n_views orbit cameras (same
+ * resolution as the scene's render params) into view-major device
+ * accumulators of n_views*width*height float4 each. All views' paths share
+ * wavefronts of paths_per_pass paths; with use_graph != 0 one pass (raygen,
+ * max_bounces x (extend, shade, shadow), pass advance) is captured once as a
+ * CUDA graph and replayed. Asynchronous on `stream`. */
+crt_status crt_render_views(crt_scene *scene, int32_t n_views, const crt_camera *cams, int32_t first_sample,
+                            int32_t spp, float *d_direct, float *d_indirect, float *d_sumsq, int32_t use_graph,
+                            void *stream);
 
 /* ---- SVGF denoising ---------------------------------------------------- */
 
