@@ -269,6 +269,55 @@ def batch_leg(ctx, stream):
             "paths_per_pass": tune["paths_per_pass"], "autotune_ms": tune.get("timings_ms")}
 
 
+def serve_leg(ctx, quick=False):
+    """Serving (survey config C4) on a bounded sample. 8 resident scenes of
+    the icosphere-field generator with {1, 4, 8, 16, 32, 64, 128, 256}
+    level-5 spheres (20k to 5.2M triangles, 2048x1024 env each). Requests
+    draw resolution from {256^2, 512^2, 1280x720, 1920x1080}, spp from
+    {1, 4, 16, 64} and a random orbit pose. Poisson arrivals at 5, 20 and
+    80 per second (40, 120 and 320 requests instead of 2,000 per rate) and a
+    saturated burst (160 requests at t=0), each served by crt_server
+    (continuous batching, HBM budget 150 GiB, 8M-path wavefronts) and by the
+    one-request-at-a-time loop (Scene.render_device per request) over the
+    same requests. Latency = completion - arrival (host clock)."""
+    from cudaraytracer_b200 import Scene, scenes
+    from cudaraytracer_b200.serve import Server, poisson_requests, run_one_at_a_time, run_served
+
+    counts = (1, 4, 8, 16, 32, 64, 128, 256)
+    t0 = time.perf_counter()
+    scs = [Scene.from_spec(ctx, scenes.icosphere_field(n_spheres=c, seed=100 + k)) for k, c in enumerate(counts)]
+    load_s = time.perf_counter() - t0
+    cams = [sc.camera() for sc in scs]
+    res = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
+    spps = [1, 4, 16, 64]
+    srv = Server(ctx, hbm_budget_bytes=150 << 30, paths_per_pass=8 << 20, passes_in_flight=2)
+    for sc in scs:
+        srv.add_scene(sc)
+    warm = poisson_requests(8, 0.0, cams, res, [1, 4], seed=99)
+    run_served(srv, warm)
+    run_one_at_a_time(scs, warm)
+    plan = [(5.0, 40), (20.0, 120), (80.0, 320)] if not quick else [(80.0, 48)]
+    out = {"workload": "8 resident icosphere-field scenes (1..256 level-5 spheres, 20k-5.2M tris); requests of "
+                       "{256^2, 512^2, 1280x720, 1920x1080} x {1, 4, 16, 64} spp, random poses",
+           "scenes_tris": [int(sc.info()["num_triangles"]) for sc in scs], "scene_build_s": round(load_s, 2),
+           "hbm": {k: v for k, v in srv.stats().items() if k.startswith("bytes")}, "rates": {}}
+    for rate, n in plan:
+        reqs = poisson_requests(n, rate, cams, res, spps, seed=int(rate))
+        served = run_served(srv, reqs)
+        plain = run_one_at_a_time(scs, reqs)
+        out["rates"][f"{rate:g}/s"] = {"served": served, "one_at_a_time": plain}
+    burst = poisson_requests(160 if not quick else 32, 0.0, cams, res, spps, seed=7)
+    served = run_served(srv, burst)
+    plain = run_one_at_a_time(scs, burst)
+    out["saturated"] = {"served": served, "one_at_a_time": plain,
+                        "req_per_s_ratio": round(served["req_per_s"] / plain["req_per_s"], 3)}
+    out["server_stats"] = {k: v for k, v in srv.stats().items() if k in ("passes", "paths")}
+    srv.close()
+    for sc in scs:
+        sc.close()
+    return out
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU implementation of the path
     (rank 0 only), on the same scene, metric and unit."""
@@ -322,6 +371,7 @@ def main():
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA traversal")
     ap.add_argument("--no-render", action="store_true", help="skip the full-frame render leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the multi-scene serving leg")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays (and shadow queries) per step per GPU")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -399,6 +449,9 @@ def main():
     batch = None
     if rank == 0 and not args.no_batch:
         batch = batch_leg(ctx, stream)
+    serve = None
+    if rank == 0 and not args.no_serve:
+        serve = serve_leg(ctx)
 
     # e2e through the host-buffer API: pinned host inputs, results back.
     pin_r = torch.from_numpy(rays_np).pin_memory()
@@ -469,6 +522,7 @@ def main():
             "reference_cuda": ref_cuda,
             "render": render,
             "batch": batch,
+            "serve": serve,
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
         }

@@ -104,6 +104,81 @@ class DenoiseParams(C.Structure):
     ]
 
 
+class MaterialDesc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("basecolor", C.c_float * 3),
+        ("emission", C.c_float * 3),
+        ("roughness", C.c_float),
+        ("metallic", C.c_float),
+        ("transmission", C.c_float),
+        ("scatter_distance", C.c_float * 3),
+        ("ior", C.c_float),
+    ]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("material", C.c_int32), ("first", C.c_int32), ("count", C.c_int32)]
+
+
+class LightDesc(C.Structure):
+    _fields_ = [("type", C.c_int32), ("mesh", C.c_int32), ("emission", C.c_float * 3)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("n_tris", C.c_int64),
+        ("verts", C.c_void_p),
+        ("normals", C.c_void_p),
+        ("uvs", C.c_void_p),
+        ("n_meshes", C.c_int32),
+        ("n_materials", C.c_int32),
+        ("n_lights", C.c_int32),
+        ("meshes", C.c_void_p),
+        ("materials", C.c_void_p),
+        ("lights", C.c_void_p),
+        ("env_width", C.c_int32),
+        ("env_height", C.c_int32),
+        ("env_rgba", C.c_void_p),
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("spp", C.c_int32),
+        ("max_bounces", C.c_int32),
+        ("rr", C.c_float),
+        ("fovy", C.c_float),
+        ("direction", C.c_float * 3),
+    ]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [
+        ("hbm_budget_bytes", C.c_int64),
+        ("paths_per_pass", C.c_int32),
+        ("max_requests", C.c_int32),
+        ("passes_in_flight", C.c_int32),
+    ]
+
+
+class Request(C.Structure):
+    _fields_ = [
+        ("scene", C.c_int32),
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("spp", C.c_int32),
+        ("max_bounces", C.c_int32),
+        ("rr", C.c_float),
+        ("rr_start_bounce", C.c_int32),
+        ("seed", C.c_uint64),
+        ("camera", Camera),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("queued", "running", "done", "passes", "paths", "bytes_budget",
+                                         "bytes_scenes", "bytes_wavefront", "bytes_requests", "bytes_pool")] + [
+        ("num_scenes", C.c_int32), ("passes_in_flight", C.c_int32)]
+
+
 def build(force: bool = False) -> None:
     """Compiles libcrt.so in-tree with nvcc for sm_100a (make in csrc/)."""
     csrc = os.path.join(_HERE, "csrc")
@@ -128,6 +203,7 @@ _SIGS = {
     "crt_scene_free": (None, [_VP]),
     "crt_scene_info": (C.c_int, [_VP, C.POINTER(SceneInfo)]),
     "crt_scene_load_json": (C.c_int, [_VP, C.c_char_p, C.POINTER(_VP)]),
+    "crt_scene_from_arrays": (C.c_int, [_VP, C.POINTER(SceneDesc), C.POINTER(_VP)]),
     "crt_scene_export_geometry": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "crt_scene_export_tables": (C.c_int, [_VP, _VP, _VP, _VP]),
     "crt_get_render_params": (C.c_int, [_VP, C.POINTER(RenderParams)]),
@@ -138,6 +214,16 @@ _SIGS = {
     "crt_render_device": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
     "crt_render_device_noalloc": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
     "crt_render_views": (C.c_int, [_VP, C.c_int32, _VP, C.c_int32, C.c_int32, _VP, _VP, _VP, C.c_int32, _VP]),
+    "crt_server_create": (C.c_int, [_VP, C.POINTER(ServerConfig), C.POINTER(_VP)]),
+    "crt_server_free": (None, [_VP]),
+    "crt_server_add_scene": (C.c_int, [_VP, _VP, C.POINTER(C.c_int32)]),
+    "crt_server_submit": (C.c_int, [_VP, C.POINTER(Request), C.POINTER(C.c_int64)]),
+    "crt_server_step": (C.c_int, [_VP, C.c_int32, C.POINTER(C.c_int32)]),
+    "crt_server_poll": (C.c_int, [_VP, C.c_int64, C.POINTER(C.c_int32)]),
+    "crt_server_result": (C.c_int, [_VP, C.c_int64, _VP, _VP]),
+    "crt_server_result_device": (C.c_int, [_VP, C.c_int64, C.POINTER(_VP), C.POINTER(_VP)]),
+    "crt_server_release": (C.c_int, [_VP, C.c_int64]),
+    "crt_server_get_stats": (C.c_int, [_VP, C.POINTER(ServerStats)]),
     "crt_denoise_params_default": (C.c_int, [C.POINTER(DenoiseParams)]),
     "crt_gbuffer_from_primary": (C.c_int, [_VP, C.POINTER(Camera), C.POINTER(GBuffer), _VP]),
     "crt_svgf_create": (C.c_int, [_VP, C.c_int32, C.c_int32, C.POINTER(_VP)]),

@@ -208,6 +208,134 @@ crt_status crt_trace_shadow(crt_scene *scene, const crt_shadow_query *q, int64_t
 
 extern "C" {
 
+namespace {
+
+// Host scene -> device: BVH build over the vertices, render data upload,
+// render parameters and the orbit camera from the camera block
+// (Scene::Scene, Src/Core/scene.cpp:50-57 with BuildBVH :115 and
+// InitCameraParam :646).
+void finish_scene(crt_scene *s) {
+    HostScene &h = s->host;
+    size_t n = h.prim_mesh.size();
+    CRT_CHECK(n < (size_t)(1 << 27) - 1, CRT_ERR_CAPACITY, "too many triangles");
+    CRT_CUDA(cudaMalloc(&s->d_verts, h.verts.size() * sizeof(float)));
+    CRT_CUDA(cudaMemcpy(s->d_verts, h.verts.data(), h.verts.size() * sizeof(float), cudaMemcpyHostToDevice));
+    build_bvh(s->d_verts, (int)n, s->ctx->stream, s->bvh);
+    upload_render_data(h, s->rd);
+    s->rp.width = h.width;
+    s->rp.height = h.height;
+    s->rp.spp = h.spp;
+    s->rp.max_bounces = h.max_bounces;
+    s->rp.rr = h.rr;
+    init_camera(s->cam, s->bvh.bounds_min, s->bvh.bounds_max, h.direction, h.fovy, h.width, h.height);
+    s->renderable = true;
+}
+
+void host_scene_from_desc(const crt_scene_desc &d, HostScene &h) {
+    CRT_CHECK(d.n_tris > 0 && d.verts, CRT_ERR_INVALID, "crt_scene_from_arrays: no triangles");
+    CRT_CHECK(d.n_tris < (1 << 27) - 1, CRT_ERR_CAPACITY, "crt_scene_from_arrays: too many triangles");
+    CRT_CHECK(d.n_meshes > 0 && d.meshes && d.n_materials > 0 && d.materials, CRT_ERR_INVALID,
+              "crt_scene_from_arrays: meshes and materials required");
+    CRT_CHECK(d.n_lights >= 0 && (d.n_lights == 0 || d.lights), CRT_ERR_INVALID, "crt_scene_from_arrays: lights");
+    CRT_CHECK(d.width > 0 && d.height > 0 && d.spp >= 0 && d.max_bounces >= 0, CRT_ERR_INVALID,
+              "crt_scene_from_arrays: bad camera block");
+    const size_t n = (size_t)d.n_tris;
+    h.width = d.width;
+    h.height = d.height;
+    h.spp = d.spp;
+    h.max_bounces = d.max_bounces;
+    h.rr = d.rr;
+    h.fovy = d.fovy;
+    for (int k = 0; k < 3; ++k) h.direction[k] = d.direction[k];
+    h.materials.resize(d.n_materials);
+    h.material_names.resize(d.n_materials);
+    for (int i = 0; i < d.n_materials; ++i) {
+        const crt_material_desc &md = d.materials[i];
+        CRT_CHECK(md.type >= MAT_LIGHT && md.type <= MAT_SUBSURFACE, CRT_ERR_INVALID,
+                  "crt_scene_from_arrays: bad material type");
+        DMaterial m = default_material_record();
+        m.type = md.type;
+        for (int k = 0; k < 3; ++k) {
+            m.base[k] = md.basecolor[k];
+            m.ke[k] = md.emission[k];
+            m.scatter[k] = md.scatter_distance[k];
+        }
+        m.roughness = md.roughness;
+        m.metallic = md.metallic;
+        m.transmission = md.transmission;
+        m.ior = md.ior;
+        h.materials[i] = m;
+        h.material_names[i] = "material" + std::to_string(i);
+    }
+    h.verts.assign(d.verts, d.verts + 9 * n);
+    if (d.normals) {
+        h.normals.assign(d.normals, d.normals + 9 * n);
+    } else {
+        h.normals.resize(9 * n);
+        for (size_t t = 0; t < n; ++t) {
+            float fn[3];
+            face_normal(&h.verts[9 * t], fn);
+            for (int c = 0; c < 3; ++c)
+                for (int k = 0; k < 3; ++k) h.normals[9 * t + 3 * c + k] = fn[k];
+        }
+    }
+    if (d.uvs)
+        h.uvs.assign(d.uvs, d.uvs + 6 * n);
+    else
+        h.uvs.assign(6 * n, 0.f);
+    h.prim_mesh.resize(n);
+    int64_t next = 0;
+    for (int i = 0; i < d.n_meshes; ++i) {
+        const crt_mesh_desc &md = d.meshes[i];
+        CRT_CHECK(md.first == next && md.count > 0 && md.first + (int64_t)md.count <= d.n_tris, CRT_ERR_INVALID,
+                  "crt_scene_from_arrays: meshes must tile the triangles in order");
+        CRT_CHECK(md.material >= 0 && md.material < d.n_materials, CRT_ERR_INVALID,
+                  "crt_scene_from_arrays: bad mesh material");
+        DMesh dm;
+        std::memset(&dm, 0, sizeof(dm));
+        dm.material = md.material;
+        dm.light = -1;
+        dm.start = md.first;
+        dm.count = md.count;
+        float area = 0.f;
+        for (int t = 0; t < md.count; ++t) {
+            area += triangle_area(&h.verts[9 * (size_t)(md.first + t)]);
+            h.prim_mesh[md.first + t] = i;
+        }
+        dm.area = area;
+        h.meshes.push_back(dm);
+        h.mesh_names.push_back("mesh" + std::to_string(i));
+        next += md.count;
+    }
+    CRT_CHECK(next == d.n_tris, CRT_ERR_INVALID, "crt_scene_from_arrays: meshes must cover every triangle");
+    for (int i = 0; i < d.n_lights; ++i) {
+        const crt_light_desc &ld = d.lights[i];
+        DLight dl;
+        std::memset(&dl, 0, sizeof(dl));
+        dl.mesh = -1;
+        if (ld.type == LIGHT_AREA) {
+            CRT_CHECK(ld.mesh >= 0 && ld.mesh < d.n_meshes, CRT_ERR_INVALID, "crt_scene_from_arrays: bad light mesh");
+            dl.type = LIGHT_AREA;
+            dl.mesh = ld.mesh;
+            for (int k = 0; k < 3; ++k) dl.emission[k] = ld.emission[k];
+            h.meshes[ld.mesh].light = (int)h.lights.size();
+        } else if (ld.type == LIGHT_ENV) {
+            CRT_CHECK(d.env_rgba && d.env_width > 0 && d.env_height > 0, CRT_ERR_INVALID,
+                      "crt_scene_from_arrays: environment light without an image");
+            dl.type = LIGHT_ENV;
+            h.env_w = d.env_width;
+            h.env_h = d.env_height;
+            h.env.assign(d.env_rgba, d.env_rgba + (size_t)4 * d.env_width * d.env_height);
+            h.env_light = (int)h.lights.size();
+        } else {
+            throw Error(CRT_ERR_INVALID, "crt_scene_from_arrays: unsupported light type");
+        }
+        h.lights.push_back(dl);
+    }
+}
+
+}  // namespace
+
 crt_status crt_scene_load_json(crt_ctx *ctx, const char *path, crt_scene **out) {
     return guard([&] {
         CRT_CHECK(ctx && path && out, CRT_ERR_INVALID, "crt_scene_load_json: null argument");
@@ -216,20 +344,24 @@ crt_status crt_scene_load_json(crt_ctx *ctx, const char *path, crt_scene **out) 
         s->ctx = ctx;
         try {
             load_scene_json(path, s->host);
-            HostScene &h = s->host;
-            size_t n = h.prim_mesh.size();
-            CRT_CHECK(n < (size_t)(1 << 27) - 1, CRT_ERR_CAPACITY, "too many triangles");
-            CRT_CUDA(cudaMalloc(&s->d_verts, h.verts.size() * sizeof(float)));
-            CRT_CUDA(cudaMemcpy(s->d_verts, h.verts.data(), h.verts.size() * sizeof(float), cudaMemcpyHostToDevice));
-            build_bvh(s->d_verts, (int)n, ctx->stream, s->bvh);
-            upload_render_data(h, s->rd);
-            s->rp.width = h.width;
-            s->rp.height = h.height;
-            s->rp.spp = h.spp;
-            s->rp.max_bounces = h.max_bounces;
-            s->rp.rr = h.rr;
-            init_camera(s->cam, s->bvh.bounds_min, s->bvh.bounds_max, h.direction, h.fovy, h.width, h.height);
-            s->renderable = true;
+            finish_scene(s);
+        } catch (...) {
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+crt_status crt_scene_from_arrays(crt_ctx *ctx, const crt_scene_desc *desc, crt_scene **out) {
+    return guard([&] {
+        CRT_CHECK(ctx && desc && out, CRT_ERR_INVALID, "crt_scene_from_arrays: null argument");
+        CRT_CUDA(cudaSetDevice(ctx->device));
+        auto *s = new crt_scene();
+        s->ctx = ctx;
+        try {
+            host_scene_from_desc(*desc, s->host);
+            finish_scene(s);
         } catch (...) {
             delete s;
             throw;

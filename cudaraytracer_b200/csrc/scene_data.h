@@ -91,4 +91,12 @@ void load_scene_json(const std::string &path, HostScene &out);
 // (Src/Core/triangle.cu:3-10).
 float triangle_area(const float *v);
 
+// Unit face normal of a triangle (9 floats) as the OBJ import computes it
+// for faces without vertex normals (Src/Utils/objloader.cpp:192-198).
+void face_normal(const float *v, float *n);
+
+// Material record with the defaults of Src/Core/material.h before any
+// per-type field is parsed.
+DMaterial default_material_record();
+
 }  // namespace crt

@@ -794,6 +794,18 @@ float triangle_area(const float *v) {
     return 0.5f * std::sqrt(fdot(n, n));
 }
 
+void face_normal(const float *v, float *n) {
+    float e1[3], e2[3];
+    for (int k = 0; k < 3; ++k) {
+        e1[k] = v[3 + k] - v[k];
+        e2[k] = v[6 + k] - v[k];
+    }
+    fcross(e1, e2, n);
+    fnormalize(n);
+}
+
+DMaterial default_material_record() { return default_material(); }
+
 void load_scene_json(const std::string &path, HostScene &s) {
     std::string text = read_file(path);
     Json root = JsonParser(text).parse();

@@ -6,6 +6,7 @@
 * Scene.trace_closest  - BVH::IsIntersect (Src/Core/bvh.cu:253).
 * Scene.trace_shadow   - Light::Visible (Src/Core/light.cu:5).
 * Scene.load           - Scene::Scene(jsonPath) (Src/Core/scene.cpp:50).
+* Scene.from_spec      - the same scene built from generator arrays.
 * Scene.render         - the non-denoised progressive frame loop of
                          Renderer::RenderLoop (Src/Core/renderer.cuh:1144-1193)
                          returning the float accumulators.
@@ -80,6 +81,102 @@ class Scene:
         """Loads a scene JSON (reference schema) with its OBJ / HDR assets."""
         h = C.c_void_p()
         _lib.call("crt_scene_load_json", ctx.handle, str(path).encode(), C.byref(h))
+        return cls(ctx, h)
+
+    @classmethod
+    def from_spec(cls, ctx: Context, spec) -> "Scene":
+        """Builds a generated scene (cudaraytracer_b200.scenes.SceneSpec)
+        from memory through crt_scene_from_arrays: the scene that
+        Scene.load(spec.write(...)) builds, without writing OBJ/HDR files.
+        Material fields take the defaults of the JSON schema
+        (Src/Core/scene.cpp:283-378), an area light takes its emission from
+        its material's ke (or its own "ke"), and the environment image goes
+        through the Radiance RGBE quantisation its .hdr file would apply."""
+        from .scenes import decode_hdr_rgbe
+
+        cam = spec.camera
+        mats = _lib.MaterialDesc * len(spec.materials)
+        md = mats()
+        index = {}
+        for i, m in enumerate(spec.materials):
+            d = md[i]
+            t = {"light": 0, "diffuse": 1, "pbr": 2, "dielectric": 3, "glass": 3, "subsurface": 4}[m["type"]]
+            d.type = t
+            base = [0.0, 0.0, 0.0]
+            ke = [0.0, 0.0, 0.0]
+            scatter = [0.0, 0.0, 0.0]
+            rough, metal, trans, ior = 0.5, 0.0, 1.0, 1.0
+            if t in (1, 2, 4) and "basecolor" in m:
+                base = m["basecolor"]
+            if t == 0 and "emission" in m:
+                ke = m["emission"]
+            if t == 2:
+                metal = m.get("metallic", 0.0)
+                rough = m.get("roughness", 0.5)
+            if t == 4:
+                scatter = m.get("scatter_distance", [1.0, 1.0, 1.0])
+                ior = m.get("ior", ior)
+                rough = m.get("roughness", rough)
+                metal = 0.0
+            if t == 3:
+                base = m.get("basecolor", [1.0, 1.0, 1.0])
+                ior = m.get("ior", 1.5)
+                trans = m.get("transmission", 1.0)
+                rough = m.get("roughness", 0.0)
+                metal = 0.0
+            for k in range(3):
+                d.basecolor[k], d.emission[k], d.scatter_distance[k] = base[k], ke[k], scatter[k]
+            d.roughness, d.metallic, d.transmission, d.ior = rough, metal, trans, ior
+            index[m["name"]] = i
+        tris = [np.ascontiguousarray(m.tris, dtype=np.float32).reshape(-1, 9) for m in spec.meshes]
+        verts = np.ascontiguousarray(np.concatenate(tris))
+        meshes = (_lib.MeshDesc * len(tris))()
+        first = 0
+        mesh_index = {}
+        for i, (m, t) in enumerate(zip(spec.meshes, tris)):
+            meshes[i].material = index[m.material]
+            meshes[i].first = first
+            meshes[i].count = t.shape[0]
+            first += t.shape[0]
+            mesh_index[m.name] = i
+        lights = (_lib.LightDesc * max(1, len(spec.lights)))()
+        env = None
+        for i, l in enumerate(spec.lights):
+            if l["type"] == "area":
+                lights[i].type = 0
+                lights[i].mesh = mesh_index[l["lightMeshName"]]
+                ke = l.get("ke", [0.0, 0.0, 0.0])
+                if "material" in l:
+                    mm = md[index[l["material"]]]
+                    ke = [mm.emission[k] for k in range(3)]
+                for k in range(3):
+                    lights[i].emission[k] = ke[k]
+            elif l["type"] == "env":
+                lights[i].type = 2
+                rgb = decode_hdr_rgbe(spec.env)
+                env = np.ascontiguousarray(np.concatenate([rgb, np.ones(rgb.shape[:2] + (1,), np.float32)], 2))
+            else:
+                raise ValueError(f"unsupported light type {l['type']}")
+        d = _lib.SceneDesc()
+        d.n_tris = verts.shape[0]
+        d.verts = verts.ctypes.data
+        d.n_meshes, d.n_materials, d.n_lights = len(tris), len(spec.materials), len(spec.lights)
+        d.meshes = C.addressof(meshes)
+        d.materials = C.addressof(md)
+        d.lights = C.addressof(lights)
+        if env is not None:
+            d.env_height, d.env_width = env.shape[0], env.shape[1]
+            d.env_rgba = env.ctypes.data
+        d.width, d.height = int(cam["resolution"][0]), int(cam["resolution"][1])
+        d.spp = int(cam.get("spp", 16))
+        d.max_bounces = int(cam.get("max_bounces", 5))
+        d.rr = float(cam.get("rr", 0.8))
+        d.fovy = float(cam.get("fov", 40))
+        direction = cam.get("direction", [0.0, 0.0, -1.0])
+        for k in range(3):
+            d.direction[k] = direction[k]
+        h = C.c_void_p()
+        _lib.call("crt_scene_from_arrays", ctx.handle, C.byref(d), C.byref(h))
         return cls(ctx, h)
 
     @property

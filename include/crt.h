@@ -116,6 +116,48 @@ crt_status crt_scene_info(const crt_scene *scene, crt_scene_info_t *info);
  * with ParseSceneFile (:129), BuildBVH (:115), InitCameraParam (:646). */
 crt_status crt_scene_load_json(crt_ctx *ctx, const char *path, crt_scene **out);
 
+/* A renderable scene from in-memory arrays, for generators: the same scene
+ * crt_scene_load_json builds from the equivalent JSON/OBJ/HDR files, with
+ * the JSON references already resolved (material per mesh, light mesh and
+ * emission per light). Material types follow Src/Core/material.h:6-12. */
+typedef struct crt_material_desc {
+    int32_t type;                /* 0 light, 1 diffuse, 2 pbr, 3 dielectric, 4 subsurface */
+    float basecolor[3];
+    float emission[3];           /* ke (light materials) */
+    float roughness, metallic, transmission;
+    float scatter_distance[3];
+    float ior;
+} crt_material_desc;
+
+typedef struct crt_mesh_desc {
+    int32_t material;            /* index into materials */
+    int32_t first, count;        /* triangle range; meshes tile [0, n_tris) in order */
+} crt_mesh_desc;
+
+typedef struct crt_light_desc {
+    int32_t type;                /* 0 area (over `mesh`), 2 environment (env_rgba) */
+    int32_t mesh;
+    float emission[3];           /* area lights */
+} crt_light_desc;
+
+typedef struct crt_scene_desc {
+    int64_t n_tris;
+    const float *verts;          /* n_tris x 9 (v0, v1, v2) */
+    const float *normals;        /* n_tris x 9 per-vertex normals, or NULL for face normals */
+    const float *uvs;            /* n_tris x 6, or NULL for zeros */
+    int32_t n_meshes, n_materials, n_lights;
+    const crt_mesh_desc *meshes;
+    const crt_material_desc *materials;
+    const crt_light_desc *lights;
+    int32_t env_width, env_height;
+    const float *env_rgba;       /* env_width x env_height RGBA floats, top row first */
+    int32_t width, height, spp, max_bounces;  /* camera block (Src/Core/scene.cpp:187-252) */
+    float rr, fovy;
+    float direction[3];
+} crt_scene_desc;
+
+crt_status crt_scene_from_arrays(crt_ctx *ctx, const crt_scene_desc *desc, crt_scene **out);
+
 /* Loaded geometry in scene order (arrays sized by crt_scene_info):
  * verts n x 9, normals n x 9 (per vertex), uvs n x 6, prim_mesh n. Any
  * pointer may be NULL. Mirrors Scene's host triangle arrays
@@ -197,6 +239,74 @@ crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_sample, int
 crt_status crt_render_views(crt_scene *scene, int32_t n_views, const crt_camera *cams, int32_t first_sample,
                             int32_t spp, float *d_direct, float *d_indirect, float *d_sumsq, int32_t use_graph,
                             void *stream);
+
+/* ---- multi-scene render server ----------------------------------------- */
+
+/* Continuous batching of render requests over resident scenes (no reference
+ * counterpart: the reference renders one scene, one request at a time, behind
+ * the renderParam singleton, Src/Core/scene.h:20-46, and
+ * Renderer::RenderLoop, Src/Core/renderer.cuh:1106-1307). Scenes added to a
+ * server stay resident and owned by the caller, who keeps them alive until
+ * crt_server_free. Requests (scene, resolution, spp, camera, seed) queue and
+ * are admitted, oldest first, while a request slot is free and the HBM
+ * budget holds the scenes, the shared wavefront and every admitted request's
+ * accumulators. Each wavefront pass packs up to paths_per_pass paths of the
+ * admitted requests in admission order; up to passes_in_flight passes are
+ * queued on the GPU ahead of the host. A request's image equals that of
+ * crt_render_device with the same camera, render parameters and seed, up to
+ * the order of float additions into its pixels. */
+typedef struct crt_server crt_server;
+
+typedef struct crt_server_config {
+    int64_t hbm_budget_bytes; /* scenes + wavefront + request accumulators; 0 = 150 GiB */
+    int32_t paths_per_pass;   /* shared wavefront size; 0 = 8M paths */
+    int32_t max_requests;     /* admitted (unreleased) request slots; 0 = 4096; at most 2^20 */
+    int32_t passes_in_flight; /* passes queued on the GPU; 0 = 2; at most 64 */
+} crt_server_config;
+
+typedef struct crt_request {
+    int32_t scene;            /* id from crt_server_add_scene */
+    int32_t width, height;    /* resolution */
+    int32_t spp;              /* samples per pixel */
+    int32_t max_bounces;      /* extend/shade iterations */
+    float rr;                 /* Russian-roulette continuation probability */
+    int32_t rr_start_bounce;  /* first bounce that applies RR; 0 = reference */
+    uint64_t seed;            /* PCG32 seed of the request's path streams */
+    crt_camera camera;        /* orbit parameters (target, distance, theta, phi, fovy); derived fields ignored */
+} crt_request;
+
+typedef enum crt_request_state { CRT_REQ_QUEUED = 0, CRT_REQ_RUNNING = 1, CRT_REQ_DONE = 2 } crt_request_state;
+
+typedef struct crt_server_stats {
+    int64_t queued, running, done; /* requests by state (done = finished, not yet released) */
+    int64_t passes, paths;         /* wavefront passes and paths enqueued so far */
+    int64_t bytes_budget, bytes_scenes, bytes_wavefront, bytes_requests, bytes_pool;
+    int32_t num_scenes, passes_in_flight;
+} crt_server_stats;
+
+crt_status crt_server_create(crt_ctx *ctx, const crt_server_config *cfg, crt_server **out);
+void crt_server_free(crt_server *srv);
+/* Makes a loaded scene resident in the server; CRT_ERR_CAPACITY when its
+ * device bytes do not fit the budget. */
+crt_status crt_server_add_scene(crt_server *srv, crt_scene *scene, int32_t *scene_id);
+/* Queues a request; CRT_ERR_CAPACITY when it could never fit the budget. */
+crt_status crt_server_submit(crt_server *srv, const crt_request *req, int64_t *request_id);
+/* Retires finished passes, admits queued requests and enqueues passes up to
+ * passes_in_flight. Non-blocking unless `wait` != 0, which blocks until at
+ * least one request finishes when work is in flight. *n_done (may be NULL)
+ * = requests that finished during this call. */
+crt_status crt_server_step(crt_server *srv, int32_t wait, int32_t *n_done);
+/* *state = a crt_request_state. */
+crt_status crt_server_poll(crt_server *srv, int64_t request_id, int32_t *state);
+/* Copies a finished request's accumulators (width*height float4 each, sums
+ * over spp, rows bottom-up) to host memory. */
+crt_status crt_server_result(crt_server *srv, int64_t request_id, float *direct, float *indirect);
+/* Device pointers to a finished request's accumulators, valid until release. */
+crt_status crt_server_result_device(crt_server *srv, int64_t request_id, const float **d_direct,
+                                    const float **d_indirect);
+/* Frees a finished or still-queued request's slot and buffers. */
+crt_status crt_server_release(crt_server *srv, int64_t request_id);
+crt_status crt_server_get_stats(crt_server *srv, crt_server_stats *st);
 
 /* ---- SVGF denoising ---------------------------------------------------- */
 
