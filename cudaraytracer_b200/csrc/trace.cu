@@ -2,49 +2,92 @@
 // ray batches in HBM.
 //
 // Extend replaces IntersectionKernel's traversal (Src/Core/renderer.cuh:132
-// -> TraceRay :124 -> BVH::IsIntersect Src/Core/bvh.cu:253): one ray per
-// thread, 32 B in (two float4 loads), 16 B out (one float4 store), node
-// boxes and triangles through the read-only path.
+// -> TraceRay :124 -> BVH::IsIntersect Src/Core/bvh.cu:253): 32 B in per ray
+// (two float4 loads), 16 B out (one float4 store), node boxes and triangles
+// through the read-only path, persistent warps with lane refill.
 #include "trace.cuh"
+#include "traverse.cuh"
+#include "render_kernels.cuh"  // persistent_grid
 
 namespace crt {
 
 constexpr int kTraceBlock = 128;
 
-__global__ void __launch_bounds__(kTraceBlock) k_trace_closest(BvhView bvh, const float4 *__restrict__ rays,
-                                                               int64_t n, float4 *__restrict__ hits) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        float4 r0 = __ldg(rays + 2 * i), r1 = __ldg(rays + 2 * i + 1);
-        Hit h = closest_hit<false>(bvh, v3(r0.x, r0.y, r0.z), v3(r1.x, r1.y, r1.z), r0.w, r1.w);
-        int prim = h.slot >= 0 ? tri_prim(bvh, h.slot) : -1;
+namespace {
+
+struct ClosestJob {
+    BvhView bvh;
+    const float4 *rays;
+    float4 *hits;
+    __device__ void setup(int i, BvhView &b, V3 &o, V3 &d, float &tmin, float &tmax, float &t_exit) {
+        b = bvh;
+        float4 r0 = __ldg(rays + 2 * (size_t)i), r1 = __ldg(rays + 2 * (size_t)i + 1);
+        o = v3(r0.x, r0.y, r0.z);
+        d = v3(r1.x, r1.y, r1.z);
+        tmin = r0.w;
+        tmax = r1.w;
+        t_exit = 0.f;
+    }
+    __device__ void finish(int i, const BvhView &b, const Hit &h) {
+        int prim = h.slot >= 0 ? tri_prim(b, h.slot) : -1;
         hits[i] = make_float4(h.t, __int_as_float(prim), h.b1, h.b2);
     }
-}
+};
 
-__global__ void __launch_bounds__(kTraceBlock) k_trace_shadow(BvhView bvh, const float4 *__restrict__ q, int64_t n,
-                                                              uint8_t *__restrict__ occ) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        float4 a = __ldg(q + 3 * i), b = __ldg(q + 3 * i + 1), c = __ldg(q + 3 * i + 2);
-        bool vis = visible(bvh, v3(a.x, a.y, a.z), v3(a.w, b.x, b.y), v3(b.z, b.w, c.x), v3(c.y, c.z, c.w));
-        occ[i] = vis ? 0 : 1;
+struct ShadowJob {
+    BvhView bvh;
+    const float4 *q;
+    uint8_t *occ;
+    ShadowRay r;
+    __device__ void setup(int i, BvhView &b, V3 &o, V3 &d, float &tmin, float &tmax, float &t_exit) {
+        b = bvh;
+        float4 a = __ldg(q + 3 * (size_t)i), bb = __ldg(q + 3 * (size_t)i + 1), c = __ldg(q + 3 * (size_t)i + 2);
+        shadow_ray_init(r, v3(a.x, a.y, a.z), v3(a.w, bb.x, bb.y), v3(bb.z, bb.w, c.x), v3(c.y, c.z, c.w));
+        o = r.o;
+        d = r.dir;
+        tmin = 1e-6f;
+        tmax = 1e8f;
+        t_exit = r.t_exit;
     }
+    __device__ void finish(int i, const BvhView &b, const Hit &h) { occ[i] = shadow_ray_visible(r, b, h) ? 0 : 1; }
+};
+
+}  // namespace
+
+// Each warp traces its contiguous share of the batch, refilling lanes as
+// their rays finish (traverse.cuh).
+__global__ void __launch_bounds__(kTraceBlock) k_trace_closest(BvhView bvh, const float4 *__restrict__ rays, int n,
+                                                               float4 *__restrict__ hits) {
+    ClosestJob job{bvh, rays, hits};
+    trace_dynamic<true>(job, n);
 }
 
-static int trace_grid(int64_t n) {
-    int64_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
-    const int64_t cap = 148LL * 16 * 64;  // grid-stride beyond this
-    return (int)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
+__global__ void __launch_bounds__(kTraceBlock) k_trace_shadow(BvhView bvh, const float4 *__restrict__ q, int n,
+                                                              uint8_t *__restrict__ occ) {
+    ShadowJob job{bvh, q, occ, {}};
+    trace_dynamic<true>(job, n);
+}
+
+// Persistent grid (all SMs at full occupancy), fewer blocks for small
+// batches so every warp gets rays.
+static int trace_grid(const void *kernel, int64_t n) {
+    const int full = persistent_grid(kernel, kTraceBlock);
+    const int64_t want = (n + kTraceBlock - 1) / kTraceBlock;
+    return (int)(want < full ? (want > 0 ? want : 1) : full);
 }
 
 void launch_trace_closest(const BvhView &bvh, const float4 *d_rays, int64_t n, float4 *d_hits, cudaStream_t s) {
     if (n <= 0) return;
-    k_trace_closest<<<trace_grid(n), kTraceBlock, 0, s>>>(bvh, d_rays, n, d_hits);
+    CRT_CHECK(n < (int64_t)1 << 31, CRT_ERR_CAPACITY, "trace batch larger than 2^31 rays");
+    k_trace_closest<<<trace_grid((const void *)k_trace_closest, n), kTraceBlock, 0, s>>>(bvh, d_rays, (int)n, d_hits);
     CRT_CUDA(cudaGetLastError());
 }
 
 void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_t *d_occ, cudaStream_t s) {
     if (n <= 0) return;
-    k_trace_shadow<<<trace_grid(n), kTraceBlock, 0, s>>>(bvh, reinterpret_cast<const float4 *>(d_q), n, d_occ);
+    CRT_CHECK(n < (int64_t)1 << 31, CRT_ERR_CAPACITY, "trace batch larger than 2^31 queries");
+    k_trace_shadow<<<trace_grid((const void *)k_trace_shadow, n), kTraceBlock, 0, s>>>(
+        bvh, reinterpret_cast<const float4 *>(d_q), (int)n, d_occ);
     CRT_CUDA(cudaGetLastError());
 }
 

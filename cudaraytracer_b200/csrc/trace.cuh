@@ -28,21 +28,37 @@ __device__ __forceinline__ V3 hit_point(const BvhView &bvh, const Hit &h) {
 // Any accepted hit with t < t_exit already fixes the answer to "occluded"
 // (the closest hit is then at least as near, hence more than 0.1 short of the
 // shading point on both tests), so traversal stops there.
-__device__ __forceinline__ bool visible(const BvhView &bvh, V3 hp, V3 hn, V3 lp, V3 ln) {
-    V3 h = vadd(hp, vscale(hn, 1e-4f));
-    V3 l = vadd(lp, vscale(ln, 1e-4f));
-    V3 diff = vsub(h, l);
-    float sd = vnorm(diff);
-    V3 dir = vnormalized(diff);
-    V3 o = vadd(l, vscale(dir, 1e-2f));
-    float t_exit = sd * 0.9999f - 0.1101f;
-    Hit hit = closest_hit<true>(bvh, o, dir, 1e-6f, 1e8f, t_exit);
+struct ShadowRay {
+    V3 h, l, o, dir;
+    float sd, t_exit;
+};
+
+__device__ __forceinline__ void shadow_ray_init(ShadowRay &r, V3 hp, V3 hn, V3 lp, V3 ln) {
+    r.h = vadd(hp, vscale(hn, 1e-4f));
+    r.l = vadd(lp, vscale(ln, 1e-4f));
+    V3 diff = vsub(r.h, r.l);
+    r.sd = vnorm(diff);
+    r.dir = vnormalized(diff);
+    r.o = vadd(r.l, vscale(r.dir, 1e-2f));
+    r.t_exit = r.sd * 0.9999f - 0.1101f;
+}
+
+// The predicate from the closest hit of closest_hit<true>(bvh, r.o, r.dir,
+// 1e-6, 1e8, r.t_exit).
+__device__ __forceinline__ bool shadow_ray_visible(const ShadowRay &r, const BvhView &bvh, const Hit &hit) {
     if (hit.slot < 0) return true;
-    if (hit.t < t_exit) return false;
+    if (hit.t < r.t_exit) return false;
     V3 thp = hit_point(bvh, hit);
-    float td = vnorm(vsub(thp, l));
-    if (vnorm(vsub(h, thp)) >= 0.1f && fabsf(rsub(td, sd)) >= 0.1f) return false;
+    float td = vnorm(vsub(thp, r.l));
+    if (vnorm(vsub(r.h, thp)) >= 0.1f && fabsf(rsub(td, r.sd)) >= 0.1f) return false;
     return true;
+}
+
+__device__ __forceinline__ bool visible(const BvhView &bvh, V3 hp, V3 hn, V3 lp, V3 ln) {
+    ShadowRay r;
+    shadow_ray_init(r, hp, hn, lp, ln);
+    Hit hit = closest_hit<true>(bvh, r.o, r.dir, 1e-6f, 1e8f, r.t_exit);
+    return shadow_ray_visible(r, bvh, hit);
 }
 
 #endif

@@ -1,0 +1,129 @@
+// Persistent-warp BVH traversal with dynamic ray refill.
+//
+// Random rays in one warp need very different numbers of traversal steps, so
+// a warp that traces one ray per lane runs until its slowest ray finishes
+// with most lanes idle. Here each warp keeps up to 32 rays in flight: one
+// loop turn runs one while-while iteration per active lane (descend interior
+// nodes to a leaf, test the leaf's triangles), and lanes whose ray finished
+// take the next rays of the warp's contiguous share of [0, n) (no atomics:
+// with incoherent rays the shares even out). Per ray, the node visit order
+// and every
+// arithmetic step are those of closest_hit (bvh.cuh), so results are
+// bit-identical.
+//
+// Used by the standalone ray-batch kernels (trace.cu), whose rays are
+// incoherent. The wavefront stages keep one path per thread: their primary
+// rays are coherent within a warp, and refilling lanes would break that.
+//
+// A Job supplies, per ray index, the BVH and ray (setup) and consumes the
+// hit (finish):
+//   __device__ void setup(int i, BvhView &bvh, V3 &o, V3 &d, float &tmin,
+//                         float &tmax, float &t_exit);
+//   __device__ void finish(int i, const BvhView &bvh, const Hit &hit);
+// An accepted hit with t < t_exit ends the traversal (closest_hit<true>'s
+// early exit; t_exit = 0 never fires).
+#pragma once
+#include "bvh.cuh"
+
+namespace crt {
+
+#ifdef __CUDACC__
+
+template <bool kCull, class Job>
+__device__ __forceinline__ void trace_dynamic(Job &job, int n) {
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    // warp-uniform: the rays [cbase, cbase + cleft) of this warp not yet started
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int cbase = (int)(w * n / warps);
+    int cleft = (int)((w + 1) * n / warps) - cbase;
+    // per-lane ray state
+    int idx = -1;
+    BvhView bvh{nullptr, nullptr, 0};
+    V3 o{0.f, 0.f, 0.f}, d{0.f, 0.f, 0.f}, inv{0.f, 0.f, 0.f};
+    float tmin = 0.f, t_exit = 0.f;
+    Hit hit;
+    hit.t = 0.f;
+    hit.slot = -1;
+    hit.b1 = hit.b2 = 0.f;
+    int stack[kStackSize];
+    int sp = 0, link = kSentinel;
+
+    auto start = [&](int k) {
+        idx = k;
+        float tmax;
+        job.setup(k, bvh, o, d, tmin, tmax, t_exit);
+        inv = v3(rrcp(d.x), rrcp(d.y), rrcp(d.z));
+        hit.t = tmax;
+        hit.slot = -1;
+        hit.b1 = hit.b2 = 0.f;
+        sp = 0;
+        stack[sp++] = kSentinel;
+        link = 0;
+    };
+
+    while (true) {
+        const unsigned idle = __ballot_sync(0xffffffffu, idx < 0);
+        if (idle && cleft > 0) {
+            const int take = min(__popc(idle), cleft);
+            const int rank = __popc(idle & lt);
+            if (idx < 0 && rank < take) start(cbase + rank);
+            cbase += take;
+            cleft -= take;
+        }
+        if (__ballot_sync(0xffffffffu, idx >= 0) == 0) break;  // nothing in flight and nothing left
+        if (idx < 0) continue;
+        // one while-while iteration of closest_hit
+        while (link >= 0) {
+            const float4 *nd = bvh.nodes + 4 * (size_t)link;
+            float4 n0 = __ldg(nd + 0), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2);
+            int4 n3 = __ldg(reinterpret_cast<const int4 *>(nd + 3));
+            float t0, t1;
+            bool h0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, tmin, hit.t, t0);
+            bool h1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, tmin, hit.t, t1);
+            if (h0 && h1) {
+                int near = n3.x, far = n3.y;
+                if (t1 < t0) {
+                    near = n3.y;
+                    far = n3.x;
+                }
+                stack[sp++] = far;
+                link = near;
+            } else if (h0) {
+                link = n3.x;
+            } else if (h1) {
+                link = n3.y;
+            } else {
+                link = stack[--sp];
+            }
+        }
+        bool finished = link == kSentinel;
+        if (!finished) {
+            const int code = ~link;
+            const int first = code >> 4, count = code & 15;
+            for (int k = 0; k < count; ++k) {
+                const int slot = first + k;
+                const float4 *tp = bvh.tris + 3 * (size_t)slot;
+                float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                const bool acc = intersect_triangle<kCull>(o, d, a, b, c, slot, hit);
+                if (acc && hit.t < t_exit) {
+                    finished = true;
+                    break;
+                }
+            }
+            if (!finished) {
+                link = stack[--sp];
+                finished = link == kSentinel;
+            }
+        }
+        if (finished) {
+            job.finish(idx, bvh, hit);
+            idx = -1;
+        }
+    }
+}
+
+#endif  // __CUDACC__
+
+}  // namespace crt
