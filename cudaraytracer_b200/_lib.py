@@ -232,6 +232,13 @@ _SIGS = {
     "crt_svgf_frame": (C.c_int, [_VP, C.POINTER(DenoiseParams), C.POINTER(GBuffer), C.POINTER(GBuffer), _VP, _VP,
                                  _VP, _VP, _VP]),
     "crt_render_svgf_frame": (C.c_int, [_VP, _VP, C.POINTER(DenoiseParams), C.c_int32, _VP, _VP, _VP]),
+    "crt_conv3x3_forward": (C.c_int, [_VP, _VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _VP, _VP, C.c_int32,
+                                      C.c_int32, _VP, _VP, _VP]),
+    "crt_conv3x3_backward_data": (C.c_int, [_VP, _VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _VP, C.c_int32,
+                                            _VP, _VP, _VP]),
+    "crt_conv3x3_backward_weights": (C.c_int, [_VP, _VP, _VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                               C.c_int32, _VP, _VP]),
+    "crt_check_device_errors": (C.c_int, [_VP]),
     "crt_trace_closest": (C.c_int, [_VP, _VP, C.c_int64, _VP]),
     "crt_trace_closest_device": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
     "crt_trace_shadow": (C.c_int, [_VP, _VP, C.c_int64, _VP]),

@@ -78,6 +78,8 @@ crt_status crt_create(int device, crt_ctx **out) {
         c->device = device;
         for (int i = 0; i < 2; ++i) CRT_CUDA(cudaStreamCreateWithFlags(&c->streams[i], cudaStreamNonBlocking));
         c->stream = c->streams[0];
+        CRT_CUDA(cudaMalloc(&c->d_err, sizeof(int)));
+        CRT_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
         *out = c;
     });
 }
@@ -87,6 +89,7 @@ void crt_destroy(crt_ctx *ctx) {
     cudaSetDevice(ctx->device);
     for (int i = 0; i < 2; ++i)
         if (ctx->streams[i]) cudaStreamDestroy(ctx->streams[i]);
+    if (ctx->d_err) cudaFree(ctx->d_err);
     delete ctx;
 }
 

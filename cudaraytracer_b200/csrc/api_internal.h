@@ -1,6 +1,7 @@
 // Internal definitions behind the opaque handles of include/crt.h.
 #pragma once
 #include "common.cuh"
+#include <cuda_bf16.h>
 #include "bvh_build.h"
 #include "trace.cuh"
 #include "render.h"
@@ -49,7 +50,19 @@ struct crt_ctx {
     cudaStream_t streams[2] = {nullptr, nullptr};
     cudaStream_t stream = nullptr;
     crt::DeviceScratch stage[2];
+    // Device word set by tensor-core kernels whose bounded waits ran out
+    // (read and cleared by crt_check_device_errors).
+    int *d_err = nullptr;
 };
+
+namespace crt {
+// Tensor-core 3x3 convolutions (conv.cu).
+void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const float *bias, const __nv_bfloat16 *mask,
+                    __nv_bfloat16 *out, float *out_f32, int *err, int nimg, int h, int w, int C, int N, bool flip,
+                    bool relu, cudaStream_t s);
+void conv3x3_wgrad_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *g, float *dw, int *err, int nimg, int h, int w,
+                          int C, int N, cudaStream_t s);
+}  // namespace crt
 
 namespace crt {
 struct Scene {

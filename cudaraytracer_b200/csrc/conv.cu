@@ -1,0 +1,465 @@
+// 3x3 convolutions (stride 1, zero padding 1) on NHWC BF16 activations as
+// implicit GEMMs on the sm_100a tensor cores (tcgen05.mma kind::f16, BF16 x
+// BF16 -> FP32 in TMEM). These are the dense contractions of the learned
+// kernel-predicting denoiser (kpcn.cu); the reference has no learned part.
+//
+// Forward and data gradient share one kernel: output pixel tile (M = 128
+// pixels) x all output channels (N), K = 9 taps x C input channels.
+//   forward : out[p, n] = sum_{t, c} in[p + off(t), c] * w[t][n][c]
+//   data grad: out[p, n] = sum_{t, c} g[p - off(t), c] * wt[t][n][c]
+//             (wt = w transposed per tap, flip = 1)
+// The A tile is gathered per tap with 16 B cp.async copies (zero-filled
+// outside the image) into the K-major core-matrix layout of tc.cuh; B is the
+// tap's weight slice. A 4-stage pipeline overlaps the copies of later steps
+// with the MMAs of earlier ones: one thread issues the MMAs of a step and
+// commits them to the stage's mbarrier, which frees the stage for reuse.
+// The epilogue reads the FP32 accumulators from TMEM (one pixel per thread)
+// and applies bias + ReLU (forward) or the ReLU mask of the layer below
+// (data gradient), writing BF16 (or FP32) NHWC.
+//
+// The weight gradient is a second kernel: rows M = (tap, c) (9C rows in
+// 128-row tiles), columns N = output channels, K = pixels split across
+// CTAs; both operands MN-major, partial sums added to FP32 dW with atomics.
+#include "api_internal.h"
+#include "tc.cuh"
+#include <algorithm>
+
+namespace crt {
+namespace {
+
+constexpr int kBM = 128;      // pixels (or (tap, c) rows) per tile
+constexpr int kThreads = 128;
+constexpr int kStages = 4;
+constexpr int kWgradBK = 64;  // pixels per weight-gradient K step
+
+struct ConvArgs {
+    const __nv_bfloat16 *in;    // [P][C]
+    const __nv_bfloat16 *wgt;   // [9][N][C]
+    const float *bias;          // [N] or null
+    const __nv_bfloat16 *mask;  // [P][N] or null: out *= (mask > 0)
+    __nv_bfloat16 *out;         // [P][N] or null
+    float *out_f32;             // [P][N] or null
+    int *err;
+    int nimg, h, wd, C, N, KC;
+    int flip, relu;
+};
+
+__device__ __forceinline__ uint32_t tmem_cols(int n) {
+    uint32_t c = 32;
+    while ((int)c < n) c <<= 1;
+    return c;
+}
+
+__global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ uint64_t bars[kStages + 1];
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int C = a.C, N = a.N, KC = a.KC;
+    const int P = a.nimg * a.h * a.wd, HW = a.h * a.wd;
+    const int ntiles = (P + kBM - 1) / kBM;
+    const int chunks = C / KC, steps = 9 * chunks;
+    const uint32_t a_bytes = kBM * KC * 2, b_bytes = (uint32_t)N * KC * 2;
+    const uint32_t stage_bytes = a_bytes + b_bytes;
+    const uint32_t lbo_a = (kBM / 8) * 128, lbo_b = (uint32_t)(N / 8) * 128;
+    const uint32_t idesc = tc::idesc_bf16(kBM, N, false, false);
+    const uint32_t ncols = tmem_cols(N);
+
+    if (tid == 0) {
+        for (int s = 0; s <= kStages; ++s) tc::mbar_init(&bars[s], 1);
+        tc::fence_mbar_init();
+    }
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, ncols);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+
+    uint32_t g = 0;        // global K-step counter (stage = g % kStages)
+    uint32_t tiles_done = 0;
+    bool failed = false;
+    for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+        const int m0 = tile * kBM;
+        // this thread's A row: pixel m0 + tid
+        const int p = m0 + tid;
+        const bool pin = p < P;
+        int pb = 0, py = 0, px = 0;
+        if (pin) {
+            pb = p / HW;
+            const int r = p - pb * HW;
+            py = r / a.wd;
+            px = r - py * a.wd;
+        }
+        const uint32_t g0 = g;
+        for (int s = 0; s < steps + kStages - 1; ++s) {
+            bool ok = true;
+            if (s < steps) {
+                const uint32_t gs = g0 + s, st = gs % kStages;
+                if (gs >= kStages) ok = tc::mbar_wait(&bars[st], ((gs / kStages) - 1) & 1);
+                unsigned char *sa = smem_raw + st * stage_bytes, *sb = sa + a_bytes;
+                const int tap = s / chunks, c0 = (s - tap * chunks) * KC;
+                int dy = tap / 3 - 1, dx = tap % 3 - 1;
+                if (a.flip) {
+                    dy = -dy;
+                    dx = -dx;
+                }
+                const int sy = py + dy, sx = px + dx;
+                const bool valid = pin && sy >= 0 && sy < a.h && sx >= 0 && sx < a.wd;
+                const __nv_bfloat16 *src =
+                    valid ? a.in + ((size_t)(pb * HW + sy * a.wd + sx) * C + c0) : a.in;
+                for (int kg = 0; kg < KC / 8; ++kg)
+                    tc::cp_async16(sa + (tid & 7) * 16 + (tid >> 3) * 128 + kg * lbo_a, valid ? src + kg * 8 : src,
+                                   valid ? 16u : 0u);
+                const int vecs = N * (KC / 8);
+                for (int v = tid; v < vecs; v += kThreads) {
+                    const int r = v / (KC / 8), kg = v - r * (KC / 8);
+                    tc::cp_async16(sb + (r & 7) * 16 + (r >> 3) * 128 + kg * lbo_b,
+                                   a.wgt + ((size_t)tap * N + r) * C + c0 + kg * 8, 16u);
+                }
+            }
+            tc::cp_async_commit();
+            const int c = s - (kStages - 1);
+            if (c >= 0) {
+                tc::cp_async_wait<kStages - 1>();
+                tc::fence_proxy_async();
+                if (__syncthreads_or(!ok)) {
+                    failed = true;
+                    break;
+                }
+                if (tid == 0) {
+                    const uint32_t gc = g0 + c, st = gc % kStages;
+                    const uint32_t sa = tc::smem_addr(smem_raw + st * stage_bytes), sb = sa + a_bytes;
+                    tc::fence_after_sync();
+                    for (int j = 0; j < KC / 16; ++j)
+                        tc::mma_bf16(tmem, tc::smem_desc(sa + 2 * j * lbo_a, lbo_a, 128),
+                                     tc::smem_desc(sb + 2 * j * lbo_b, lbo_b, 128), idesc, c > 0 || j > 0);
+                    tc::mma_commit(tc::smem_addr(&bars[st]));
+                }
+            } else if (__syncthreads_or(!ok)) {
+                failed = true;
+                break;
+            }
+        }
+        if (failed) break;
+        g = g0 + steps;
+        // all MMAs of the tile done -> accumulators readable
+        if (tid == 0) tc::mma_commit(tc::smem_addr(&bars[kStages]));
+        const bool ok = tc::mbar_wait(&bars[kStages], tiles_done & 1);
+        ++tiles_done;
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        tc::fence_after_sync();
+        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int n0 = 0; n0 < N; n0 += 16) {
+            float v[16];
+            tc::tmem_ld16(lane_base + n0, v);
+            if (!pin) continue;
+            if (a.bias)
+                for (int i = 0; i < 16; ++i) v[i] += a.bias[n0 + i];
+            if (a.relu)
+                for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
+            if (a.mask) {
+                const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + (size_t)p * N + n0);
+                uint4 mv[2] = {mp[0], mp[1]};
+                const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(mv);
+                for (int i = 0; i < 16; ++i)
+                    if (!(__bfloat162float(mb[i]) > 0.f)) v[i] = 0.f;
+            }
+            if (a.out) {
+                uint4 ov[2];
+                __nv_bfloat16 *ob = reinterpret_cast<__nv_bfloat16 *>(ov);
+                for (int i = 0; i < 16; ++i) ob[i] = __float2bfloat16_rn(v[i]);
+                uint4 *op = reinterpret_cast<uint4 *>(a.out + (size_t)p * N + n0);
+                op[0] = ov[0];
+                op[1] = ov[1];
+            }
+            if (a.out_f32) {
+                float4 *op = reinterpret_cast<float4 *>(a.out_f32 + (size_t)p * N + n0);
+                for (int i = 0; i < 4; ++i) op[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            }
+        }
+        tc::fence_before_sync();
+        __syncthreads();  // TMEM reads done before the next tile's MMAs
+    }
+    if (failed && tid == 0) atomicExch(a.err, 1);
+    tc::cp_async_wait_all();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+}
+
+struct WgradArgs {
+    const __nv_bfloat16 *in;   // [P][C] layer input
+    const __nv_bfloat16 *g;    // [P][N] gradient of the layer's pre-activation output
+    float *dw;                 // [9][N][C], accumulated
+    int *err;
+    int nimg, h, wd, C, N;
+    int pix_per_cta;           // multiple of kWgradBK
+};
+
+// dW[t][n][c] += sum_p in[p + off(t), c] * g[p, n] over this CTA's pixels.
+// Tile rows m = t * C + c (blockIdx.y selects 128 of them), columns n.
+__global__ void __launch_bounds__(kThreads) k_conv3x3_wgrad(WgradArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ uint64_t bars[kStages + 1];
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int C = a.C, N = a.N;
+    const int P = a.nimg * a.h * a.wd, HW = a.h * a.wd;
+    const int rows = 9 * C, m0 = blockIdx.y * kBM;
+    const int k0 = blockIdx.x * a.pix_per_cta, k1 = min(P, k0 + a.pix_per_cta);
+    const int steps = (k1 - k0 + kWgradBK - 1) / kWgradBK;
+    const uint32_t a_bytes = kBM * kWgradBK * 2, b_bytes = (uint32_t)N * kWgradBK * 2;
+    const uint32_t stage_bytes = a_bytes + b_bytes;
+    const uint32_t sbo = 128, lbo_a = (kBM / 8) * 128, lbo_b = (uint32_t)(N / 8) * 128;
+    const uint32_t idesc = tc::idesc_bf16(kBM, N, true, true);
+    const uint32_t ncols = tmem_cols(N);
+    if (steps <= 0) return;
+
+    if (tid == 0) {
+        for (int s = 0; s <= kStages; ++s) tc::mbar_init(&bars[s], 1);
+        tc::fence_mbar_init();
+    }
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, ncols);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+    bool failed = false;
+
+    for (int s = 0; s < steps + kStages - 1; ++s) {
+        bool ok = true;
+        if (s < steps) {
+            const uint32_t st = s % kStages;
+            if (s >= kStages) ok = tc::mbar_wait(&bars[st], ((s / kStages) - 1) & 1);
+            unsigned char *sa = smem_raw + st * stage_bytes, *sb = sa + a_bytes;
+            const int kb = k0 + s * kWgradBK;
+            // A: 16 row groups x 64 pixels, one 16 B vector (8 channels of one tap) each
+            for (int v = tid; v < (kBM / 8) * kWgradBK; v += kThreads) {
+                const int k = v % kWgradBK, mg = v / kWgradBK;
+                const int m = m0 + mg * 8, p = kb + k;
+                bool valid = m < rows && p < k1;
+                const __nv_bfloat16 *src = a.in;
+                if (valid) {
+                    const int tap = m / C, c0 = m - tap * C;
+                    const int b = p / HW, r = p - b * HW, y = r / a.wd, x = r - y * a.wd;
+                    const int sy = y + tap / 3 - 1, sx = x + tap % 3 - 1;
+                    valid = sy >= 0 && sy < a.h && sx >= 0 && sx < a.wd;
+                    if (valid) src = a.in + (size_t)(b * HW + sy * a.wd + sx) * C + c0;
+                }
+                tc::cp_async16(sa + mg * sbo + (k >> 3) * lbo_a + (k & 7) * 16, src, valid ? 16u : 0u);
+            }
+            // B: N/8 column groups x 64 pixels
+            for (int v = tid; v < (N / 8) * kWgradBK; v += kThreads) {
+                const int k = v % kWgradBK, ng = v / kWgradBK;
+                const int p = kb + k;
+                const bool valid = p < k1;
+                const __nv_bfloat16 *src = valid ? a.g + (size_t)p * N + ng * 8 : a.g;
+                tc::cp_async16(sb + ng * sbo + (k >> 3) * lbo_b + (k & 7) * 16, src, valid ? 16u : 0u);
+            }
+        }
+        tc::cp_async_commit();
+        const int c = s - (kStages - 1);
+        if (c >= 0) {
+            tc::cp_async_wait<kStages - 1>();
+            tc::fence_proxy_async();
+            if (__syncthreads_or(!ok)) {
+                failed = true;
+                break;
+            }
+            if (tid == 0) {
+                const uint32_t st = c % kStages;
+                const uint32_t sa = tc::smem_addr(smem_raw + st * stage_bytes), sb = sa + a_bytes;
+                tc::fence_after_sync();
+                for (int j = 0; j < kWgradBK / 16; ++j)
+                    tc::mma_bf16(tmem, tc::smem_desc(sa + 2 * j * lbo_a, lbo_a, sbo),
+                                 tc::smem_desc(sb + 2 * j * lbo_b, lbo_b, sbo), idesc, c > 0 || j > 0);
+                tc::mma_commit(tc::smem_addr(&bars[st]));
+            }
+        } else if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+    }
+    if (!failed) {
+        if (tid == 0) tc::mma_commit(tc::smem_addr(&bars[kStages]));
+        const bool ok = tc::mbar_wait(&bars[kStages], 0);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+        } else {
+            tc::fence_after_sync();
+            const int m = m0 + tid;
+            const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+            for (int n0 = 0; n0 < N; n0 += 16) {
+                float v[16];
+                tc::tmem_ld16(lane_base + n0, v);
+                if (m < rows) {
+                    const int tap = m / C, c = m - tap * C;
+                    float *dst = a.dw + ((size_t)tap * N + n0) * C + c;
+                    for (int i = 0; i < 16; ++i) atomicAdd(dst + (size_t)i * C, v[i]);
+                }
+            }
+        }
+    }
+    if (failed && tid == 0) atomicExch(a.err, 1);
+    tc::cp_async_wait_all();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+}
+
+int g_sms = 0;
+
+int sm_count() {
+    if (!g_sms) {
+        int dev;
+        CRT_CUDA(cudaGetDevice(&dev));
+        CRT_CUDA(cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return g_sms;
+}
+
+int host_tmem_cols(int n) {
+    int c = 32;
+    while (c < n) c <<= 1;
+    return c;
+}
+
+}  // namespace
+
+void conv3x3_check(int C, int N) {
+    CRT_CHECK(C > 0 && C % 16 == 0 && C <= 512, CRT_ERR_INVALID, "conv3x3: input channels must be a multiple of 16");
+    CRT_CHECK(N >= 16 && N % 16 == 0 && N <= 256, CRT_ERR_INVALID,
+              "conv3x3: output channels must be a multiple of 16 in [16, 256]");
+}
+
+// out = conv3x3(in) (+ bias, ReLU) or the data gradient (flip = 1, weights
+// transposed per tap, optional ReLU mask of the layer below).
+void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const float *bias, const __nv_bfloat16 *mask,
+                    __nv_bfloat16 *out, float *out_f32, int *err, int nimg, int h, int w, int C, int N, bool flip,
+                    bool relu, cudaStream_t s) {
+    conv3x3_check(C, N);
+    const int64_t P = (int64_t)nimg * h * w;
+    CRT_CHECK(P > 0 && P < (1LL << 31) - kBM, CRT_ERR_INVALID, "conv3x3: bad image size");
+    ConvArgs a;
+    a.in = in;
+    a.wgt = wgt;
+    a.bias = bias;
+    a.mask = mask;
+    a.out = out;
+    a.out_f32 = out_f32;
+    a.err = err;
+    a.nimg = nimg;
+    a.h = h;
+    a.wd = w;
+    a.C = C;
+    a.N = N;
+    a.KC = C % 64 == 0 ? 64 : (C % 32 == 0 ? 32 : 16);
+    a.flip = flip ? 1 : 0;
+    a.relu = relu ? 1 : 0;
+    const size_t smem = (size_t)kStages * (kBM * a.KC * 2 + (size_t)N * a.KC * 2);
+    CRT_CHECK(smem <= 200 * 1024, CRT_ERR_INVALID, "conv3x3: tile does not fit shared memory");
+    CRT_CUDA(cudaFuncSetAttribute(k_conv3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3x3, kThreads, smem));
+    per_sm = std::max(1, std::min(per_sm, 512 / host_tmem_cols(N)));
+    const int64_t tiles = (P + kBM - 1) / kBM;
+    const int grid = (int)std::min<int64_t>(tiles, (int64_t)sm_count() * per_sm);
+    k_conv3x3<<<grid, kThreads, smem, s>>>(a);
+    CRT_CUDA(cudaGetLastError());
+}
+
+// dw[9][N][C] += weight gradient of a 3x3 conv with input `in` [P][C] and
+// pre-activation output gradient `g` [P][N].
+void conv3x3_wgrad_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *g, float *dw, int *err, int nimg, int h, int w,
+                          int C, int N, cudaStream_t s) {
+    conv3x3_check(C, N);
+    const int64_t P = (int64_t)nimg * h * w;
+    CRT_CHECK(P > 0 && P < (1LL << 31) - kWgradBK, CRT_ERR_INVALID, "conv3x3_wgrad: bad image size");
+    WgradArgs a;
+    a.in = in;
+    a.g = g;
+    a.dw = dw;
+    a.err = err;
+    a.nimg = nimg;
+    a.h = h;
+    a.wd = w;
+    a.C = C;
+    a.N = N;
+    const int mtiles = (9 * C + kBM - 1) / kBM;
+    const size_t smem = (size_t)kStages * (kBM * kWgradBK * 2 + (size_t)N * kWgradBK * 2);
+    CRT_CHECK(smem <= 200 * 1024, CRT_ERR_INVALID, "conv3x3_wgrad: tile does not fit shared memory");
+    CRT_CUDA(cudaFuncSetAttribute(k_conv3x3_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3x3_wgrad, kThreads, smem));
+    per_sm = std::max(1, std::min(per_sm, 512 / host_tmem_cols(N)));
+    // enough pixel splits for about two waves, at least 8 K steps per CTA
+    const int64_t want = std::max<int64_t>(1, 2LL * sm_count() * per_sm / mtiles);
+    int64_t ppc = (P + want - 1) / want;
+    ppc = std::max<int64_t>(ppc, 8 * kWgradBK);
+    ppc = (ppc + kWgradBK - 1) / kWgradBK * kWgradBK;
+    a.pix_per_cta = (int)ppc;
+    dim3 grid((unsigned)((P + ppc - 1) / ppc), (unsigned)mtiles);
+    k_conv3x3_wgrad<<<grid, kThreads, smem, s>>>(a);
+    CRT_CUDA(cudaGetLastError());
+}
+
+}  // namespace crt
+
+using namespace crt;
+
+extern "C" crt_status crt_check_device_errors(crt_ctx *ctx) {
+    return guard([&] {
+        CRT_CHECK(ctx, CRT_ERR_INVALID, "crt_check_device_errors: null context");
+        CRT_CUDA(cudaSetDevice(ctx->device));
+        int e = 0;
+        CRT_CUDA(cudaDeviceSynchronize());
+        CRT_CUDA(cudaMemcpy(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) {
+            CRT_CUDA(cudaMemset(ctx->d_err, 0, sizeof(int)));
+            throw Error(CRT_ERR_TIMEOUT, "a tensor-core kernel gave up waiting on an mbarrier");
+        }
+    });
+}
+
+extern "C" crt_status crt_conv3x3_forward(crt_ctx *ctx, const void *d_in, int32_t n, int32_t h, int32_t w,
+                                          int32_t cin, const void *d_weights, const float *d_bias, int32_t cout,
+                                          int32_t relu, void *d_out_bf16, float *d_out_f32, void *stream) {
+    return guard([&] {
+        CRT_CHECK(ctx && d_in && d_weights && (d_out_bf16 || d_out_f32), CRT_ERR_INVALID,
+                  "crt_conv3x3_forward: null argument");
+        CRT_CUDA(cudaSetDevice(ctx->device));
+        cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+        conv3x3_launch((const __nv_bfloat16 *)d_in, (const __nv_bfloat16 *)d_weights, d_bias, nullptr,
+                       (__nv_bfloat16 *)d_out_bf16, d_out_f32, ctx->d_err, n, h, w, cin, cout, false, relu != 0, s);
+    });
+}
+
+extern "C" crt_status crt_conv3x3_backward_data(crt_ctx *ctx, const void *d_grad_out, int32_t n, int32_t h, int32_t w,
+                                                int32_t cout, const void *d_weights_t, int32_t cin, const void *d_mask,
+                                                void *d_grad_in, void *stream) {
+    return guard([&] {
+        CRT_CHECK(ctx && d_grad_out && d_weights_t && d_grad_in, CRT_ERR_INVALID,
+                  "crt_conv3x3_backward_data: null argument");
+        CRT_CUDA(cudaSetDevice(ctx->device));
+        cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+        conv3x3_launch((const __nv_bfloat16 *)d_grad_out, (const __nv_bfloat16 *)d_weights_t, nullptr,
+                       (const __nv_bfloat16 *)d_mask, (__nv_bfloat16 *)d_grad_in, nullptr, ctx->d_err, n, h, w, cout,
+                       cin, true, false, s);
+    });
+}
+
+extern "C" crt_status crt_conv3x3_backward_weights(crt_ctx *ctx, const void *d_in, const void *d_grad_out, int32_t n,
+                                                   int32_t h, int32_t w, int32_t cin, int32_t cout, float *d_grad_w,
+                                                   void *stream) {
+    return guard([&] {
+        CRT_CHECK(ctx && d_in && d_grad_out && d_grad_w, CRT_ERR_INVALID,
+                  "crt_conv3x3_backward_weights: null argument");
+        CRT_CUDA(cudaSetDevice(ctx->device));
+        cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+        conv3x3_wgrad_launch((const __nv_bfloat16 *)d_in, (const __nv_bfloat16 *)d_grad_out, d_grad_w, ctx->d_err, n,
+                             h, w, cin, cout, s);
+    });
+}

@@ -386,6 +386,33 @@ crt_status crt_trace_shadow(crt_scene *scene, const crt_shadow_query *q,
 crt_status crt_trace_shadow_device(crt_scene *scene, const crt_shadow_query *d_q,
                                    int64_t n, uint8_t *d_occluded, void *stream);
 
+/* ---- tensor-core 3x3 convolutions (learned denoiser) ------------------- */
+
+/* No reference counterpart: the dense contractions of the kernel-predicting
+ * denoiser, as BF16 x BF16 -> FP32 implicit GEMMs on the sm_100a tensor cores
+ * (tcgen05). Activations are NHWC BF16 (bit patterns as uint16), n images of
+ * h x w pixels; channel counts are multiples of 16 (cout in [16, 256]);
+ * stride 1, zero padding 1; tap t = 3 * (dy + 1) + (dx + 1). All
+ * asynchronous on `stream` (NULL = the context stream). */
+/* out[p, o] = bias[o] + sum_{t, c} in[p + off(t), c] * w[t][o][c], ReLU if
+ * relu != 0; written as BF16 (d_out_bf16) and/or FP32 (d_out_f32). */
+crt_status crt_conv3x3_forward(crt_ctx *ctx, const void *d_in, int32_t n, int32_t h, int32_t w, int32_t cin,
+                               const void *d_weights, const float *d_bias, int32_t cout, int32_t relu,
+                               void *d_out_bf16, float *d_out_f32, void *stream);
+/* grad_in[p, c] = sum_{t, o} grad_out[p - off(t), o] * wt[t][c][o] with
+ * wt[t] = w[t] transposed; multiplied by (mask[p, c] > 0) when d_mask (the
+ * layer input, a ReLU output) is given. */
+crt_status crt_conv3x3_backward_data(crt_ctx *ctx, const void *d_grad_out, int32_t n, int32_t h, int32_t w,
+                                     int32_t cout, const void *d_weights_t, int32_t cin, const void *d_mask,
+                                     void *d_grad_in, void *stream);
+/* grad_w[t][o][c] += sum_p in[p + off(t), c] * grad_out[p, o] (FP32). */
+crt_status crt_conv3x3_backward_weights(crt_ctx *ctx, const void *d_in, const void *d_grad_out, int32_t n,
+                                        int32_t h, int32_t w, int32_t cin, int32_t cout, float *d_grad_w,
+                                        void *stream);
+/* Synchronises the device and returns CRT_ERR_TIMEOUT (clearing the flag)
+ * when a tensor-core kernel of this context gave up a bounded wait. */
+crt_status crt_check_device_errors(crt_ctx *ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,46 @@
+"""The CPU oracle of the denoiser's convolutions checks itself: its data and
+weight gradients are the derivatives of its forward pass (finite
+differences in float64), and BF16 rounding is round-to-nearest-even."""
+import numpy as np
+
+from oracle import kpcn_oracle as K
+
+
+def test_bf16_rounding_is_nearest_even():
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, -2.5, 0.0, 3.3e38, 1e-40], dtype=np.float32)
+    r = K.bf16_round(x)
+    assert r[0] == 1.0 and r[1] == 1.0  # tie rounds to even
+    assert r[2] == np.float32(1.0 + 4 * 2 ** -8)
+    assert r[3] == -2.5 and r[4] == 0.0
+    b = K.bf16_bits(np.float32(1.0))
+    assert int(b) == 0x3F80
+    np.testing.assert_array_equal(K.from_bf16_bits(K.bf16_bits(r)), r)
+
+
+def test_conv_gradients_match_finite_differences():
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=(2, 5, 4, 3))
+    w = rng.normal(size=(9, 2, 3))
+    g = rng.normal(size=(2, 5, 4, 2))
+    # loss = sum(conv(x, w) * g): d/dx = backward_data(g, w), d/dw = backward_weights(x, g)
+    gx = K.conv3x3_backward_data(g, w)
+    gw = K.conv3x3_backward_weights(x, g)
+    eps = 1e-6
+    for idx in [(0, 0, 0, 0), (1, 4, 3, 2), (0, 2, 1, 1), (1, 0, 3, 0)]:
+        d = np.zeros_like(x)
+        d[idx] = eps
+        num = ((K.conv3x3_forward(x + d, w) - K.conv3x3_forward(x - d, w)) * g).sum() / (2 * eps)
+        assert abs(num - gx[idx]) < 1e-6 * max(1.0, abs(num))
+    for idx in [(0, 0, 0), (4, 1, 2), (8, 0, 1), (3, 1, 0)]:
+        d = np.zeros_like(w)
+        d[idx] = eps
+        num = ((K.conv3x3_forward(x, w + d) - K.conv3x3_forward(x, w - d)) * g).sum() / (2 * eps)
+        assert abs(num - gw[idx]) < 1e-6 * max(1.0, abs(num))
+
+
+def test_backward_data_with_relu_mask():
+    rng = np.random.default_rng(1)
+    g = rng.normal(size=(1, 3, 3, 2))
+    w = rng.normal(size=(9, 2, 4))
+    m = rng.normal(size=(1, 3, 3, 4))
+    np.testing.assert_allclose(K.conv3x3_backward_data(g, w, m), K.conv3x3_backward_data(g, w) * (m > 0))
