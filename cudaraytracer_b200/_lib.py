@@ -239,6 +239,18 @@ _SIGS = {
     "crt_conv3x3_backward_weights": (C.c_int, [_VP, _VP, _VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                                C.c_int32, _VP, _VP]),
     "crt_check_device_errors": (C.c_int, [_VP]),
+    "crt_kpcn_create": (C.c_int, [_VP, C.c_uint64, C.POINTER(_VP)]),
+    "crt_kpcn_free": (None, [_VP]),
+    "crt_kpcn_num_params": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
+    "crt_kpcn_get_params": (C.c_int, [_VP, _VP]),
+    "crt_kpcn_set_params": (C.c_int, [_VP, _VP]),
+    "crt_kpcn_get_grads": (C.c_int, [_VP, _VP]),
+    "crt_kpcn_features": (C.c_int, [_VP, C.POINTER(GBuffer), _VP, _VP, C.c_int32, C.c_int64, C.c_float, _VP, _VP,
+                                    _VP]),
+    "crt_kpcn_forward": (C.c_int, [_VP, C.c_int32, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
+    "crt_kpcn_train_step": (C.c_int, [_VP, C.c_int32, C.c_int32, C.c_int32, _VP, _VP, _VP, C.c_float,
+                                      C.POINTER(C.c_float), _VP]),
+    "crt_kpcn_debug_tensor": (C.c_int, [_VP, C.c_int32, _VP, C.c_int64]),
     "crt_trace_closest": (C.c_int, [_VP, _VP, C.c_int64, _VP]),
     "crt_trace_closest_device": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
     "crt_trace_shadow": (C.c_int, [_VP, _VP, C.c_int64, _VP]),

@@ -74,3 +74,101 @@ def check_device_errors(ctx) -> None:
     """Raises CrtError (CRT_ERR_TIMEOUT) if a tensor-core kernel gave up a
     bounded wait since the last check."""
     _lib.call("crt_check_device_errors", ctx.handle)
+
+
+class Kpcn:
+    """The kernel-predicting denoiser (crt_kpcn_*): a 3-level U-Net on the
+    tensor-core convolutions predicting a 5x5 filter per pixel. Tensors are
+    CUDA torch tensors: features (n, h, w, 16) bfloat16, radiance (n, h, w, 4)
+    float32 (rgb, unused); h and w multiples of 4."""
+
+    LAYERS = ["e0a", "e0b", "e1a", "e1b", "e2a", "e2b", "d1a", "d1b", "d0a", "d0b", "out"]
+    SPEC = [(16, 32), (32, 32), (32, 64), (64, 64), (64, 96), (96, 96), (160, 64), (64, 64), (96, 32), (32, 32),
+            (32, 32)]
+
+    def __init__(self, ctx, seed: int = 0):
+        self.ctx = ctx
+        h = C.c_void_p()
+        _lib.call("crt_kpcn_create", ctx.handle, int(seed), C.byref(h))
+        self._h = h
+        n = C.c_int64()
+        _lib.call("crt_kpcn_num_params", self._h, C.byref(n))
+        self.num_params = n.value
+
+    def close(self):
+        if self._h:
+            _lib.lib().crt_kpcn_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self):
+        import numpy as np
+
+        p = np.empty(self.num_params, np.float32)
+        _lib.call("crt_kpcn_get_params", self._h, p.ctypes.data)
+        return p
+
+    def set_params(self, p):
+        import numpy as np
+
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.num_params:
+            raise ValueError(f"expected {self.num_params} parameters, got {p.size}")
+        _lib.call("crt_kpcn_set_params", self._h, p.ctypes.data)
+
+    def get_grads(self):
+        import numpy as np
+
+        g = np.empty(self.num_params, np.float32)
+        _lib.call("crt_kpcn_get_grads", self._h, g.ctypes.data)
+        return g
+
+    def forward(self, features, noisy, out=None, stream=None):
+        import torch
+
+        n, h, w, _ = features.shape
+        if out is None:
+            out = torch.empty((n, h, w, 4), dtype=torch.float32, device=features.device)
+        _lib.call("crt_kpcn_forward", self._h, n, h, w, _ptr(features), _ptr(noisy), _ptr(out),
+                  C.c_void_p(_torch_stream(features.device, stream)))
+        return out
+
+    def train_step(self, features, noisy, target, lr: float, stream=None) -> float:
+        """Forward, relMSE loss, backward and (lr > 0) an Adam step; returns
+        the batch loss (synchronises)."""
+        n, h, w, _ = features.shape
+        loss = C.c_float()
+        _lib.call("crt_kpcn_train_step", self._h, n, h, w, _ptr(features), _ptr(noisy), _ptr(target), float(lr),
+                  C.byref(loss), C.c_void_p(_torch_stream(features.device, stream)))
+        return loss.value
+
+    def debug_tensor(self, which: int, shape, dtype):
+        """Internal tensor of the last forward (0..9 layer outputs, 10 logits,
+        11 pool0, 12 pool1, 13 cat1, 14 cat0) as a numpy array."""
+        import numpy as np
+
+        a = np.empty(shape, dtype)
+        _lib.call("crt_kpcn_debug_tensor", self._h, int(which), a.ctypes.data, int(a.nbytes))
+        return a
+
+
+def make_features(scene, gbuffer: dict, direct, indirect, spp: int, depth_scale: float, stream=None):
+    """Network input of one rendered view: (features (h, w, 16) bfloat16,
+    noisy radiance (h, w, 4) float32 = (direct + indirect) / spp) from the
+    render accumulators and the view's G-buffer (Scene.gbuffer())."""
+    import torch
+
+    from .tracer import _gbuffer_struct
+
+    h, w = direct.shape[0], direct.shape[1]
+    feat = torch.empty((h, w, 16), dtype=torch.bfloat16, device=direct.device)
+    noisy = torch.empty((h, w, 4), dtype=torch.float32, device=direct.device)
+    gb = _gbuffer_struct(gbuffer)
+    _lib.call("crt_kpcn_features", scene.handle, C.byref(gb), _ptr(direct), _ptr(indirect), int(spp), h * w,
+              float(depth_scale), _ptr(feat), _ptr(noisy), C.c_void_p(_torch_stream(direct.device, stream)))
+    return feat, noisy

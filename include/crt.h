@@ -409,6 +409,42 @@ crt_status crt_conv3x3_backward_data(crt_ctx *ctx, const void *d_grad_out, int32
 crt_status crt_conv3x3_backward_weights(crt_ctx *ctx, const void *d_in, const void *d_grad_out, int32_t n,
                                         int32_t h, int32_t w, int32_t cin, int32_t cout, float *d_grad_w,
                                         void *stream);
+/* ---- learned kernel-predicting denoiser (KPCN) ------------------------ */
+
+/* A 3-level U-Net (32/64/96 channels) on the tensor-core convolutions above
+ * that predicts a 5x5 filter per pixel, applied to the noisy radiance; no
+ * reference counterpart (the reference filters with SVGF only). Images are
+ * n x h x w with h, w multiples of 4. Features: 16 BF16 channels per pixel
+ * (crt_kpcn_features); radiance: float4 per pixel (rgb, unused). */
+typedef struct crt_kpcn crt_kpcn;
+crt_status crt_kpcn_create(crt_ctx *ctx, uint64_t seed, crt_kpcn **out);
+void crt_kpcn_free(crt_kpcn *k);
+/* Parameters as one FP32 vector: per layer (e0a e0b e1a e1b e2a e2b d1a d1b
+ * d0a d0b out) the weights [9][cout][cin] then the bias [cout]. */
+crt_status crt_kpcn_num_params(const crt_kpcn *k, int64_t *n);
+crt_status crt_kpcn_get_params(crt_kpcn *k, float *host);
+crt_status crt_kpcn_set_params(crt_kpcn *k, const float *host);
+crt_status crt_kpcn_get_grads(crt_kpcn *k, float *host);
+/* Network input from a render: noisy = (direct + indirect) / spp per pixel
+ * (float4) and the 16 feature channels: log(1 + noisy rgb), albedo of the
+ * primary-hit material, decoded shading normal, linear depth / depth_scale,
+ * motion (from a crt_gbuffer of the same view), 4 zeros. */
+crt_status crt_kpcn_features(crt_scene *scene, const crt_gbuffer *gb, const float *d_direct, const float *d_indirect,
+                             int32_t spp, int64_t pixels, float depth_scale, void *d_features, float *d_noisy,
+                             void *stream);
+/* d_out (float4 per pixel) = the filtered radiance. */
+crt_status crt_kpcn_forward(crt_kpcn *k, int32_t n, int32_t h, int32_t w, const void *d_features,
+                            const float *d_noisy, float *d_out, void *stream);
+/* Forward, relMSE loss against d_target (mean over pixels and RGB of
+ * (out - ref)^2 / (ref^2 + 0.01)), backward; then an Adam step when lr > 0.
+ * *loss (may be NULL) receives the batch loss (synchronises). */
+crt_status crt_kpcn_train_step(crt_kpcn *k, int32_t n, int32_t h, int32_t w, const void *d_features,
+                               const float *d_noisy, const float *d_target, float lr, float *loss, void *stream);
+/* Internal tensors of the last forward (tests): 0..9 layer outputs (BF16),
+ * 10 filter logits (FP32, 32 per pixel), 11 pool0, 12 pool1, 13 cat1,
+ * 14 cat0; `bytes` must equal the tensor's size. */
+crt_status crt_kpcn_debug_tensor(crt_kpcn *k, int32_t which, void *host, int64_t bytes);
+
 /* Synchronises the device and returns CRT_ERR_TIMEOUT (clearing the flag)
  * when a tensor-core kernel of this context gave up a bounded wait. */
 crt_status crt_check_device_errors(crt_ctx *ctx);

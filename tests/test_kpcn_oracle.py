@@ -44,3 +44,38 @@ def test_backward_data_with_relu_mask():
     w = rng.normal(size=(9, 2, 4))
     m = rng.normal(size=(1, 3, 3, 4))
     np.testing.assert_allclose(K.conv3x3_backward_data(g, w, m), K.conv3x3_backward_data(g, w) * (m > 0))
+
+
+def test_network_gradient_matches_finite_differences():
+    """Exact (float64, no BF16 rounding) U-Net: backward == d loss / d params."""
+    rng = np.random.default_rng(2)
+    n, h, w = 1, 8, 8
+    nparams = sum(9 * co * ci + co for ci, co, _ in K.SPEC)
+    params = rng.normal(size=nparams) * 0.1
+    feat = np.zeros((n, h, w, 16))
+    feat[..., :12] = rng.normal(size=(n, h, w, 12))
+    noisy = np.abs(rng.normal(size=(n, h, w, 4)))
+    ref = np.abs(rng.normal(size=(n, h, w, 4)))
+    ident = lambda x: np.asarray(x, dtype=np.float64)
+
+    def loss(p):
+        a, logits, _ = K.kpcn_forward(p, feat, noisy, rnd=ident)
+        return K.filter_loss_grad(logits, noisy, ref)[0]
+
+    a, logits, _ = K.kpcn_forward(params, feat, noisy, rnd=ident)
+    _, dl = K.filter_loss_grad(logits, noisy, ref)
+    g = K.kpcn_backward(params, a, feat, dl, rnd=ident)
+    # offsets of each layer's weights and bias
+    offs, off = [], 0
+    for ci, co, _ in K.SPEC:
+        offs.append((off, off + 9 * co * ci))
+        off += 9 * co * ci + co
+    idx = []
+    for wo, bo in offs:
+        idx += [wo + int(rng.integers(0, bo - wo)), bo]
+    eps = 1e-6
+    for i in idx:
+        d = np.zeros_like(params)
+        d[i] = eps
+        num = (loss(params + d) - loss(params - d)) / (2 * eps)
+        assert abs(num - g[i]) <= 1e-5 * max(1e-3, abs(num)) + 1e-9, (i, num, g[i])
