@@ -318,6 +318,49 @@ def serve_leg(ctx, quick=False):
     return out
 
 
+def denoise_leg(ctx):
+    """Learned denoiser (survey config C5 on a bounded sample): the KPCN is
+    trained on the GPU on 64 views of seeded Cornell variants (scene seeds
+    100-131, 256x256, 1-16 spp inputs, 1024-spp references) for 1500 Adam
+    steps of 8 random 128x128 crops, then evaluated on unseen scenes (seeds
+    200-207, one 256x256 view each) by relMSE against 4096-spp references:
+    raw and KPCN at 1-32 spp, SVGF at 64 spp. The smallest spp at which the
+    KPCN matches 64 spp + SVGF then sets the learned pipeline of the
+    requests/s comparison: 32 requests at 512x512 served through the
+    multi-scene server at that spp + KPCN, against the one-request-at-a-time
+    loop of 64 spp + SVGF."""
+    import torch
+
+    from cudaraytracer_b200 import denoise as D
+    from cudaraytracer_b200.kpcn import Kpcn
+
+    t0 = time.perf_counter()
+    data = D.build_dataset(ctx, range(100, 132), 2, 256, 256, [1, 2, 4, 8, 16], 1024, seed=0)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    net = Kpcn(ctx, seed=0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    losses = D.train(net, data, 1500, batch=8, crop=128, lr=1e-3)
+    e1.record()
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    spp_list = [1, 2, 4, 8, 16, 32]
+    tab = D.evaluate(ctx, net, range(200, 208), 256, 256, spp_list)
+    k = D.matching_spp(tab, spp_list)
+    thr = D.pipeline_throughput(ctx, net, range(200, 208), 512, 512, 32, k or 32)
+    # training throughput: pixels x (forward + backward) per second
+    px = 1500 * 8 * 128 * 128
+    net.close()
+    return {"workload": "Cornell variants: train seeds 100-131 (64 views, 256^2, 1-16 spp, 1024-spp refs), "
+                        "test seeds 200-207 (256^2, 4096-spp refs)",
+            "dataset_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2), "train_steps": 1500,
+            "train_mpix_per_s": round(px / (e0.elapsed_time(e1) * 1e-3) / 1e6, 1),
+            "loss_first": round(float(sum(losses[:20]) / 20), 5), "loss_last": round(float(sum(losses[-50:]) / 50), 5),
+            "relmse": {k2: round(v, 6) for k2, v in tab.items()}, "kpcn_spp_matching_svgf64": k,
+            "throughput": thr}
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU implementation of the path
     (rank 0 only), on the same scene, metric and unit."""
@@ -372,6 +415,7 @@ def main():
     ap.add_argument("--no-render", action="store_true", help="skip the full-frame render leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the multi-scene serving leg")
+    ap.add_argument("--no-denoise", action="store_true", help="skip the learned-denoiser leg")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays (and shadow queries) per step per GPU")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -452,6 +496,9 @@ def main():
     serve = None
     if rank == 0 and not args.no_serve:
         serve = serve_leg(ctx)
+    denoise = None
+    if rank == 0 and not args.no_denoise:
+        denoise = denoise_leg(ctx)
 
     # e2e through the host-buffer API: pinned host inputs, results back.
     pin_r = torch.from_numpy(rays_np).pin_memory()
@@ -523,6 +570,7 @@ def main():
             "render": render,
             "batch": batch,
             "serve": serve,
+            "denoise": denoise,
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
         }

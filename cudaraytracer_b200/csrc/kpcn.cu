@@ -14,7 +14,8 @@
 //   out 32->32 (25 used): filter logits (FP32)
 // Every conv but `out` is followed by ReLU; pooling is 2x2 averaging,
 // upsampling nearest. Input features (16 channels): log(1 + radiance) (3),
-// albedo (3), shading normal (3), linear depth (1), motion (2), zeros (4).
+// albedo (3), shading normal (3), linear depth (1), motion (2),
+// 1 / sqrt(spp) (1), zeros (3).
 // Output: softmax over the 25 logits weights the 5x5 neighbourhood of the
 // noisy radiance (clamped at the image border).
 //
@@ -41,7 +42,7 @@ struct LayerSpec {
     bool relu;
 };
 // e0a e0b e1a e1b e2a e2b d1a d1b d0a d0b out
-constexpr LayerSpec kSpec[kLayers] = {{16, 32, 12, true},  {32, 32, 32, true},   {32, 64, 32, true}, {64, 64, 64, true},
+constexpr LayerSpec kSpec[kLayers] = {{16, 32, 13, true},  {32, 32, 32, true},   {32, 64, 32, true}, {64, 64, 64, true},
                                       {64, 96, 64, true},  {96, 96, 96, true},   {160, 64, 160, true},
                                       {64, 64, 64, true},  {96, 32, 96, true},   {32, 32, 32, true}, {32, 32, 32, false}};
 enum { E0A, E0B, E1A, E1B, E2A, E2B, D1A, D1B, D0A, D0B, OUT };
@@ -186,6 +187,7 @@ __global__ void k_features(FeatureArgs a) {
         f[0] = log1pf(fmaxf(r, 0.f));
         f[1] = log1pf(fmaxf(g, 0.f));
         f[2] = log1pf(fmaxf(b, 0.f));
+        f[12] = sqrtf(a.inv_spp);  // noise level of the estimate
         const ushort4 bm = a.bary_mesh[p];
         if (bm.w != 0) {  // a primary hit (mesh id + 1)
             const ushort4 nm = a.normal_mat[p];

@@ -1,0 +1,273 @@
+"""Training data, training and evaluation of the learned denoiser (kpcn.py)
+against SVGF, on seeded Cornell-box variants rendered by the tracer itself.
+
+* A training example is one rendered view: the network input (features of
+  a k-spp render and its G-buffer) and the reference radiance of the same
+  view from an independent sample range (samples from 2^20 on), many spp.
+* Training draws random crops of random examples per step and runs the
+  GPU's own forward, backward and Adam step (crt_kpcn_train_step).
+* Evaluation measures relMSE = mean((x - ref)^2 / (ref^2 + 0.01)) against a
+  4096-spp reference for: the raw k-spp image, the KPCN output at k spp, and
+  SVGF (the reference's filter: TemporalDenoising, variance estimate and 5
+  a-trous passes) applied to a k-spp image as a two-frame sequence of the
+  same image, which runs the variance estimate and the a-trous passes that a
+  first frame skips.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from .kpcn import Kpcn, make_features
+from .tracer import Scene, Svgf
+
+REF_FIRST_SAMPLE = 1 << 20
+DEPTH_SCALE = 4.0
+
+
+@dataclass
+class Example:
+    feat: object   # (h, w, 16) bfloat16 CUDA tensor
+    noisy: object  # (h, w, 4) float32
+    ref: object    # (h, w, 4) float32
+    spp: int
+
+
+def view_cameras(scene: Scene, n: int, seed: int):
+    """n orbit poses looking into the open side of a Cornell box: elevation
+    U[75, 105] deg, azimuth U[-20, 20] deg, distance x U[0.85, 1.1]."""
+    rng = np.random.default_rng(seed)
+    c = scene.camera()
+    out = []
+    for _ in range(n):
+        out.append({"target": list(c["target"]), "distance": float(c["distance"]) * float(rng.uniform(0.85, 1.1)),
+                    "theta_deg": float(rng.uniform(75, 105)), "phi_deg": float(rng.uniform(-20, 20)),
+                    "fovy_deg": float(c["fovy_deg"])})
+    return out
+
+
+def render_view(scene: Scene, cam: dict, width: int, height: int, spp: int, seed: int, first_sample: int = 0):
+    """(direct, indirect) float32 (h, w, 4) CUDA sums over spp samples."""
+    import torch
+
+    scene.set_render_params(width=width, height=height, seed=seed)
+    scene.set_camera_orbit(cam["target"], cam["distance"], cam["theta_deg"], cam["phi_deg"], cam["fovy_deg"])
+    d = torch.zeros((height, width, 4), device="cuda")
+    i = torch.zeros_like(d)
+    if spp:
+        scene.render_device(d, i, spp, first_sample=first_sample)
+    return d, i
+
+
+def make_example(scene: Scene, cam: dict, width: int, height: int, spp: int, ref_spp: int, seed: int) -> Example:
+    d, i = render_view(scene, cam, width, height, spp, seed)
+    g = scene.gbuffer()
+    feat, noisy = make_features(scene, g, d, i, spp, DEPTH_SCALE)
+    rd, ri = render_view(scene, cam, width, height, ref_spp, seed, first_sample=REF_FIRST_SAMPLE)
+    ref = (rd + ri) / ref_spp
+    return Example(feat, noisy, ref, spp)
+
+
+def build_dataset(ctx, scene_seeds, views_per_scene: int, width: int, height: int, spp_choices, ref_spp: int,
+                  seed: int = 0):
+    """Examples over seeded Cornell variants; each view's spp drawn from
+    spp_choices."""
+    from . import scenes
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in scene_seeds:
+        sc = Scene.from_spec(ctx, scenes.cornell_box(width=width, height=height, seed=int(s)))
+        for v, cam in enumerate(view_cameras(sc, views_per_scene, int(s) * 7 + 1)):
+            spp = int(spp_choices[int(rng.integers(len(spp_choices)))])
+            out.append(make_example(sc, cam, width, height, spp, ref_spp, seed=int(s) * 1000 + v))
+        sc.close()
+    return out
+
+
+def train(net: Kpcn, data, steps: int, batch: int = 8, crop: int = 128, lr: float = 1e-3, seed: int = 0):
+    """Adam steps on random crops (crop x crop, multiple of 4) of random
+    examples; the learning rate decays by cosine to 5% of lr. Returns the
+    per-step losses."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    losses = []
+    for k in range(steps):
+        fs, ns, rs = [], [], []
+        for _ in range(batch):
+            ex = data[int(rng.integers(len(data)))]
+            h, w = ex.feat.shape[0], ex.feat.shape[1]
+            y = int(rng.integers(0, h - crop + 1)) // 4 * 4
+            x = int(rng.integers(0, w - crop + 1)) // 4 * 4
+            fs.append(ex.feat[y:y + crop, x:x + crop])
+            ns.append(ex.noisy[y:y + crop, x:x + crop])
+            rs.append(ex.ref[y:y + crop, x:x + crop])
+        f = torch.stack(fs).contiguous()
+        nz = torch.stack(ns).contiguous()
+        rf = torch.stack(rs).contiguous()
+        cur = lr * (0.05 + 0.95 * 0.5 * (1 + math.cos(math.pi * k / max(1, steps))))
+        losses.append(net.train_step(f, nz, rf, cur))
+    return losses
+
+
+def relmse(x, ref) -> float:
+    """mean over pixels and RGB of (x - ref)^2 / (ref^2 + 0.01) (CUDA tensors)."""
+    a, r = x[..., :3].double(), ref[..., :3].double()
+    return float(((a - r) ** 2 / (r * r + 0.01)).mean())
+
+
+def svgf_denoise(ctx, gbuffer: dict, d, i, spp: int, state: Svgf | None = None):
+    """SVGF (the reference's filter) on one spp-sample image: two frames of
+    the same image and G-buffer, so the variance estimate and the a-trous
+    passes run. `state` (an Svgf of the image's size, reset here) is reused
+    when given. Returns the radiance (h, w, 4)."""
+    import torch
+
+    h, w = d.shape[0], d.shape[1]
+    sv = state if state is not None else Svgf(ctx, w, h)
+    sv.reset()
+    nd, ni = (d / spp).contiguous(), (i / spp).contiguous()
+    od, oi = torch.zeros_like(nd), torch.zeros_like(ni)
+    for _ in range(2):
+        sv.frame(gbuffer, gbuffer, nd, ni, od, oi)
+    if state is None:
+        sv.close()
+    return od + oi
+
+
+def evaluate(ctx, net: Kpcn, scene_seeds, width: int, height: int, spp_list, svgf_spp: int = 64,
+             ref_spp: int = 4096):
+    """relMSE vs a ref_spp reference per test scene (one view each): raw and
+    KPCN at every spp of spp_list, SVGF at svgf_spp. Returns a dict of mean
+    relMSE values."""
+    import torch
+
+    from . import scenes
+
+    acc = {f"raw_{k}": [] for k in spp_list}
+    acc.update({f"kpcn_{k}": [] for k in spp_list})
+    acc[f"svgf_{svgf_spp}"] = []
+    acc[f"raw_{svgf_spp}"] = []
+    for s in scene_seeds:
+        sc = Scene.from_spec(ctx, scenes.cornell_box(width=width, height=height, seed=int(s)))
+        cam = view_cameras(sc, 1, int(s) * 7 + 3)[0]
+        rd, ri = render_view(sc, cam, width, height, ref_spp, seed=int(s), first_sample=REF_FIRST_SAMPLE)
+        ref = (rd + ri) / ref_spp
+        for k in sorted(set(list(spp_list) + [svgf_spp])):
+            d, i = render_view(sc, cam, width, height, k, seed=int(s))
+            g = sc.gbuffer()
+            if k in spp_list:
+                feat, noisy = make_features(sc, g, d, i, k, DEPTH_SCALE)
+                out = net.forward(feat[None].contiguous(), noisy[None].contiguous())[0]
+                acc[f"raw_{k}"].append(relmse(noisy, ref))
+                acc[f"kpcn_{k}"].append(relmse(out, ref))
+            if k == svgf_spp:
+                acc[f"svgf_{k}"].append(relmse(svgf_denoise(ctx, g, d, i, k), ref))
+                acc[f"raw_{k}"].append(relmse((d + i) / k, ref))
+        torch.cuda.synchronize()
+        sc.close()
+    return {k: float(np.mean(v)) for k, v in acc.items() if v}
+
+
+def matching_spp(table: dict, spp_list, svgf_spp: int = 64):
+    """Smallest k with KPCN relMSE at k spp <= SVGF's at svgf_spp (None if
+    none)."""
+    target = table[f"svgf_{svgf_spp}"]
+    for k in sorted(spp_list):
+        if table[f"kpcn_{k}"] <= target:
+            return k
+    return None
+
+
+def pipeline_throughput(ctx, net: Kpcn, scene_seeds, width: int, height: int, n_requests: int, learned_spp: int,
+                        plain_spp: int = 64, seed: int = 0):
+    """Requests/s of two ways to serve n_requests denoised views (scene and
+    pose drawn per request): the plain loop, one request at a time, renders
+    plain_spp spp and runs SVGF; the learned pipeline submits all requests at
+    learned_spp to the multi-scene server (continuous batching), then builds
+    features and runs the KPCN on all finished images in one batch. Both
+    end with the denoised radiance on the device; GPU work is synchronised
+    before the clock stops."""
+    import torch
+
+    from . import scenes
+    from .serve import RenderRequest, Server
+
+    rng = np.random.default_rng(seed)
+    scs = [Scene.from_spec(ctx, scenes.cornell_box(width=width, height=height, seed=int(s))) for s in scene_seeds]
+    reqs = []
+    for k in range(n_requests):
+        si = int(rng.integers(len(scs)))
+        cam = view_cameras(scs[si], 1, seed * 1000 + k)[0]
+        reqs.append((si, cam, 5000 + k))
+
+    # plain loop (warm once); one SVGF state reused across requests
+    sv = Svgf(ctx, width, height)
+
+    def plain_one(si, cam, sd):
+        d, i = render_view(scs[si], cam, width, height, plain_spp, sd)
+        g = scs[si].gbuffer()
+        return svgf_denoise(ctx, g, d, i, plain_spp, state=sv)
+
+    plain_one(*reqs[0])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in reqs:
+        plain_one(*r)
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    sv.close()
+
+    srv = Server(ctx, paths_per_pass=8 << 20)
+    for sc in scs:
+        srv.add_scene(sc)
+
+    def learned_all():
+        ids = [srv.submit(RenderRequest(si, width, height, learned_spp, cam, seed=sd)) for si, cam, sd in reqs]
+        srv.drain()
+        feats, noisy = [], []
+        for rid, (si, cam, sd) in zip(ids, reqs):
+            dp, ip = srv.result_device(rid)
+            d = torch.empty((height, width, 4), device="cuda")
+            i = torch.empty_like(d)
+            d.view(-1).copy_(_wrap_device(dp, height * width * 4))
+            i.view(-1).copy_(_wrap_device(ip, height * width * 4))
+            sc = scs[si]
+            sc.set_render_params(width=width, height=height)
+            sc.set_camera_orbit(cam["target"], cam["distance"], cam["theta_deg"], cam["phi_deg"], cam["fovy_deg"])
+            f, nz = make_features(sc, sc.gbuffer(), d, i, learned_spp, DEPTH_SCALE)
+            feats.append(f)
+            noisy.append(nz)
+            srv.release(rid)
+        return net.forward(torch.stack(feats).contiguous(), torch.stack(noisy).contiguous())
+
+    learned_all()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    learned_all()
+    torch.cuda.synchronize()
+    learned_s = time.perf_counter() - t0
+    srv.close()
+    for sc in scs:
+        sc.close()
+    return {"requests": n_requests, "resolution": [width, height],
+            "plain": {"spp": plain_spp, "denoiser": "svgf", "wall_s": round(plain_s, 4),
+                      "req_per_s": round(n_requests / plain_s, 2)},
+            "learned": {"spp": learned_spp, "denoiser": "kpcn", "wall_s": round(learned_s, 4),
+                        "req_per_s": round(n_requests / learned_s, 2)},
+            "req_per_s_ratio": round(plain_s / learned_s, 3)}
+
+
+def _wrap_device(ptr: int, count: int):
+    """A float32 CUDA tensor view of `count` floats at device address ptr
+    (server-owned memory, valid until the request is released)."""
+    import torch
+
+    class _Arr:
+        __cuda_array_interface__ = {"shape": (count,), "typestr": "<f4", "data": (ptr, False), "version": 3}
+
+    return torch.as_tensor(_Arr(), device="cuda")

@@ -91,6 +91,7 @@ class Kpcn:
         h = C.c_void_p()
         _lib.call("crt_kpcn_create", ctx.handle, int(seed), C.byref(h))
         self._h = h
+        ctx._adopt(self)
         n = C.c_int64()
         _lib.call("crt_kpcn_num_params", self._h, C.byref(n))
         self.num_params = n.value

@@ -166,19 +166,38 @@ GREEN = [0.14, 0.45, 0.09]
 LIGHT_KE = [17.0, 12.0, 4.0]
 
 
-def cornell_box(width=256, height=256, spp=16, max_bounces=8, rr=0.8) -> SceneSpec:
+def cornell_box(width=256, height=256, spp=16, max_bounces=8, rr=0.8, seed=None) -> SceneSpec:
+    """The 36-triangle Cornell box. With a seed, a variant of it: box
+    positions, sizes and rotations, wall colours and the light's size and
+    emission drawn from ranges around the canonical values (the
+    denoiser's training and test scenes)."""
     P = lambda x, y, z: (float(x), float(y), float(z))
     white, red, green = [], [], []
+    wall_l, wall_r, ke = RED, GREEN, LIGHT_KE
+    b1 = ((0.33, 0.30, 0.36), (0.28, 0.60, 0.28), 18.0)
+    b2 = ((0.67, 0.15, 0.63), (0.28, 0.30, 0.28), -18.0)
+    half = 0.125
+    if seed is not None:
+        rng = np.random.default_rng(seed)
+        hue = lambda base: np.clip(np.asarray(base) * rng.uniform(0.6, 1.4, 3), 0.02, 0.9).round(4).tolist()
+        wall_l, wall_r = hue(RED), hue(GREEN)
+        ke = (np.asarray(LIGHT_KE) * rng.uniform(0.7, 1.3)).round(3).tolist()
+        half = float(rng.uniform(0.09, 0.17))
+        hgt1, hgt2 = rng.uniform(0.4, 0.7), rng.uniform(0.2, 0.35)
+        s1, s2 = rng.uniform(0.22, 0.30, 2)
+        b1 = ((rng.uniform(0.27, 0.38), hgt1 / 2, rng.uniform(0.30, 0.42)), (s1, hgt1, s1), rng.uniform(8, 30))
+        b2 = ((rng.uniform(0.62, 0.72), hgt2 / 2, rng.uniform(0.58, 0.70)), (s2, hgt2, s2), -rng.uniform(8, 30))
     # floor y=0 (+y), ceiling y=1 (-y), back z=0 (+z): CCW seen from inside
     white += _quad(P(0, 0, 0), P(0, 0, 1), P(1, 0, 1), P(1, 0, 0))
     white += _quad(P(0, 1, 0), P(1, 1, 0), P(1, 1, 1), P(0, 1, 1))
     white += _quad(P(0, 0, 0), P(1, 0, 0), P(1, 1, 0), P(0, 1, 0))
     red += _quad(P(0, 0, 0), P(0, 1, 0), P(0, 1, 1), P(0, 0, 1))  # x=0, +x
     green += _quad(P(1, 0, 0), P(1, 0, 1), P(1, 1, 1), P(1, 1, 0))  # x=1, -x
-    boxes = _box((0.33, 0.30, 0.36), (0.28, 0.60, 0.28), 18.0)
-    boxes += _box((0.67, 0.15, 0.63), (0.28, 0.30, 0.28), -18.0)
+    boxes = _box(*b1)
+    boxes += _box(*b2)
     h = 0.999
-    light = _quad(P(0.375, h, 0.375), P(0.625, h, 0.375), P(0.625, h, 0.625), P(0.375, h, 0.625))
+    lo, hi = 0.5 - half, 0.5 + half
+    light = _quad(P(lo, h, lo), P(hi, h, lo), P(hi, h, hi), P(lo, h, hi))
 
     def arr(t):
         return np.asarray(t, dtype=np.float32).reshape(-1, 9)
@@ -192,9 +211,9 @@ def cornell_box(width=256, height=256, spp=16, max_bounces=8, rr=0.8) -> SceneSp
     ]
     materials = [
         {"name": "white", "type": "diffuse", "basecolor": WHITE},
-        {"name": "red", "type": "diffuse", "basecolor": RED},
-        {"name": "green", "type": "diffuse", "basecolor": GREEN},
-        {"name": "light", "type": "light", "emission": LIGHT_KE},
+        {"name": "red", "type": "diffuse", "basecolor": wall_l},
+        {"name": "green", "type": "diffuse", "basecolor": wall_r},
+        {"name": "light", "type": "light", "emission": ke},
     ]
     lights = [{"type": "area", "lightMeshName": "light", "material": "light"}]
     camera = {

@@ -49,6 +49,7 @@ class Server:
         _lib.call("crt_server_create", ctx._h, C.byref(cfg), C.byref(h))
         self._h = h
         self._scenes = []
+        ctx._adopt(self)
 
     def close(self):
         if self._h:

@@ -39,19 +39,36 @@ def _torch_stream(device, stream=None) -> int:
 
 
 class Context:
-    """A crt_ctx bound to one CUDA device."""
+    """A crt_ctx bound to one CUDA device. Objects created on it (scenes,
+    servers, SVGF states, denoiser networks) register here and are closed
+    before the context, so none outlives the crt_ctx it points to."""
 
     def __init__(self, device: int = 0):
+        import weakref
+
         self._h = C.c_void_p()
         _lib.call("crt_create", int(device), C.byref(self._h))
         self.device = device
+        self._children = weakref.WeakSet()
 
     @property
     def handle(self):
         return self._h
 
+    def _adopt(self, obj):
+        if not self._h:
+            raise RuntimeError("context is closed")
+        self._children.add(obj)
+
     def close(self):
         if self._h:
+            # servers first: they reference scenes
+            kids = sorted(list(self._children), key=lambda o: 0 if type(o).__name__ == "Server" else 1)
+            for obj in kids:
+                try:
+                    obj.close()
+                except Exception:
+                    pass
             _lib.lib().crt_destroy(self._h)
             self._h = C.c_void_p()
 
@@ -68,6 +85,7 @@ class Scene:
     def __init__(self, ctx: Context, handle: C.c_void_p):
         self.ctx = ctx
         self._h = handle
+        ctx._adopt(self)
 
     @classmethod
     def from_triangles(cls, ctx: Context, tris: np.ndarray) -> "Scene":
@@ -398,6 +416,7 @@ class Svgf:
         self.width, self.height = width, height
         self._h = C.c_void_p()
         _lib.call("crt_svgf_create", ctx.handle, int(width), int(height), C.byref(self._h))
+        ctx._adopt(self)
 
     @property
     def handle(self):

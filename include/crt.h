@@ -428,7 +428,7 @@ crt_status crt_kpcn_get_grads(crt_kpcn *k, float *host);
 /* Network input from a render: noisy = (direct + indirect) / spp per pixel
  * (float4) and the 16 feature channels: log(1 + noisy rgb), albedo of the
  * primary-hit material, decoded shading normal, linear depth / depth_scale,
- * motion (from a crt_gbuffer of the same view), 4 zeros. */
+ * motion (from a crt_gbuffer of the same view), 1 / sqrt(spp), 3 zeros. */
 crt_status crt_kpcn_features(crt_scene *scene, const crt_gbuffer *gb, const float *d_direct, const float *d_indirect,
                              int32_t spp, int64_t pixels, float depth_scale, void *d_features, float *d_noisy,
                              void *stream);

@@ -62,9 +62,10 @@ def test_forward_loss_and_gradients_match_oracle(crt_ctx):
     ref_loss, dl = K.filter_loss_grad(ref_logits, noisy, ref)
     ref_grads = K.kpcn_backward(params, a, feat, dl)
 
-    # activations: BF16 values equal up to rare one-ulp rounding flips
+    # activations: BF16 values equal up to rare one-ulp rounding flips (and
+    # ReLU kinks, where FP32 accumulation error decides the sign)
     assert np.mean(e0b != a["e0b"]) < 0.02
-    assert np.allclose(e0b, a["e0b"], rtol=2 ** -7, atol=1e-6)
+    assert np.allclose(e0b, a["e0b"], rtol=2 ** -7, atol=1e-4)
     err = np.linalg.norm(logits[..., :25] - ref_logits[..., :25]) / np.linalg.norm(ref_logits[..., :25])
     assert err < 5e-3
     assert not logits[..., 25:].any()
@@ -127,5 +128,6 @@ def test_features_from_a_render(tmp_path, crt_ctx):
     nrm = np.linalg.norm(f[..., 6:9], axis=-1)
     assert np.all(np.abs(nrm - 1) < 0.02)
     assert np.all((f[..., 3:6] >= 0) & (f[..., 3:6] <= 1))
-    assert np.all(f[..., 9] > 0) and not f[..., 12:].any()
+    assert np.all(f[..., 9] > 0) and not f[..., 13:].any()
+    assert np.all(f[..., 12] == K.bf16_round(np.array([2 ** -0.5], np.float32))[0])
     sc.close()
