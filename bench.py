@@ -318,6 +318,49 @@ def serve_leg(ctx, quick=False):
     return out
 
 
+def conv_leg(ctx, h=1080, w=1920, cin=64, cout=64, reps=10):
+    """Tensor-core 3x3 convolution at 1920x1080 with 64 -> 64 channels
+    (the denoiser's most common shape): forward (bias + ReLU), data gradient
+    and weight gradient, each timed with CUDA events over `reps` launches
+    after a warm-up. FLOPs = 2 * 9 * cin * cout * pixels per launch;
+    roofline against the measured BF16 peak (burst)."""
+    import torch
+
+    from cudaraytracer_b200 import kpcn
+
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn((1, h, w, cin), device="cuda", generator=g).to(torch.bfloat16)
+    wt = (torch.randn((9, cout, cin), device="cuda", generator=g) / 24).to(torch.bfloat16)
+    wtt = wt.permute(0, 2, 1).contiguous()
+    b = torch.zeros(cout, device="cuda")
+    gy = torch.randn((1, h, w, cout), device="cuda", generator=g).to(torch.bfloat16)
+    y = torch.empty((1, h, w, cout), dtype=torch.bfloat16, device="cuda")
+    gx = torch.empty((1, h, w, cin), dtype=torch.bfloat16, device="cuda")
+    dw = torch.zeros((9, cout, cin), device="cuda")
+    ops = {"forward": lambda: kpcn.conv3x3_forward(ctx, x, wt, b, relu=True, out=y),
+           "backward_data": lambda: kpcn.conv3x3_backward_data(ctx, gy, wtt, out=gx),
+           "backward_weights": lambda: kpcn.conv3x3_backward_weights(ctx, x, gy, dw=dw)}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, kind = (float(json.load(open(pp))["bf16_tflops"]), "measured") if os.path.exists(pp) else (1590.0, "fallback")
+    flops = 2.0 * 9 * cin * cout * h * w
+    out = {"shape": f"1x{h}x{w}, {cin}->{cout}", "flops_per_launch": flops, "peak_tflops": peak, "peak_kind": kind}
+    for name, fn in ops.items():
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        tf = flops / (ms * 1e-3) / 1e12
+        out[name] = {"ms_per_launch": round(ms, 4), "tflops": round(tf, 1), "frac": round(tf / peak, 4)}
+    kpcn.check_device_errors(ctx)
+    return out
+
+
 def denoise_leg(ctx):
     """Learned denoiser (survey config C5 on a bounded sample): the KPCN is
     trained on the GPU on 64 views of seeded Cornell variants (scene seeds
@@ -416,6 +459,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the multi-scene serving leg")
     ap.add_argument("--no-denoise", action="store_true", help="skip the learned-denoiser leg")
+    ap.add_argument("--only", choices=["conv"], default=None,
+                    help="run one micro-benchmark alone (conv: the tensor-core convolutions at 1080p)")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays (and shadow queries) per step per GPU")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -424,6 +469,16 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.only == "conv":
+        import torch
+
+        from cudaraytracer_b200 import Context
+
+        torch.cuda.set_device(local_rank)
+        ctx = Context(local_rank)
+        print(json.dumps({"conv": conv_leg(ctx, reps=args.steps)}))
+        ctx.close()
         return
 
     import torch
@@ -499,6 +554,7 @@ def main():
     denoise = None
     if rank == 0 and not args.no_denoise:
         denoise = denoise_leg(ctx)
+        denoise["conv"] = conv_leg(ctx)
 
     # e2e through the host-buffer API: pinned host inputs, results back.
     pin_r = torch.from_numpy(rays_np).pin_memory()
