@@ -114,7 +114,12 @@ class MaterialDesc(C.Structure):
         ("transmission", C.c_float),
         ("scatter_distance", C.c_float * 3),
         ("ior", C.c_float),
+        ("texture", C.c_int32),
     ]
+
+
+class TextureDesc(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("rgba", C.c_void_p)]
 
 
 class MeshDesc(C.Structure):
@@ -140,6 +145,8 @@ class SceneDesc(C.Structure):
         ("env_width", C.c_int32),
         ("env_height", C.c_int32),
         ("env_rgba", C.c_void_p),
+        ("n_textures", C.c_int32),
+        ("textures", C.c_void_p),
         ("width", C.c_int32),
         ("height", C.c_int32),
         ("spp", C.c_int32),
@@ -204,6 +211,7 @@ _SIGS = {
     "crt_scene_info": (C.c_int, [_VP, C.POINTER(SceneInfo)]),
     "crt_scene_load_json": (C.c_int, [_VP, C.c_char_p, C.POINTER(_VP)]),
     "crt_scene_from_arrays": (C.c_int, [_VP, C.POINTER(SceneDesc), C.POINTER(_VP)]),
+    "crt_image_decode": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _VP]),
     "crt_scene_export_geometry": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "crt_scene_export_tables": (C.c_int, [_VP, _VP, _VP, _VP]),
     "crt_get_render_params": (C.c_int, [_VP, C.POINTER(RenderParams)]),
@@ -214,6 +222,7 @@ _SIGS = {
     "crt_render_device": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
     "crt_render_device_noalloc": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP, _VP, _VP]),
     "crt_render_views": (C.c_int, [_VP, C.c_int32, _VP, C.c_int32, C.c_int32, _VP, _VP, _VP, C.c_int32, _VP]),
+    "crt_gather": (C.c_int, [_VP, C.c_int32, C.c_int32, C.c_int32, _VP, _VP, C.POINTER(GBuffer), _VP, _VP]),
     "crt_server_create": (C.c_int, [_VP, C.POINTER(ServerConfig), C.POINTER(_VP)]),
     "crt_server_free": (None, [_VP]),
     "crt_server_add_scene": (C.c_int, [_VP, _VP, C.POINTER(C.c_int32)]),

@@ -250,6 +250,19 @@ void host_scene_from_desc(const crt_scene_desc &d, HostScene &h) {
     h.rr = d.rr;
     h.fovy = d.fovy;
     for (int k = 0; k < 3; ++k) h.direction[k] = d.direction[k];
+    CRT_CHECK(d.n_textures >= 0 && (d.n_textures == 0 || d.textures), CRT_ERR_INVALID,
+              "crt_scene_from_arrays: textures");
+    for (int i = 0; i < d.n_textures; ++i) {
+        const crt_texture_desc &td = d.textures[i];
+        CRT_CHECK(td.width > 0 && td.height > 0 && td.width <= (1 << 15) && td.height <= (1 << 15) && td.rgba,
+                  CRT_ERR_INVALID, "crt_scene_from_arrays: bad texture");
+        HostTexture t;
+        t.name = "texture" + std::to_string(i);
+        t.width = td.width;
+        t.height = td.height;
+        t.rgba.assign(td.rgba, td.rgba + (size_t)4 * td.width * td.height);
+        h.textures.push_back(std::move(t));
+    }
     h.materials.resize(d.n_materials);
     h.material_names.resize(d.n_materials);
     for (int i = 0; i < d.n_materials; ++i) {
@@ -267,6 +280,9 @@ void host_scene_from_desc(const crt_scene_desc &d, HostScene &h) {
         m.metallic = md.metallic;
         m.transmission = md.transmission;
         m.ior = md.ior;
+        CRT_CHECK(md.texture >= -1 && md.texture < d.n_textures, CRT_ERR_INVALID,
+                  "crt_scene_from_arrays: bad material texture");
+        m.tex = md.texture;
         h.materials[i] = m;
         h.material_names[i] = "material" + std::to_string(i);
     }

@@ -50,23 +50,54 @@ __device__ __forceinline__ uint32_t tmem_cols(int n) {
     return c;
 }
 
+constexpr int kHalo = kBM + 2;  // rows of one halo region
+constexpr int kConvStages = 3;
+
+// Position q of the padded linear image space (rows of W + 2: columns W and
+// W + 1 are zero padding, column W + 1 doubling as column -1 of the next
+// row; row 0 and one row after every image are zero rows) -> NHWC pixel
+// index, or -1 for padding.
+// (32-bit arithmetic: the host refuses images whose padded space reaches 2^31.)
+__device__ __forceinline__ int padded_to_pixel(int q, int W, int H, int NR) {
+    if (q < 0) return -1;
+    const int Wp = W + 2;
+    const int R = q / Wp;
+    const int x = q - R * Wp;
+    if (x >= W || R < 1 || R > NR - 2) return -1;
+    const int rr = R - 1;
+    const int b = rr / (H + 1);
+    const int r = rr - b * (H + 1);
+    if (r >= H) return -1;
+    return (b * H + r) * W + x;
+}
+
+// One CTA walks its tiles of 128 consecutive padded positions. Per tile and
+// channel chunk of KC, a stage holds three halo regions (input rows shifted
+// by -1, 0, +1; 130 positions each: the tile plus one on either side) and the
+// chunk of all 9 taps' weights. Tap (dy, dx) is then the MMA whose A operand
+// starts dx + 1 rows (16 B each) into region dy + 1: no per-tap gather. Two
+// TMEM accumulator slots let a tile's epilogue overlap the first MMAs of
+// the next tile.
 __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ uint64_t bars[kStages + 1];
+    __shared__ uint64_t bars[kConvStages + 2];
     __shared__ uint32_t tmem_slot;
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int C = a.C, N = a.N, KC = a.KC;
-    const int P = a.nimg * a.h * a.wd, HW = a.h * a.wd;
-    const int ntiles = (P + kBM - 1) / kBM;
-    const int chunks = C / KC, steps = 9 * chunks;
-    const uint32_t a_bytes = kBM * KC * 2, b_bytes = (uint32_t)N * KC * 2;
+    const int C = a.C, N = a.N, KC = a.KC, W = a.wd, H = a.h;
+    const int Wp = W + 2, NR = a.nimg * (H + 1) + 1;
+    const int qbeg = Wp, qend = Wp * (NR - 1);
+    const int ntiles = (qend - qbeg + kBM - 1) / kBM;
+    const int chunks = C / KC, KG = KC / 8;
+    const uint32_t lbo_a = kHalo * 16, region_bytes = KG * lbo_a, a_bytes = 3 * region_bytes;
+    const uint32_t lbo_b = (uint32_t)N * 16, tap_bytes = KG * lbo_b, b_bytes = 9 * tap_bytes;
     const uint32_t stage_bytes = a_bytes + b_bytes;
-    const uint32_t lbo_a = (kBM / 8) * 128, lbo_b = (uint32_t)(N / 8) * 128;
     const uint32_t idesc = tc::idesc_bf16(kBM, N, false, false);
-    const uint32_t ncols = tmem_cols(N);
+    const uint32_t ncols = tmem_cols(2 * N);
+    const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int total = my_tiles * chunks;
 
     if (tid == 0) {
-        for (int s = 0; s <= kStages; ++s) tc::mbar_init(&bars[s], 1);
+        for (int i = 0; i < kConvStages + 2; ++i) tc::mbar_init(&bars[i], 1);
         tc::fence_mbar_init();
     }
     if (warp == 0) tc::tmem_alloc(&tmem_slot, ncols);
@@ -74,94 +105,27 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
-
-    uint32_t g = 0;        // global K-step counter (stage = g % kStages)
-    uint32_t tiles_done = 0;
     bool failed = false;
-    for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-        const int m0 = tile * kBM;
-        // this thread's A row: pixel m0 + tid
-        const int p = m0 + tid;
-        const bool pin = p < P;
-        int pb = 0, py = 0, px = 0;
-        if (pin) {
-            pb = p / HW;
-            const int r = p - pb * HW;
-            py = r / a.wd;
-            px = r - py * a.wd;
-        }
-        const uint32_t g0 = g;
-        for (int s = 0; s < steps + kStages - 1; ++s) {
-            bool ok = true;
-            if (s < steps) {
-                const uint32_t gs = g0 + s, st = gs % kStages;
-                if (gs >= kStages) ok = tc::mbar_wait(&bars[st], ((gs / kStages) - 1) & 1);
-                unsigned char *sa = smem_raw + st * stage_bytes, *sb = sa + a_bytes;
-                const int tap = s / chunks, c0 = (s - tap * chunks) * KC;
-                int dy = tap / 3 - 1, dx = tap % 3 - 1;
-                if (a.flip) {
-                    dy = -dy;
-                    dx = -dx;
-                }
-                const int sy = py + dy, sx = px + dx;
-                const bool valid = pin && sy >= 0 && sy < a.h && sx >= 0 && sx < a.wd;
-                const __nv_bfloat16 *src =
-                    valid ? a.in + ((size_t)(pb * HW + sy * a.wd + sx) * C + c0) : a.in;
-                for (int kg = 0; kg < KC / 8; ++kg)
-                    tc::cp_async16(sa + (tid & 7) * 16 + (tid >> 3) * 128 + kg * lbo_a, valid ? src + kg * 8 : src,
-                                   valid ? 16u : 0u);
-                const int vecs = N * (KC / 8);
-                for (int v = tid; v < vecs; v += kThreads) {
-                    const int r = v / (KC / 8), kg = v - r * (KC / 8);
-                    tc::cp_async16(sb + (r & 7) * 16 + (r >> 3) * 128 + kg * lbo_b,
-                                   a.wgt + ((size_t)tap * N + r) * C + c0 + kg * 8, 16u);
-                }
-            }
-            tc::cp_async_commit();
-            const int c = s - (kStages - 1);
-            if (c >= 0) {
-                tc::cp_async_wait<kStages - 1>();
-                tc::fence_proxy_async();
-                if (__syncthreads_or(!ok)) {
-                    failed = true;
-                    break;
-                }
-                if (tid == 0) {
-                    const uint32_t gc = g0 + c, st = gc % kStages;
-                    const uint32_t sa = tc::smem_addr(smem_raw + st * stage_bytes), sb = sa + a_bytes;
-                    tc::fence_after_sync();
-                    for (int j = 0; j < KC / 16; ++j)
-                        tc::mma_bf16(tmem, tc::smem_desc(sa + 2 * j * lbo_a, lbo_a, 128),
-                                     tc::smem_desc(sb + 2 * j * lbo_b, lbo_b, 128), idesc, c > 0 || j > 0);
-                    tc::mma_commit(tc::smem_addr(&bars[st]));
-                }
-            } else if (__syncthreads_or(!ok)) {
-                failed = true;
-                break;
-            }
-        }
-        if (failed) break;
-        g = g0 + steps;
-        // all MMAs of the tile done -> accumulators readable
-        if (tid == 0) tc::mma_commit(tc::smem_addr(&bars[kStages]));
-        const bool ok = tc::mbar_wait(&bars[kStages], tiles_done & 1);
-        ++tiles_done;
-        if (__syncthreads_or(!ok)) {
-            failed = true;
-            break;
-        }
+
+    // epilogue of tile-local index tl: accumulators -> bias / ReLU / mask -> NHWC
+    auto epilogue = [&](int tl) -> bool {
+        const int slot = tl & 1;
+        const bool ok = tc::mbar_wait(&bars[kConvStages + slot], (tl >> 1) & 1);
+        if (__syncthreads_or(!ok)) return false;
         tc::fence_after_sync();
-        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+        const int tile = blockIdx.x + tl * gridDim.x;
+        const int64_t p = padded_to_pixel(qbeg + tile * kBM + tid, W, H, NR);
+        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + slot * N;
         for (int n0 = 0; n0 < N; n0 += 16) {
             float v[16];
             tc::tmem_ld16(lane_base + n0, v);
-            if (!pin) continue;
+            if (p < 0) continue;
             if (a.bias)
                 for (int i = 0; i < 16; ++i) v[i] += a.bias[n0 + i];
             if (a.relu)
                 for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
             if (a.mask) {
-                const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + (size_t)p * N + n0);
+                const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + p * N + n0);
                 uint4 mv[2] = {mp[0], mp[1]};
                 const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(mv);
                 for (int i = 0; i < 16; ++i)
@@ -171,18 +135,79 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
                 uint4 ov[2];
                 __nv_bfloat16 *ob = reinterpret_cast<__nv_bfloat16 *>(ov);
                 for (int i = 0; i < 16; ++i) ob[i] = __float2bfloat16_rn(v[i]);
-                uint4 *op = reinterpret_cast<uint4 *>(a.out + (size_t)p * N + n0);
+                uint4 *op = reinterpret_cast<uint4 *>(a.out + p * N + n0);
                 op[0] = ov[0];
                 op[1] = ov[1];
             }
             if (a.out_f32) {
-                float4 *op = reinterpret_cast<float4 *>(a.out_f32 + (size_t)p * N + n0);
+                float4 *op = reinterpret_cast<float4 *>(a.out_f32 + p * N + n0);
                 for (int i = 0; i < 4; ++i) op[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
             }
         }
         tc::fence_before_sync();
-        __syncthreads();  // TMEM reads done before the next tile's MMAs
+        __syncthreads();  // this slot's TMEM reads are done before it is reused
+        return true;
+    };
+
+    for (int s = 0; s < total + kConvStages - 1 && !failed; ++s) {
+        bool ok = true;
+        if (s < total) {
+            const int st = s % kConvStages;
+            if (s >= kConvStages) ok = tc::mbar_wait(&bars[st], ((s / kConvStages) - 1) & 1);
+            unsigned char *sa = smem_raw + st * stage_bytes, *sb = sa + a_bytes;
+            const int tile = blockIdx.x + (s / chunks) * gridDim.x, c0 = (s % chunks) * KC;
+            const int t0 = qbeg + tile * kBM;
+            // halo: one pixel per (region, row), its KC channels as KG vectors
+            for (int pr = tid; pr < 3 * kHalo; pr += kThreads) {
+                const int r = pr / kHalo, j = pr - r * kHalo;
+                const int p = padded_to_pixel(t0 + (r - 1) * Wp + j - 1, W, H, NR);
+                const __nv_bfloat16 *src = p >= 0 ? a.in + (size_t)p * C + c0 : a.in;
+                unsigned char *dst = sa + r * region_bytes + j * 16;
+                for (int kg = 0; kg < KG; ++kg)
+                    tc::cp_async16(dst + kg * lbo_a, p >= 0 ? src + kg * 8 : src, p >= 0 ? 16u : 0u);
+            }
+            // weights: one (tap, output channel) row per iteration
+            for (int pr = tid; pr < 9 * N; pr += kThreads) {
+                const int t = pr / N, n = pr - t * N;
+                const __nv_bfloat16 *src = a.wgt + ((size_t)t * N + n) * C + c0;
+                unsigned char *dst = sb + t * tap_bytes + n * 16;
+                for (int kg = 0; kg < KG; ++kg) tc::cp_async16(dst + kg * lbo_b, src + kg * 8, 16u);
+            }
+        }
+        tc::cp_async_commit();
+        const int c = s - (kConvStages - 1);
+        if (c < 0) {
+            if (__syncthreads_or(!ok)) failed = true;
+            continue;
+        }
+        tc::cp_async_wait<kConvStages - 1>();
+        tc::fence_proxy_async();
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        const int tl = c / chunks, chunk = c % chunks, slot = tl & 1, st = c % kConvStages;
+        if (tid == 0) {
+            const uint32_t sa = tc::smem_addr(smem_raw + st * stage_bytes), sb = sa + a_bytes;
+            tc::fence_after_sync();
+            for (int tap = 0; tap < 9; ++tap) {
+                int sy = tap / 3 - 1, sx = tap % 3 - 1;
+                if (a.flip) {
+                    sy = -sy;
+                    sx = -sx;
+                }
+                for (int jj = 0; jj < KG / 2; ++jj)
+                    tc::mma_bf16(tmem + slot * N,
+                                 tc::smem_desc(sa + (sy + 1) * region_bytes + 2 * jj * lbo_a + (sx + 1) * 16, lbo_a, 128),
+                                 tc::smem_desc(sb + tap * tap_bytes + 2 * jj * lbo_b, lbo_b, 128), idesc,
+                                 chunk > 0 || tap > 0 || jj > 0);
+            }
+            tc::mma_commit(tc::smem_addr(&bars[st]));
+            if (chunk == chunks - 1) tc::mma_commit(tc::smem_addr(&bars[kConvStages + slot]));
+        }
+        if (chunk == 0 && tl > 0 && !epilogue(tl - 1)) failed = true;
     }
+    if (!failed && my_tiles > 0 && !epilogue(my_tiles - 1)) failed = true;
     if (failed && tid == 0) atomicExch(a.err, 1);
     tc::cp_async_wait_all();
     tc::fence_before_sync();
@@ -356,16 +381,25 @@ void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const flo
     a.wd = w;
     a.C = C;
     a.N = N;
-    a.KC = C % 64 == 0 ? 64 : (C % 32 == 0 ? 32 : 16);
     a.flip = flip ? 1 : 0;
     a.relu = relu ? 1 : 0;
-    const size_t smem = (size_t)kStages * (kBM * a.KC * 2 + (size_t)N * a.KC * 2);
+    // largest channel chunk (64, 32 or 16, dividing C) whose stages fit
+    auto stage = [&](int kc) { return (size_t)kc * (3 * kHalo * 2 + 18 * (size_t)N); };
+    a.KC = 16;
+    for (int kc : {64, 32})
+        if (C % kc == 0 && kConvStages * stage(kc) <= 200 * 1024) {
+            a.KC = kc;
+            break;
+        }
+    const size_t smem = kConvStages * stage(a.KC);
     CRT_CHECK(smem <= 200 * 1024, CRT_ERR_INVALID, "conv3x3: tile does not fit shared memory");
     CRT_CUDA(cudaFuncSetAttribute(k_conv3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3x3, kThreads, smem));
-    per_sm = std::max(1, std::min(per_sm, 512 / host_tmem_cols(N)));
-    const int64_t tiles = (P + kBM - 1) / kBM;
+    per_sm = std::max(1, std::min(per_sm, 512 / host_tmem_cols(2 * N)));
+    const int64_t padded = (int64_t)(w + 2) * (nimg * (int64_t)(h + 1) + 1);
+    CRT_CHECK(padded < (1LL << 31) - 4 * kBM, CRT_ERR_INVALID, "conv3x3: image too large");
+    const int64_t tiles = ((int64_t)(w + 2) * (nimg * (int64_t)(h + 1) - 1) + kBM - 1) / kBM;
     const int grid = (int)std::min<int64_t>(tiles, (int64_t)sm_count() * per_sm);
     k_conv3x3<<<grid, kThreads, smem, s>>>(a);
     CRT_CUDA(cudaGetLastError());

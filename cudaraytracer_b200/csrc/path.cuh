@@ -144,7 +144,21 @@ __device__ inline StepResult path_step(const SceneView &s, const StepParams &sp,
     float b0 = rsub(rsub(1.f, h.b1), h.b2);
     V3 sn = normalized((b0 * V3{A0.x, A0.y, A0.z} + h.b1 * V3{A1.x, A1.y, A1.z}) + h.b2 * V3{A2.x, A2.y, A2.z});
     const DMesh &M = s.meshes[__float_as_int(A3.w)];
-    const DMaterial mat = s.materials[M.material];
+    DMaterial mat = s.materials[M.material];
+    if (mat.tex >= 0 && (mat.type == MAT_DIFFUSE || mat.type == MAT_PBR || mat.type == MAT_SUBSURFACE)) {
+        // Texture::Sample (texture.cu:243-252) at the interpolated texCoord
+        // (triangle.cu:128): u, v clamped to [0, 0.999999], v flipped; it
+        // replaces basecolor where the reference reads its diffuse texture
+        // (material.cu:70, 211, 246, 283, 336).
+        float tu = (b0 * A0.w + h.b1 * A2.w) + h.b2 * A3.y;
+        float tv = (b0 * A1.w + h.b1 * A3.x) + h.b2 * A3.z;
+        tu = fminf(fmaxf(tu, 0.0f), 0.999999f);
+        tv = fminf(fmaxf(tv, 0.0f), 0.999999f);
+        const float4 tc = tex2D<float4>(s.textures[mat.tex], tu, 1.0f - tv);
+        mat.base[0] = tc.x;
+        mat.base[1] = tc.y;
+        mat.base[2] = tc.z;
+    }
 
     V3 geomNormal = normalized(infoNormal);
     V3 hitNormal = (double)sqnorm(sn) > kEpsD ? normalized(sn) : geomNormal;

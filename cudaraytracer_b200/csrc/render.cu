@@ -38,6 +38,9 @@ RenderData::~RenderData() {
     if (env_vcdf) cudaFree(env_vcdf);
     if (env_row_alias) cudaFree(env_row_alias);
     if (env_col_alias) cudaFree(env_col_alias);
+    for (cudaTextureObject_t t : tex_objects) cudaDestroyTextureObject(t);
+    for (cudaArray_t a : tex_arrays) cudaFreeArray(a);
+    if (d_textures) cudaFree(d_textures);
 }
 
 template <class T>
@@ -106,6 +109,31 @@ void upload_render_data(const HostScene &hs, RenderData &rd) {
     rd.num_materials = (int)hs.materials.size();
     rd.num_lights = (int)hs.lights.size();
     rd.env_light = hs.env_light;
+    // Texture::Load (Src/Core/texture.cu:207-240): uchar4 array, wrap u,
+    // clamp v, linear filtering, normalised coordinates, [0, 255] -> [0, 1]
+    for (const HostTexture &t : hs.textures) {
+        cudaChannelFormatDesc cd = cudaCreateChannelDesc<uchar4>();
+        cudaArray_t arr = nullptr;
+        CRT_CUDA(cudaMallocArray(&arr, &cd, t.width, t.height));
+        rd.tex_arrays.push_back(arr);
+        CRT_CUDA(cudaMemcpy2DToArray(arr, 0, 0, t.rgba.data(), (size_t)t.width * 4, (size_t)t.width * 4, t.height,
+                                     cudaMemcpyHostToDevice));
+        cudaResourceDesc res;
+        std::memset(&res, 0, sizeof(res));
+        res.resType = cudaResourceTypeArray;
+        res.res.array.array = arr;
+        cudaTextureDesc td;
+        std::memset(&td, 0, sizeof(td));
+        td.addressMode[0] = cudaAddressModeWrap;
+        td.addressMode[1] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeNormalizedFloat;
+        td.normalizedCoords = 1;
+        cudaTextureObject_t obj = 0;
+        CRT_CUDA(cudaCreateTextureObject(&obj, &res, &td, nullptr));
+        rd.tex_objects.push_back(obj);
+    }
+    rd.d_textures = upload(rd.tex_objects);
     if (hs.env_light >= 0) {
         const int W = hs.env_w, H = hs.env_h;
         rd.env_w = W;
@@ -188,6 +216,7 @@ SceneView make_view(const BvhBuffers &bvh, const RenderData &rd) {
     s.env.vcdf = rd.env_vcdf;
     s.env.row_alias = rd.env_row_alias;
     s.env.col_alias = rd.env_col_alias;
+    s.textures = rd.d_textures;
     // Bounds3D::Center / DiagonalLength of the scene bounds (Src/Core/bounds.h:110-118).
     float e[3];
     for (int k = 0; k < 3; ++k) {

@@ -29,6 +29,10 @@ struct RenderData {
     float *env_ucdf = nullptr, *env_vcdf = nullptr;
     float2 *env_row_alias = nullptr, *env_col_alias = nullptr;
     int env_w = 0, env_h = 0;
+    // diffuse textures: uchar4 arrays behind normalised-float texture objects
+    std::vector<cudaArray_t> tex_arrays;
+    std::vector<cudaTextureObject_t> tex_objects;
+    cudaTextureObject_t *d_textures = nullptr;
     ~RenderData();
 };
 

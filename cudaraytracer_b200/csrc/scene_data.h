@@ -55,6 +55,13 @@ struct CameraState {
     float focal, ratio;
 };
 
+// A decoded diffuse texture: 8-bit RGBA, rows top-down.
+struct HostTexture {
+    std::string name;
+    int width = 0, height = 0;
+    std::vector<uint8_t> rgba;
+};
+
 struct HostScene {
     // camera block
     std::string camera_type = "pinhole";
@@ -75,6 +82,7 @@ struct HostScene {
     std::vector<DMaterial> materials;
     std::vector<std::string> material_names;
     std::vector<DLight> lights;
+    std::vector<HostTexture> textures;
     int env_light = -1;
     // environment map (RGBA float, top row first)
     int env_w = 0, env_h = 0;
@@ -86,6 +94,9 @@ struct HostScene {
 // (Src/Core/scene.cpp:129-252, :254-396, :398-537, :539-616; OBJ import
 // Src/Utils/objloader.cpp:66-210; HDR via the Radiance format).
 void load_scene_json(const std::string &path, HostScene &out);
+
+// Decodes a texture image file (PNG or binary PPM) to 8-bit RGBA (image.cpp).
+void load_texture_image(const std::string &path, HostTexture &out);
 
 // Triangle area and unit face normal exactly as Triangle::Triangle
 // (Src/Core/triangle.cu:3-10).

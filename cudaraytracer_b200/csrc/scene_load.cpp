@@ -654,8 +654,16 @@ void parse_materials(const Json &arr, HostScene &s, std::unordered_map<std::stri
             m.roughness = j.has("roughness") ? (float)j["roughness"].number("roughness") : 0.f;
             m.metallic = 0.f;
         }
-        if (j.has("diffuse_texture"))
-            s.warnings.push_back("diffuse textures are not loaded; material '" + j["name"].str + "' uses basecolor");
+        if (j.has("diffuse_texture")) {  // Src/Core/scene.cpp:380-386
+            const std::string tn = j["diffuse_texture"].string("diffuse_texture");
+            int found = -1;
+            for (size_t t = 0; t < s.textures.size(); ++t)
+                if (s.textures[t].name == tn) found = (int)t;
+            if (found >= 0)
+                m.tex = found;
+            else
+                s.warnings.push_back("texture '" + tn + "' not found for material '" + j["name"].str + "'");
+        }
         std::string name = j["name"].string("material.name");
         s.materials[i] = m;
         s.material_names[i] = name;
@@ -813,7 +821,23 @@ void load_scene_json(const std::string &path, HostScene &s) {
     parse_camera(root["camera"], s);
     std::unordered_map<std::string, int> mat_map, mesh_map;
     CRT_CHECK(root["textures"].kind == Json::ARR, CRT_ERR_PARSE, "'textures' should be an array");
-    if (!root["textures"].arr.empty()) s.warnings.push_back("textures are not loaded");
+    // ParseTextures (Src/Core/scene.cpp:618-644); an image that does not
+    // decode leaves its materials on their basecolor
+    for (const Json &tj : root["textures"].arr) {
+        if (!tj.has("path") || !tj.has("name")) {
+            s.warnings.push_back("texture missing 'path' or 'name'");
+            continue;
+        }
+        HostTexture t;
+        t.name = tj["name"].string("texture.name");
+        try {
+            load_texture_image(tj["path"].string("texture.path"), t);
+        } catch (const Error &e) {
+            s.warnings.push_back(std::string("texture '") + t.name + "' not loaded: " + e.what());
+            continue;
+        }
+        s.textures.push_back(std::move(t));
+    }
     parse_materials(root["materials"], s, mat_map);
     parse_objects(root["objects"], s, mat_map, mesh_map);
     parse_lights(root["lights"], s, mat_map, mesh_map);

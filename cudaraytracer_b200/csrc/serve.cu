@@ -223,6 +223,7 @@ size_t scene_device_bytes(const Scene &sc) {
     b += n * 64;                                              // shading attributes
     b += sc.host.meshes.size() * sizeof(DMesh) + sc.host.materials.size() * sizeof(DMaterial) +
          sc.host.lights.size() * sizeof(DLight);
+    for (const HostTexture &t : sc.host.textures) b += (size_t)t.width * t.height * 4;
     if (sc.host.env_light >= 0) {
         const size_t px = (size_t)sc.host.env_w * sc.host.env_h;
         b += px * 16 + px * 4 + (size_t)sc.host.env_h * 4 + (px + sc.host.env_h) * 8;  // texels, CDFs, alias tables

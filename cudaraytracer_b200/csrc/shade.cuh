@@ -37,6 +37,7 @@ struct SceneView {
     EnvView env;
     float center[3];
     float diag;
+    const cudaTextureObject_t *textures;  // DMaterial::tex indexes this
 };
 
 #ifdef __CUDACC__

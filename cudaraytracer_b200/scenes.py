@@ -63,6 +63,7 @@ class Mesh:
     name: str
     material: str
     tris: np.ndarray  # (n, 9) float32
+    uvs: np.ndarray | None = None  # (n, 6) float32 texture coordinates per corner
 
 
 @dataclass
@@ -75,6 +76,7 @@ class SceneSpec:
     camera: dict
     env: np.ndarray | None = None  # (H, W, 3) float32
     extra: dict = field(default_factory=dict)
+    textures: dict = field(default_factory=dict)  # name -> (h, w, 4) uint8 RGBA, top row first
 
     def triangles(self) -> np.ndarray:
         return np.concatenate([m.tris for m in self.meshes]).astype(np.float32)
@@ -87,8 +89,13 @@ class SceneSpec:
         objects = []
         for m in self.meshes:
             path = os.path.join(directory, f"{name}_{m.name}.obj")
-            write_obj(path, m.tris)
+            write_obj(path, m.tris, m.uvs)
             objects.append({"name": m.name, "path": path, "material": m.material})
+        textures = []
+        for tname, img in self.textures.items():
+            path = os.path.join(directory, f"{name}_tex_{tname}.png")
+            write_png(path, img)
+            textures.append({"name": tname, "path": path})
         lights = []
         for l in self.lights:
             l = dict(l)
@@ -99,7 +106,7 @@ class SceneSpec:
             lights.append(l)
         doc = {
             "camera": self.camera,
-            "textures": [],
+            "textures": textures,
             "materials": self.materials,
             "objects": objects,
             "lights": lights,
@@ -110,21 +117,84 @@ class SceneSpec:
         return jpath
 
 
-def write_obj(path: str, tris: np.ndarray) -> None:
+def write_obj(path: str, tris: np.ndarray, uvs: np.ndarray | None = None) -> None:
     """OBJ with one vertex per triangle corner, %.9g so floats round-trip
     exactly, no normals (the reference then uses face normals,
-    Src/Utils/objloader.cpp:192-198)."""
+    Src/Utils/objloader.cpp:192-198); texture coordinates (vt) when given."""
     t = np.asarray(tris, dtype=np.float32).reshape(-1, 3, 3)
     lines = []
     for tri in t:
         for v in tri:
             lines.append("v %.9g %.9g %.9g" % (float(v[0]), float(v[1]), float(v[2])))
     n = t.shape[0]
+    if uvs is not None:
+        u = np.asarray(uvs, dtype=np.float32).reshape(-1, 3, 2)
+        for tri in u:
+            for c in tri:
+                lines.append("vt %.9g %.9g" % (float(c[0]), float(c[1])))
     for i in range(n):
         b = 3 * i + 1
-        lines.append("f %d %d %d" % (b, b + 1, b + 2))
+        if uvs is not None:
+            lines.append("f %d/%d %d/%d %d/%d" % (b, b, b + 1, b + 1, b + 2, b + 2))
+        else:
+            lines.append("f %d %d %d" % (b, b + 1, b + 2))
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
+
+
+def write_png(path: str, rgba: np.ndarray) -> None:
+    """8-bit RGBA PNG, rows top-down; row filters cycle through the five PNG
+    filter types (None, Sub, Up, Average, Paeth) so a decoder meets all."""
+    import struct
+    import zlib
+
+    img = np.ascontiguousarray(rgba, dtype=np.uint8)
+    h, w, _ = img.shape
+    bpp = 4
+    rows = []
+    prev = np.zeros(w * 4, np.int32)
+    for y in range(h):
+        cur = img[y].reshape(-1).astype(np.int32)
+        ft = y % 5
+        a = np.concatenate([np.zeros(bpp, np.int32), cur[:-bpp]])
+        c = np.concatenate([np.zeros(bpp, np.int32), prev[:-bpp]])
+        if ft == 0:
+            f = cur
+        elif ft == 1:
+            f = cur - a
+        elif ft == 2:
+            f = cur - prev
+        elif ft == 3:
+            f = cur - ((a + prev) >> 1)
+        else:
+            p = a + prev - c
+            pa, pb, pc = np.abs(p - a), np.abs(p - prev), np.abs(p - c)
+            pr = np.where((pa <= pb) & (pa <= pc), a, np.where(pb <= pc, prev, c))
+            f = cur - pr
+        rows.append(bytes([ft]) + (f & 255).astype(np.uint8).tobytes())
+        prev = cur
+
+    def chunk(tag, body):
+        return struct.pack(">I", len(body)) + tag + body + struct.pack(">I", zlib.crc32(tag + body) & 0xFFFFFFFF)
+
+    raw = b"".join(rows)
+    with open(path, "wb") as f:
+        f.write(b"\x89PNG\r\n\x1a\n")
+        f.write(chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 6, 0, 0, 0)))
+        f.write(chunk(b"IDAT", zlib.compress(raw, 6)))
+        f.write(chunk(b"IEND", b""))
+
+
+def checker_texture(w=64, h=48, seed=0) -> np.ndarray:
+    """A seeded RGBA test texture: a coloured checkerboard over a gradient."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:h, 0:w]
+    cols = rng.integers(40, 230, size=(2, 3))
+    chk = ((xx // 8 + yy // 8) % 2).astype(np.int32)
+    img = np.zeros((h, w, 4), np.uint8)
+    img[..., :3] = np.clip(cols[chk] * (0.6 + 0.4 * xx[..., None] / max(1, w - 1)), 0, 255).astype(np.uint8)
+    img[..., 3] = 255
+    return img
 
 
 def write_hdr(path: str, img: np.ndarray) -> None:
@@ -166,11 +236,15 @@ GREEN = [0.14, 0.45, 0.09]
 LIGHT_KE = [17.0, 12.0, 4.0]
 
 
-def cornell_box(width=256, height=256, spp=16, max_bounces=8, rr=0.8, seed=None) -> SceneSpec:
+def cornell_box(width=256, height=256, spp=16, max_bounces=8, rr=0.8, seed=None, textured=False,
+                lights=1) -> SceneSpec:
     """The 36-triangle Cornell box. With a seed, a variant of it: box
     positions, sizes and rotations, wall colours and the light's size and
     emission drawn from ranges around the canonical values (the
-    denoiser's training and test scenes)."""
+    denoiser's training and test scenes). textured=True puts a diffuse
+    texture on the back wall (UVs spanning the wall) and a textured PBR
+    material on the boxes (planar UVs); lights=2 splits the ceiling light
+    into two area lights."""
     P = lambda x, y, z: (float(x), float(y), float(z))
     white, red, green = [], [], []
     wall_l, wall_r, ke = RED, GREEN, LIGHT_KE
@@ -190,24 +264,35 @@ def cornell_box(width=256, height=256, spp=16, max_bounces=8, rr=0.8, seed=None)
     # floor y=0 (+y), ceiling y=1 (-y), back z=0 (+z): CCW seen from inside
     white += _quad(P(0, 0, 0), P(0, 0, 1), P(1, 0, 1), P(1, 0, 0))
     white += _quad(P(0, 1, 0), P(1, 1, 0), P(1, 1, 1), P(0, 1, 1))
-    white += _quad(P(0, 0, 0), P(1, 0, 0), P(1, 1, 0), P(0, 1, 0))
+    back = _quad(P(0, 0, 0), P(1, 0, 0), P(1, 1, 0), P(0, 1, 0))
+    if not textured:
+        white += back
     red += _quad(P(0, 0, 0), P(0, 1, 0), P(0, 1, 1), P(0, 0, 1))  # x=0, +x
     green += _quad(P(1, 0, 0), P(1, 0, 1), P(1, 1, 1), P(1, 1, 0))  # x=1, -x
     boxes = _box(*b1)
     boxes += _box(*b2)
     h = 0.999
     lo, hi = 0.5 - half, 0.5 + half
-    light = _quad(P(lo, h, lo), P(hi, h, lo), P(hi, h, hi), P(lo, h, hi))
 
     def arr(t):
         return np.asarray(t, dtype=np.float32).reshape(-1, 9)
 
+    def planar_uv(t, ax_u, ax_v):
+        v = arr(t).reshape(-1, 3, 3)
+        return np.stack([v[:, :, ax_u], v[:, :, ax_v]], -1).reshape(-1, 6).astype(np.float32)
+
+    if lights == 2:  # two ceiling lights side by side, same material
+        mid = 0.5
+        light_meshes = [Mesh("light", "light", arr(_quad(P(lo, h, lo), P(mid - 0.02, h, lo), P(mid - 0.02, h, hi),
+                                                         P(lo, h, hi)))),
+                        Mesh("light_b", "light", arr(_quad(P(mid + 0.02, h, lo), P(hi, h, lo), P(hi, h, hi),
+                                                           P(mid + 0.02, h, hi))))]
+    else:
+        light_meshes = [Mesh("light", "light", arr(_quad(P(lo, h, lo), P(hi, h, lo), P(hi, h, hi), P(lo, h, hi))))]
     meshes = [
         Mesh("walls_white", "white", arr(white)),
         Mesh("wall_red", "red", arr(red)),
         Mesh("wall_green", "green", arr(green)),
-        Mesh("boxes", "white", arr(boxes)),
-        Mesh("light", "light", arr(light)),
     ]
     materials = [
         {"name": "white", "type": "diffuse", "basecolor": WHITE},
@@ -215,7 +300,21 @@ def cornell_box(width=256, height=256, spp=16, max_bounces=8, rr=0.8, seed=None)
         {"name": "green", "type": "diffuse", "basecolor": wall_r},
         {"name": "light", "type": "light", "emission": ke},
     ]
-    lights = [{"type": "area", "lightMeshName": "light", "material": "light"}]
+    textures = {}
+    if textured:
+        meshes.append(Mesh("wall_back", "checker", arr(back), planar_uv(back, 0, 1)))
+        meshes.append(Mesh("boxes", "pbr_tex", arr(boxes), planar_uv(boxes, 0, 1)))
+        materials.append({"name": "checker", "type": "diffuse", "basecolor": WHITE, "diffuse_texture": "checker"})
+        materials.append({"name": "pbr_tex", "type": "pbr", "basecolor": WHITE, "metallic": 0.3, "roughness": 0.45,
+                          "diffuse_texture": "stripes"})
+        textures["checker"] = checker_texture(64, 48, seed=1)
+        stripes = checker_texture(32, 32, seed=2)
+        stripes[:, ::4, :3] = 240
+        textures["stripes"] = stripes
+    else:
+        meshes.append(Mesh("boxes", "white", arr(boxes)))
+    meshes += light_meshes
+    lights = [{"type": "area", "lightMeshName": m.name, "material": "light"} for m in light_meshes]
     camera = {
         "type": "pinhole",
         "resolution": [width, height],
@@ -226,7 +325,7 @@ def cornell_box(width=256, height=256, spp=16, max_bounces=8, rr=0.8, seed=None)
         "direction": [0, 0, 1],
         "denoise": False,
     }
-    return SceneSpec(meshes, materials, lights, camera)
+    return SceneSpec(meshes, materials, lights, camera, textures=textures)
 
 
 # --------------------------------------------------------------------------

@@ -116,6 +116,8 @@ class Scene:
         mats = _lib.MaterialDesc * len(spec.materials)
         md = mats()
         index = {}
+        tex_names = list(getattr(spec, "textures", {}) or {})
+        tex_imgs = [np.ascontiguousarray(spec.textures[n], dtype=np.uint8) for n in tex_names]
         for i, m in enumerate(spec.materials):
             d = md[i]
             t = {"light": 0, "diffuse": 1, "pbr": 2, "dielectric": 3, "glass": 3, "subsurface": 4}[m["type"]]
@@ -145,9 +147,15 @@ class Scene:
             for k in range(3):
                 d.basecolor[k], d.emission[k], d.scatter_distance[k] = base[k], ke[k], scatter[k]
             d.roughness, d.metallic, d.transmission, d.ior = rough, metal, trans, ior
+            d.texture = tex_names.index(m["diffuse_texture"]) if m.get("diffuse_texture") in tex_names else -1
             index[m["name"]] = i
         tris = [np.ascontiguousarray(m.tris, dtype=np.float32).reshape(-1, 9) for m in spec.meshes]
         verts = np.ascontiguousarray(np.concatenate(tris))
+        uvs = None
+        if any(getattr(m, "uvs", None) is not None for m in spec.meshes):
+            uvs = np.ascontiguousarray(np.concatenate([
+                np.asarray(m.uvs, dtype=np.float32).reshape(-1, 6) if getattr(m, "uvs", None) is not None
+                else np.zeros((t.shape[0], 6), np.float32) for m, t in zip(spec.meshes, tris)]))
         meshes = (_lib.MeshDesc * len(tris))()
         first = 0
         mesh_index = {}
@@ -178,6 +186,15 @@ class Scene:
         d = _lib.SceneDesc()
         d.n_tris = verts.shape[0]
         d.verts = verts.ctypes.data
+        if uvs is not None:
+            d.uvs = uvs.ctypes.data
+        if tex_imgs:
+            tds = (_lib.TextureDesc * len(tex_imgs))()
+            for k, img in enumerate(tex_imgs):
+                tds[k].height, tds[k].width = img.shape[0], img.shape[1]
+                tds[k].rgba = img.ctypes.data
+            d.n_textures = len(tex_imgs)
+            d.textures = C.addressof(tds)
         d.n_meshes, d.n_materials, d.n_lights = len(tris), len(spec.materials), len(spec.lights)
         d.meshes = C.addressof(meshes)
         d.materials = C.addressof(md)
@@ -283,6 +300,24 @@ class Scene:
         _lib.call("crt_gbuffer_from_primary", self._h, C.byref(cam) if cam is not None else None, C.byref(gb),
                   C.c_void_p(s))
         return g
+
+    def gather(self, mode: int = 0, spp: int = 1, direct=None, indirect=None, gbuffer: dict | None = None,
+               denoised: bool = False, stream=None):
+        """GatherKernel: the display image (mode 0) or a debug view (1 depth,
+        2 normal, 3 mesh id, 4 position) as a CUDA uint8 tensor (H, W, 4)
+        in the reference's display-buffer layout."""
+        import torch
+
+        rp = self.render_params()
+        dev = torch.device("cuda", self.ctx.device)
+        out = torch.empty((rp["height"], rp["width"], 4), dtype=torch.uint8, device=dev)
+        gb = _gbuffer_struct(gbuffer) if gbuffer is not None else None
+        s = _torch_stream(dev, stream)
+        _lib.call("crt_gather", self._h, int(mode), int(spp), 1 if denoised else 0,
+                  direct.data_ptr() if direct is not None else None,
+                  indirect.data_ptr() if indirect is not None else None, C.byref(gb) if gb is not None else None,
+                  out.data_ptr(), C.c_void_p(s))
+        return out
 
     def render_svgf_frame(self, svgf: "Svgf", frame_index: int, out_direct, out_indirect, params=None,
                           stream=None) -> None:

@@ -127,7 +127,13 @@ typedef struct crt_material_desc {
     float roughness, metallic, transmission;
     float scatter_distance[3];
     float ior;
+    int32_t texture;             /* diffuse texture index, -1 = none */
 } crt_material_desc;
+
+typedef struct crt_texture_desc {
+    int32_t width, height;
+    const uint8_t *rgba;         /* width x height RGBA bytes, top row first (as decoded from the image file) */
+} crt_texture_desc;
 
 typedef struct crt_mesh_desc {
     int32_t material;            /* index into materials */
@@ -151,12 +157,21 @@ typedef struct crt_scene_desc {
     const crt_light_desc *lights;
     int32_t env_width, env_height;
     const float *env_rgba;       /* env_width x env_height RGBA floats, top row first */
+    int32_t n_textures;
+    const crt_texture_desc *textures;
     int32_t width, height, spp, max_bounces;  /* camera block (Src/Core/scene.cpp:187-252) */
     float rr, fovy;
     float direction[3];
 } crt_scene_desc;
 
 crt_status crt_scene_from_arrays(crt_ctx *ctx, const crt_scene_desc *desc, crt_scene **out);
+
+/* Decodes a texture image as the scene loader does (PNG: all colour types,
+ * 1-16 bit, non-interlaced; binary PPM) to 8-bit RGBA, top row first - the
+ * pixels the reference's Texture::Load gets from stbi_load with 4 channels
+ * (Src/Core/texture.cu:207-211). Host only. Call with rgba = NULL for the
+ * size, then again with a w*h*4-byte buffer. */
+crt_status crt_image_decode(const char *path, int32_t *w, int32_t *h, uint8_t *rgba);
 
 /* Loaded geometry in scene order (arrays sized by crt_scene_info):
  * verts n x 9, normals n x 9 (per vertex), uvs n x 6, prim_mesh n. Any
@@ -345,6 +360,16 @@ crt_status crt_denoise_params_default(crt_denoise_params *p);
  * camera, i.e. no motion). Replaces RenderGBuffer (renderer.cuh:1446-1503). */
 crt_status crt_gbuffer_from_primary(crt_scene *scene, const crt_camera *prev, const crt_gbuffer *out,
                                     void *stream);
+
+/* Display resolve and debug views (GatherKernel, Src/Core/renderer.cuh:956-1030)
+ * into width*height uchar4 device pixels (the scene's render resolution), in
+ * the reference's display-buffer layout: mode 0 colour ((direct + indirect)
+ * / spp, or the sum as is when `denoised`; gamma 1/2.2; vertically flipped
+ * rows), 1 linear depth, 2 shading normal, 3 mesh id colours, 4 position in
+ * the scene bounds (modes 1-4 from the G-buffer `gb`, which may be NULL for
+ * mode 0). Asynchronous on `stream`. */
+crt_status crt_gather(crt_scene *scene, int32_t mode, int32_t spp, int32_t denoised, const float *d_direct,
+                      const float *d_indirect, const crt_gbuffer *gb, void *d_pixels, void *stream);
 
 /* SVGF state (temporal history, moments, history lengths) for a w x h image. */
 crt_status crt_svgf_create(crt_ctx *ctx, int32_t width, int32_t height, crt_svgf **out);

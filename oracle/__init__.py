@@ -41,6 +41,7 @@ class _OracleSceneC(C.Structure):
         ("cam_pos", C.c_float * 3), ("cam_ld", C.c_float * 3), ("cam_du", C.c_float * 3), ("cam_dv", C.c_float * 3),
         ("width", C.c_int), ("height", C.c_int), ("max_bounces", C.c_int), ("rr", C.c_float),
         ("rr_start", C.c_int), ("seed", C.c_ulonglong),
+        ("ntex", C.c_int), ("tex", _VP), ("tex_w", _VP), ("tex_h", _VP),
     ]
 
 
@@ -82,6 +83,16 @@ def render(scene, camera, spp: int, first_sample: int = 0, seed: int = 1, max_bo
     o.rr = float(scene.rr if rr is None else rr)
     o.rr_start = rr_start
     o.seed = seed
+    texs = [np.ascontiguousarray(t, dtype=np.uint8) for t in getattr(scene, "textures", [])]
+    if texs:
+        keep.extend(texs)
+        ptrs = (C.c_void_p * len(texs))(*[t.ctypes.data for t in texs])
+        tw = np.array([t.shape[1] for t in texs], np.int32)
+        th = np.array([t.shape[0] for t in texs], np.int32)
+        keep.extend([ptrs, tw, th])
+        o.ntex = len(texs)
+        o.tex = C.addressof(ptrs)
+        o.tex_w, o.tex_h = tw.ctypes.data, th.ctypes.data
     d = np.zeros((h, w, 4), np.float32)
     i = np.zeros((h, w, 4), np.float32)
     q = np.zeros((h, w, 4), np.float32)

@@ -39,6 +39,10 @@ typedef struct oracle_scene {
     float rr;
     int rr_start;
     unsigned long long seed;
+    /* diffuse textures: RGBA bytes, top row first (material entry 14 = index) */
+    int ntex;
+    const unsigned char *const *tex;
+    const int *tex_w, *tex_h;
 } oracle_scene;
 
 /* Path-traces samples [first_sample, first_sample + spp) of every pixel and

@@ -87,6 +87,26 @@ typedef struct {
     float ior;
 } mat_t;
 
+/* tex2D<float4> of a uchar4 texture read as normalised float (byte / 255),
+ * linear filtering with 8-bit fractional weights, wrap u / clamp v. */
+static vec tex_fetch(const ctx_t *c, int t, float u, float v) {
+    int W = c->s->tex_w[t], H = c->s->tex_h[t];
+    const unsigned char *e = c->s->tex[t];
+    float x = (u - floorf(u)) * W, y = v * H;
+    float xb = x - 0.5f, yb = y - 0.5f;
+    int i = (int)floorf(xb), j = (int)floorf(yb);
+    float a = floorf((xb - i) * 256.f + 0.5f) / 256.f, b = floorf((yb - j) * 256.f + 0.5f) / 256.f;
+    int i0 = ((i % W) + W) % W, i1 = (((i + 1) % W) + W) % W;
+    int j0 = j < 0 ? 0 : (j >= H ? H - 1 : j), j1 = j + 1 < 0 ? 0 : (j + 1 >= H ? H - 1 : j + 1);
+    const unsigned char *t00 = e + 4 * ((size_t)j0 * W + i0), *t10 = e + 4 * ((size_t)j0 * W + i1);
+    const unsigned char *t01 = e + 4 * ((size_t)j1 * W + i0), *t11 = e + 4 * ((size_t)j1 * W + i1);
+    float r[3];
+    for (int k = 0; k < 3; ++k)
+        r[k] = (1 - a) * (1 - b) * (t00[k] / 255.f) + a * (1 - b) * (t10[k] / 255.f) + (1 - a) * b * (t01[k] / 255.f) +
+               a * b * (t11[k] / 255.f);
+    return V(r[0], r[1], r[2]);
+}
+
 static mat_t get_mat(const ctx_t *c, int i) {
     const float *m = c->s->materials + 16 * i;
     mat_t r;
@@ -531,6 +551,17 @@ static int path_step(const ctx_t *c, int bounce, path_t *ps, hit_t h) {
     vec sn = vnorm(vadd(vadd(vs(L3(nn), b0), vs(L3(nn + 3), h.b1)), vs(L3(nn + 6), h.b2)));
     const float *M = s->meshes + 8 * s->prim_mesh[prim];
     mat_t mat = get_mat(c, (int)M[0]);
+    {   /* diffuse texture (Texture::Sample, texture.cu:243-252): clamped uv, v flipped */
+        int ti = (int)s->materials[16 * (int)M[0] + 14];
+        if (ti >= 0 && ti < s->ntex && (mat.type == M_DIFFUSE || mat.type == M_PBR || mat.type == M_SUBSURFACE)) {
+            const float *uv = s->uvs + 6 * (size_t)prim;
+            float tu = (b0 * uv[0] + h.b1 * uv[2]) + h.b2 * uv[4];
+            float tv = (b0 * uv[1] + h.b1 * uv[3]) + h.b2 * uv[5];
+            tu = tu < 0.f ? 0.f : (tu > 0.999999f ? 0.999999f : tu);
+            tv = tv < 0.f ? 0.f : (tv > 0.999999f ? 0.999999f : tv);
+            mat.base = tex_fetch(c, ti, tu, 1.0f - tv);
+        }
+    }
     int mesh_light = (int)M[1];
 
     vec geomNormal = vnorm(infoNormal);

@@ -41,6 +41,7 @@ class OracleScene:
     mesh_names: list = field(default_factory=list)
     env_light: int = -1
     env: np.ndarray = None        # (H, W, 4) float32
+    textures: list = field(default_factory=list)  # (h, w, 4) uint8 RGBA, top row first
 
 
 def _f32cross(a, b):
@@ -174,6 +175,65 @@ def triangle_areas(v: np.ndarray) -> np.ndarray:
     return (F(0.5) * np.sqrt(_f32dot(c, c))).astype(F)
 
 
+def read_png(path: str) -> np.ndarray:
+    """(h, w, 4) uint8 RGBA of an 8-bit non-interlaced PNG (grey, RGB, RGBA,
+    grey+alpha), rows top-down: the CPU check of the library's decoder."""
+    import struct
+    import zlib
+
+    data = open(path, "rb").read()
+    if data[:8] != b"\x89PNG\r\n\x1a\n":
+        raise ValueError("not a PNG")
+    pos, idat, hdr = 8, b"", None
+    while pos < len(data):
+        ln, typ = struct.unpack(">I4s", data[pos:pos + 8])
+        body = data[pos + 8:pos + 8 + ln]
+        if typ == b"IHDR":
+            hdr = struct.unpack(">IIBBBBB", body)
+        elif typ == b"IDAT":
+            idat += body
+        elif typ == b"IEND":
+            break
+        pos += 12 + ln
+    w, h, depth, ctype, _, _, inter = hdr
+    if depth != 8 or inter or ctype not in (0, 2, 4, 6):
+        raise ValueError("unsupported PNG")
+    ch = {0: 1, 2: 3, 4: 2, 6: 4}[ctype]
+    raw = np.frombuffer(zlib.decompress(idat), np.uint8).reshape(h, 1 + w * ch)
+    img = np.zeros((h, w * ch), np.int32)
+    for y in range(h):
+        f, row = raw[y, 0], raw[y, 1:].astype(np.int32)
+        prev = img[y - 1] if y else np.zeros(w * ch, np.int32)
+        out = np.zeros(w * ch, np.int32)
+        for x in range(w * ch):
+            a = out[x - ch] if x >= ch else 0
+            b = prev[x]
+            c = prev[x - ch] if x >= ch else 0
+            if f == 0:
+                pr = 0
+            elif f == 1:
+                pr = a
+            elif f == 2:
+                pr = b
+            elif f == 3:
+                pr = (a + b) >> 1
+            else:
+                pp = a + b - c
+                pa, pb, pc = abs(pp - a), abs(pp - b), abs(pp - c)
+                pr = a if (pa <= pb and pa <= pc) else (b if pb <= pc else c)
+            out[x] = (row[x] + pr) & 255
+        img[y] = out
+    img = img.reshape(h, w, ch).astype(np.uint8)
+    rgba = np.full((h, w, 4), 255, np.uint8)
+    if ch in (1, 2):
+        rgba[..., :3] = img[..., :1]
+        if ch == 2:
+            rgba[..., 3] = img[..., 1]
+    else:
+        rgba[..., :ch] = img
+    return rgba
+
+
 def load_scene(path: str) -> OracleScene:
     doc = json.load(open(path))
     s = OracleScene()
@@ -187,6 +247,16 @@ def load_scene(path: str) -> OracleScene:
     s.spp = int(cam.get("spp", 16))
     s.direction = tuple(float(F(x)) for x in cam.get("direction", [0, 0, -1]))
     s.denoise = bool(cam.get("denoise", False))
+    tex_map = {}
+    for tj in doc.get("textures", []):
+        if "path" not in tj or "name" not in tj:
+            continue
+        try:
+            img = read_png(tj["path"])
+        except (OSError, ValueError):
+            continue
+        tex_map[tj["name"]] = len(s.textures)
+        s.textures.append(img)
     mats = np.zeros((len(doc["materials"]), 16), F)
     mats[:, 0] = 1
     mats[:, 7] = 0.5
@@ -220,6 +290,8 @@ def load_scene(path: str) -> OracleScene:
             row[9] = m.get("transmission", 1.0)
             row[7] = m.get("roughness", 0.0)
             row[8] = 0
+        if "diffuse_texture" in m and m["diffuse_texture"] in tex_map:
+            row[14] = tex_map[m["diffuse_texture"]]
         mat_map[m["name"]] = i
     s.materials = mats
     verts, normals, uvs, pm, meshes, names = [], [], [], [], [], []

@@ -5,7 +5,7 @@ prebuilt oracle/_ref libraries; writes to the directory given (default
 tests/golden). Each scene renders in a fresh process because the reference
 keeps its scene in process-global state.
 
-    python tests/golden/make_render_golden.py [outdir]
+    python tests/golden/make_render_golden.py [outdir [scene ...]]
 """
 from __future__ import annotations
 
@@ -24,6 +24,8 @@ SCENES = {
     "cornell": ("cornell_box", dict(width=128, height=128, max_bounces=8), 4096),
     "icospheres": ("icosphere_field", dict(n_spheres=8, level=2, width=64, height=64, env_size=(256, 128),
                                            max_bounces=6, sun_peak=40.0, sun_sigma=0.1), 16384),
+    # diffuse textures (PNG, on a diffuse and a PBR material) and two area lights
+    "cornell_tex2": ("cornell_box", dict(width=96, height=96, max_bounces=8, textured=True, lights=2), 4096),
 }
 
 
@@ -50,5 +52,5 @@ if __name__ == "__main__":
     else:
         out = sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__))
         os.makedirs(out, exist_ok=True)
-        for name in SCENES:
+        for name in (sys.argv[2:] or list(SCENES)):
             subprocess.run([sys.executable, os.path.abspath(__file__), "--one", name, out], check=True)

@@ -128,3 +128,31 @@ def test_max_bounces_and_survivor_drop(crt_ctx, cornell_json):
     np.testing.assert_array_equal(q[..., 3], oq[..., 3])
     assert np.abs(i).max() == 0.0
     compare(d, od, 1e-5, 0.001)
+
+
+@pytest.fixture(scope="module")
+def textured_json(tmp_path_factory):
+    d = tmp_path_factory.mktemp("tex")
+    return scenes.cornell_box(width=48, height=48, spp=4, max_bounces=6, textured=True, lights=2).write(str(d), "ct")
+
+
+def test_textured_two_light_render_matches_oracle(crt_ctx, textured_json):
+    """Diffuse textures (PNG decoded by the library; by a separate Python
+    decoder for the oracle) on a diffuse and a PBR material, two area lights
+    (uniform light selection). Texels are filtered by the texture unit on the
+    GPU and by an emulation of its 8-bit weights in the oracle."""
+    sc = Scene.load(crt_ctx, textured_json)
+    ref = osc.load_scene(textured_json)
+    assert len(ref.textures) == 2 and sc.info()["num_lights"] == 2
+    m, _, _ = sc.export_tables()
+    np.testing.assert_array_equal(m, ref.materials)
+    assert sorted(m[:, 14].tolist()) == [-1, -1, -1, -1, 0, 1]
+    sc.set_render_params(seed=11)
+    d, i = sc.render(4)
+    od, oi, _ = oracle.render(ref, cam_vectors(sc), spp=4, seed=11)
+    assert np.isfinite(d).all() and np.isfinite(i).all()
+    compare(d, od, 2e-2, 0.03)
+    compare(i, oi, 2e-2, 0.05)
+    # the textures show: the back wall is not uniform
+    back = (d + i)[..., :3][24:40, 16:32].reshape(-1, 3)
+    assert back.std(0).max() > 0.02

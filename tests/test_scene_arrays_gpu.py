@@ -11,6 +11,7 @@ SPECS = {
     "cornell": lambda: scenes.cornell_box(width=40, height=40, max_bounces=5),
     "icospheres": lambda: scenes.icosphere_field(n_spheres=10, level=2, width=36, height=28, max_bounces=8,
                                                  env_size=(96, 48), sun_peak=40.0, sun_sigma=0.1),
+    "cornell_tex2": lambda: scenes.cornell_box(width=32, height=32, max_bounces=5, textured=True, lights=2),
 }
 
 
