@@ -51,7 +51,6 @@ __device__ __forceinline__ uint32_t tmem_cols(int n) {
 }
 
 constexpr int kHalo = kBM + 2;  // rows of one halo region
-constexpr int kConvStages = 3;
 
 // Position q of the padded linear image space (rows of W + 2: columns W and
 // W + 1 are zero padding, column W + 1 doubling as column -1 of the next
@@ -78,6 +77,9 @@ __device__ __forceinline__ int padded_to_pixel(int q, int W, int H, int NR) {
 // starts dx + 1 rows (16 B each) into region dy + 1: no per-tap gather. Two
 // TMEM accumulator slots let a tile's epilogue overlap the first MMAs of
 // the next tile.
+// kResident: the layer's weights (all taps, all channel chunks) are loaded
+// into shared memory once per CTA; stages then hold only halo regions.
+template <int kConvStages, bool kResident>
 __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ uint64_t bars[kConvStages + 2];
@@ -90,7 +92,10 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
     const int chunks = C / KC, KG = KC / 8;
     const uint32_t lbo_a = kHalo * 16, region_bytes = KG * lbo_a, a_bytes = 3 * region_bytes;
     const uint32_t lbo_b = (uint32_t)N * 16, tap_bytes = KG * lbo_b, b_bytes = 9 * tap_bytes;
-    const uint32_t stage_bytes = a_bytes + b_bytes;
+    const uint32_t stage_bytes = kResident ? a_bytes : a_bytes + b_bytes;
+    // resident weights: [chunk][tap][k group][n], then the stages
+    unsigned char *const wres = smem_raw;
+    unsigned char *const stages = smem_raw + (kResident ? (size_t)chunks * b_bytes : 0);
     const uint32_t idesc = tc::idesc_bf16(kBM, N, false, false);
     const uint32_t ncols = tmem_cols(2 * N);
     const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
@@ -106,6 +111,18 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
     bool failed = false;
+    if (kResident) {
+        for (int pr = tid; pr < chunks * 9 * N; pr += kThreads) {
+            const int ch = pr / (9 * N), rest = pr - ch * 9 * N, t = rest / N, n = rest - t * N;
+            const __nv_bfloat16 *src = a.wgt + ((size_t)t * N + n) * C + ch * KC;
+            unsigned char *dst = wres + ch * b_bytes + t * tap_bytes + n * 16;
+            for (int kg = 0; kg < KG; ++kg) tc::cp_async16(dst + kg * lbo_b, src + kg * 8, 16u);
+        }
+        tc::cp_async_commit();
+        tc::cp_async_wait_all();
+        tc::fence_proxy_async();
+        __syncthreads();
+    }
 
     // epilogue of tile-local index tl: accumulators -> bias / ReLU / mask -> NHWC
     auto epilogue = [&](int tl) -> bool {
@@ -154,7 +171,7 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
         if (s < total) {
             const int st = s % kConvStages;
             if (s >= kConvStages) ok = tc::mbar_wait(&bars[st], ((s / kConvStages) - 1) & 1);
-            unsigned char *sa = smem_raw + st * stage_bytes, *sb = sa + a_bytes;
+            unsigned char *sa = stages + st * stage_bytes, *sb = sa + a_bytes;
             const int tile = blockIdx.x + (s / chunks) * gridDim.x, c0 = (s % chunks) * KC;
             const int t0 = qbeg + tile * kBM;
             // halo: one pixel per (region, row), its KC channels as KG vectors
@@ -167,7 +184,7 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
                     tc::cp_async16(dst + kg * lbo_a, p >= 0 ? src + kg * 8 : src, p >= 0 ? 16u : 0u);
             }
             // weights: one (tap, output channel) row per iteration
-            for (int pr = tid; pr < 9 * N; pr += kThreads) {
+            for (int pr = tid; pr < (kResident ? 0 : 9 * N); pr += kThreads) {
                 const int t = pr / N, n = pr - t * N;
                 const __nv_bfloat16 *src = a.wgt + ((size_t)t * N + n) * C + c0;
                 unsigned char *dst = sb + t * tap_bytes + n * 16;
@@ -188,7 +205,8 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
         }
         const int tl = c / chunks, chunk = c % chunks, slot = tl & 1, st = c % kConvStages;
         if (tid == 0) {
-            const uint32_t sa = tc::smem_addr(smem_raw + st * stage_bytes), sb = sa + a_bytes;
+            const uint32_t sa = tc::smem_addr(stages + st * stage_bytes);
+            const uint32_t sb = kResident ? tc::smem_addr(wres + chunk * b_bytes) : sa + a_bytes;
             tc::fence_after_sync();
             for (int tap = 0; tap < 9; ++tap) {
                 int sy = tap / 3 - 1, sx = tap % 3 - 1;
@@ -383,25 +401,41 @@ void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const flo
     a.N = N;
     a.flip = flip ? 1 : 0;
     a.relu = relu ? 1 : 0;
-    // largest channel chunk (64, 32 or 16, dividing C) whose stages fit
-    auto stage = [&](int kc) { return (size_t)kc * (3 * kHalo * 2 + 18 * (size_t)N); };
-    a.KC = 16;
-    for (int kc : {64, 32})
-        if (C % kc == 0 && kConvStages * stage(kc) <= 200 * 1024) {
+    // Weights resident in shared memory when they fit next to 5 halo
+    // stages, else streamed per stage with 3 stages; the channel chunk KC is
+    // the largest of 64, 32, 16 dividing C that fits.
+    const size_t kSmemCap = 220 * 1024;
+    const size_t wbytes = (size_t)9 * N * C * 2;
+    auto a_stage = [&](int kc) { return (size_t)kc * 3 * kHalo * 2; };
+    bool resident = false;
+    a.KC = 0;
+    for (int kc : {64, 32, 16})
+        if (C % kc == 0 && wbytes + 5 * a_stage(kc) <= kSmemCap) {
             a.KC = kc;
+            resident = true;
             break;
         }
-    const size_t smem = kConvStages * stage(a.KC);
-    CRT_CHECK(smem <= 200 * 1024, CRT_ERR_INVALID, "conv3x3: tile does not fit shared memory");
-    CRT_CUDA(cudaFuncSetAttribute(k_conv3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (!resident)
+        for (int kc : {64, 32, 16})
+            if (C % kc == 0 && 3 * (a_stage(kc) + (size_t)18 * N * kc) <= kSmemCap) {
+                a.KC = kc;
+                break;
+            }
+    CRT_CHECK(a.KC > 0, CRT_ERR_INVALID, "conv3x3: tile does not fit shared memory");
+    const size_t smem = resident ? wbytes + 5 * a_stage(a.KC) : 3 * (a_stage(a.KC) + (size_t)18 * N * a.KC);
+    const void *kfn = resident ? (const void *)k_conv3x3<5, true> : (const void *)k_conv3x3<3, false>;
+    CRT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3x3, kThreads, smem));
+    CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem));
     per_sm = std::max(1, std::min(per_sm, 512 / host_tmem_cols(2 * N)));
     const int64_t padded = (int64_t)(w + 2) * (nimg * (int64_t)(h + 1) + 1);
     CRT_CHECK(padded < (1LL << 31) - 4 * kBM, CRT_ERR_INVALID, "conv3x3: image too large");
     const int64_t tiles = ((int64_t)(w + 2) * (nimg * (int64_t)(h + 1) - 1) + kBM - 1) / kBM;
     const int grid = (int)std::min<int64_t>(tiles, (int64_t)sm_count() * per_sm);
-    k_conv3x3<<<grid, kThreads, smem, s>>>(a);
+    if (resident)
+        k_conv3x3<5, true><<<grid, kThreads, smem, s>>>(a);
+    else
+        k_conv3x3<3, false><<<grid, kThreads, smem, s>>>(a);
     CRT_CUDA(cudaGetLastError());
 }
 
