@@ -28,7 +28,8 @@ namespace crt {
 namespace {
 
 constexpr int kBM = 128;      // pixels (or (tap, c) rows) per tile
-constexpr int kThreads = 128;
+constexpr int kThreads = 128;      // weight-gradient kernel
+constexpr int kConvThreads = 256;  // forward / data-gradient kernel: two warps per TMEM lane quarter
 constexpr int kStages = 4;
 constexpr int kWgradBK = 64;  // pixels per weight-gradient K step
 
@@ -80,7 +81,7 @@ __device__ __forceinline__ int padded_to_pixel(int q, int W, int H, int NR) {
 // kResident: the layer's weights (all taps, all channel chunks) are loaded
 // into shared memory once per CTA; stages then hold only halo regions.
 template <int kConvStages, bool kResident>
-__global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
+__global__ void __launch_bounds__(kConvThreads) k_conv3x3(ConvArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ uint64_t bars[kConvStages + 2];
     __shared__ uint32_t tmem_slot;
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
     const uint32_t tmem = tmem_slot;
     bool failed = false;
     if (kResident) {
-        for (int pr = tid; pr < chunks * 9 * N; pr += kThreads) {
+        for (int pr = tid; pr < chunks * 9 * N; pr += kConvThreads) {
             const int ch = pr / (9 * N), rest = pr - ch * 9 * N, t = rest / N, n = rest - t * N;
             const __nv_bfloat16 *src = a.wgt + ((size_t)t * N + n) * C + ch * KC;
             unsigned char *dst = wres + ch * b_bytes + t * tap_bytes + n * 16;
@@ -131,9 +132,14 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
         if (__syncthreads_or(!ok)) return false;
         tc::fence_after_sync();
         const int tile = blockIdx.x + tl * gridDim.x;
-        const int64_t p = padded_to_pixel(qbeg + tile * kBM + tid, W, H, NR);
-        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + slot * N;
-        for (int n0 = 0; n0 < N; n0 += 16) {
+        // warp w reads TMEM lanes 32 (w % 4) .. +31 (one pixel per thread);
+        // the warp groups (w / 4) split the 16-column groups between them
+        constexpr int kGroups = kConvThreads / 128;
+        const int64_t p = padded_to_pixel(qbeg + tile * kBM + (tid & 127), W, H, NR);
+        const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16) + slot * N;
+        const int per = (N / 16 + kGroups - 1) / kGroups * 16, grp = warp >> 2;
+        const int nbeg = min(N, grp * per), nend = min(N, nbeg + per);
+        for (int n0 = nbeg; n0 < nend; n0 += 16) {
             float v[16];
             tc::tmem_ld16(lane_base + n0, v);
             if (p < 0) continue;
@@ -175,7 +181,7 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
             const int tile = blockIdx.x + (s / chunks) * gridDim.x, c0 = (s % chunks) * KC;
             const int t0 = qbeg + tile * kBM;
             // halo: one pixel per (region, row), its KC channels as KG vectors
-            for (int pr = tid; pr < 3 * kHalo; pr += kThreads) {
+            for (int pr = tid; pr < 3 * kHalo; pr += kConvThreads) {
                 const int r = pr / kHalo, j = pr - r * kHalo;
                 const int p = padded_to_pixel(t0 + (r - 1) * Wp + j - 1, W, H, NR);
                 const __nv_bfloat16 *src = p >= 0 ? a.in + (size_t)p * C + c0 : a.in;
@@ -184,7 +190,7 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3(ConvArgs a) {
                     tc::cp_async16(dst + kg * lbo_a, p >= 0 ? src + kg * 8 : src, p >= 0 ? 16u : 0u);
             }
             // weights: one (tap, output channel) row per iteration
-            for (int pr = tid; pr < (kResident ? 0 : 9 * N); pr += kThreads) {
+            for (int pr = tid; pr < (kResident ? 0 : 9 * N); pr += kConvThreads) {
                 const int t = pr / N, n = pr - t * N;
                 const __nv_bfloat16 *src = a.wgt + ((size_t)t * N + n) * C + c0;
                 unsigned char *dst = sb + t * tap_bytes + n * 16;
@@ -426,16 +432,16 @@ void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const flo
     const void *kfn = resident ? (const void *)k_conv3x3<5, true> : (const void *)k_conv3x3<3, false>;
     CRT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem));
+    CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kConvThreads, smem));
     per_sm = std::max(1, std::min(per_sm, 512 / host_tmem_cols(2 * N)));
     const int64_t padded = (int64_t)(w + 2) * (nimg * (int64_t)(h + 1) + 1);
     CRT_CHECK(padded < (1LL << 31) - 4 * kBM, CRT_ERR_INVALID, "conv3x3: image too large");
     const int64_t tiles = ((int64_t)(w + 2) * (nimg * (int64_t)(h + 1) - 1) + kBM - 1) / kBM;
     const int grid = (int)std::min<int64_t>(tiles, (int64_t)sm_count() * per_sm);
     if (resident)
-        k_conv3x3<5, true><<<grid, kThreads, smem, s>>>(a);
+        k_conv3x3<5, true><<<grid, kConvThreads, smem, s>>>(a);
     else
-        k_conv3x3<3, false><<<grid, kThreads, smem, s>>>(a);
+        k_conv3x3<3, false><<<grid, kConvThreads, smem, s>>>(a);
     CRT_CUDA(cudaGetLastError());
 }
 
