@@ -8,14 +8,16 @@
 //   forward : out[p, n] = sum_{t, c} in[p + off(t), c] * w[t][n][c]
 //   data grad: out[p, n] = sum_{t, c} g[p - off(t), c] * wt[t][n][c]
 //             (wt = w transposed per tap, flip = 1)
-// The A tile is gathered per tap with 16 B cp.async copies (zero-filled
-// outside the image) into the K-major core-matrix layout of tc.cuh; B is the
-// tap's weight slice. A 4-stage pipeline overlaps the copies of later steps
-// with the MMAs of earlier ones: one thread issues the MMAs of a step and
-// commits them to the stage's mbarrier, which frees the stage for reuse.
-// The epilogue reads the FP32 accumulators from TMEM (one pixel per thread)
-// and applies bias + ReLU (forward) or the ReLU mask of the layer below
-// (data gradient), writing BF16 (or FP32) NHWC.
+// The input is staged per (tile, channel chunk) as three halo regions with
+// 16 B cp.async copies (zero-filled outside the image) in the K-major
+// core-matrix layout of tc.cuh; every tap's A operand is a shifted
+// descriptor into them, B the tap's weight slice (resident in shared memory
+// when the layer's weights fit). Producer warps, one MMA-issuing thread and
+// epilogue warps hand stages and the two TMEM accumulator slots to each
+// other through mbarriers, so copies, MMAs and the epilogue of the previous
+// tile overlap. The epilogue reads the FP32 accumulators from TMEM (one
+// pixel per thread) and applies bias + ReLU (forward) or the ReLU mask of
+// the layer below (data gradient), writing BF16 (or FP32) NHWC.
 //
 // The weight gradient is a second kernel: rows M = (tap, c) (9C rows in
 // 128-row tiles), columns N = output channels, K = pixels split across
@@ -29,7 +31,7 @@ namespace {
 
 constexpr int kBM = 128;      // pixels (or (tap, c) rows) per tile
 constexpr int kThreads = 128;      // weight-gradient kernel
-constexpr int kConvThreads = 256;  // forward / data-gradient kernel: two warps per TMEM lane quarter
+constexpr int kConvThreads = 288;  // forward / data-gradient kernel: 4 producer, 4 epilogue, 1 MMA warp
 constexpr int kStages = 4;
 constexpr int kWgradBK = 64;  // pixels per weight-gradient K step
 
@@ -73,170 +75,211 @@ __device__ __forceinline__ int padded_to_pixel(int q, int W, int H, int NR) {
 
 // One CTA walks its tiles of 128 consecutive padded positions. Per tile and
 // channel chunk of KC, a stage holds three halo regions (input rows shifted
-// by -1, 0, +1; 130 positions each: the tile plus one on either side) and the
-// chunk of all 9 taps' weights. Tap (dy, dx) is then the MMA whose A operand
-// starts dx + 1 rows (16 B each) into region dy + 1: no per-tap gather. Two
-// TMEM accumulator slots let a tile's epilogue overlap the first MMAs of
-// the next tile.
+// by -1, 0, +1; 130 positions each: the tile plus one on either side) and,
+// unless the weights are resident, the chunk of all 9 taps' weights. Tap
+// (dy, dx) is then the MMA whose A operand starts dx + 1 rows (16 B each)
+// into region dy + 1: no per-tap gather.
+// Warp roles (no block-wide barrier inside the tile loop):
+//   warps 0-3  producers: cp.async the halo (and streamed weights) of step s
+//              into stage s % kS; once a step's copies have landed they
+//              make them visible to the tensor core (proxy fence) and
+//              arrive on full[stage]. kS - 2 steps stay in flight.
+//   warp 8     one thread issues the step's 9 taps x KC/16 MMAs into one of
+//              two TMEM accumulator slots and commits them to empty[stage]
+//              (the stage may be refilled) and, after a tile's last chunk,
+//              to tfull[slot].
+//   warps 4-7  epilogue: TMEM lane quarter (warp % 4), one pixel per thread:
+//              bias / ReLU / mask, BF16 or FP32 NHWC stores; then arrive on
+//              tempty[slot] so the MMAs of tile + 2 may overwrite the slot.
+// Every wait is bounded and also ends when another role has given up.
 // kResident: the layer's weights (all taps, all channel chunks) are loaded
 // into shared memory once per CTA; stages then hold only halo regions.
-template <int kConvStages, bool kResident>
-__global__ void __launch_bounds__(kConvThreads) k_conv3x3(ConvArgs a) {
+template <int kS, bool kResident>
+__global__ void __launch_bounds__(kConvThreads, 1) k_conv3x3(ConvArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ uint64_t bars[kConvStages + 2];
+    __shared__ uint64_t full[kS], empty[kS], tfull[2], tempty[2], mma_done;
     __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag;
+    __shared__ int hpix[3 * kHalo];  // pixel index (or -1) of each halo row of the producers' tile
+    __shared__ float sbias[256];
+    constexpr int kLag = kS - 2;     // producer steps in flight before a step is signalled
+    constexpr int kProd = 128, kEpi0 = 4, kMmaWarp = 8;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int C = a.C, N = a.N, KC = a.KC, W = a.wd, H = a.h;
     const int Wp = W + 2, NR = a.nimg * (H + 1) + 1;
     const int qbeg = Wp, qend = Wp * (NR - 1);
     const int ntiles = (qend - qbeg + kBM - 1) / kBM;
-    const int chunks = C / KC, KG = KC / 8;
+    const int chunks = C / KC, KG = KC / 8, kg_shift = KG == 8 ? 3 : KG == 4 ? 2 : 1;
     const uint32_t lbo_a = kHalo * 16, region_bytes = KG * lbo_a, a_bytes = 3 * region_bytes;
     const uint32_t lbo_b = (uint32_t)N * 16, tap_bytes = KG * lbo_b, b_bytes = 9 * tap_bytes;
     const uint32_t stage_bytes = kResident ? a_bytes : a_bytes + b_bytes;
     // resident weights: [chunk][tap][k group][n], then the stages
     unsigned char *const wres = smem_raw;
     unsigned char *const stages = smem_raw + (kResident ? (size_t)chunks * b_bytes : 0);
-    const uint32_t idesc = tc::idesc_bf16(kBM, N, false, false);
     const uint32_t ncols = tmem_cols(2 * N);
     const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-    const int total = my_tiles * chunks;
+    volatile int *abort = &abort_flag;
 
     if (tid == 0) {
-        for (int i = 0; i < kConvStages + 2; ++i) tc::mbar_init(&bars[i], 1);
+        for (int i = 0; i < kS; ++i) {
+            tc::mbar_init(&full[i], kProd);
+            tc::mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&tfull[i], 1);
+            tc::mbar_init(&tempty[i], 128);
+        }
+        tc::mbar_init(&mma_done, 1);
+        abort_flag = 0;
         tc::fence_mbar_init();
     }
-    if (warp == 0) tc::tmem_alloc(&tmem_slot, ncols);
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = tmem_slot;
-    bool failed = false;
+    for (int n = tid; n < N; n += kConvThreads) sbias[n] = a.bias ? a.bias[n] : 0.f;
+    if (warp == kMmaWarp) tc::tmem_alloc(&tmem_slot, ncols);
     if (kResident) {
-        for (int pr = tid; pr < chunks * 9 * N; pr += kConvThreads) {
-            const int ch = pr / (9 * N), rest = pr - ch * 9 * N, t = rest / N, n = rest - t * N;
-            const __nv_bfloat16 *src = a.wgt + ((size_t)t * N + n) * C + ch * KC;
-            unsigned char *dst = wres + ch * b_bytes + t * tap_bytes + n * 16;
-            for (int kg = 0; kg < KG; ++kg) tc::cp_async16(dst + kg * lbo_b, src + kg * 8, 16u);
+        for (int pr = tid; pr < chunks * 9 * N * KG; pr += kConvThreads) {
+            const int kg = pr & (KG - 1), row = pr >> kg_shift;
+            const int ch = row / (9 * N), rest = row - ch * 9 * N, t = rest / N, n = rest - t * N;
+            tc::cp_async16(wres + ch * b_bytes + t * tap_bytes + kg * lbo_b + n * 16,
+                           a.wgt + ((size_t)t * N + n) * C + ch * KC + kg * 8, 16u);
         }
         tc::cp_async_commit();
         tc::cp_async_wait_all();
         tc::fence_proxy_async();
-        __syncthreads();
     }
-
-    // epilogue of tile-local index tl: accumulators -> bias / ReLU / mask -> NHWC
-    auto epilogue = [&](int tl) -> bool {
-        const int slot = tl & 1;
-        const bool ok = tc::mbar_wait(&bars[kConvStages + slot], (tl >> 1) & 1);
-        if (__syncthreads_or(!ok)) return false;
-        tc::fence_after_sync();
-        const int tile = blockIdx.x + tl * gridDim.x;
-        // warp w reads TMEM lanes 32 (w % 4) .. +31 (one pixel per thread);
-        // the warp groups (w / 4) split the 16-column groups between them
-        constexpr int kGroups = kConvThreads / 128;
-        const int64_t p = padded_to_pixel(qbeg + tile * kBM + (tid & 127), W, H, NR);
-        const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16) + slot * N;
-        const int per = (N / 16 + kGroups - 1) / kGroups * 16, grp = warp >> 2;
-        const int nbeg = min(N, grp * per), nend = min(N, nbeg + per);
-        for (int n0 = nbeg; n0 < nend; n0 += 16) {
-            float v[16];
-            tc::tmem_ld16(lane_base + n0, v);
-            if (p < 0) continue;
-            if (a.bias)
-                for (int i = 0; i < 16; ++i) v[i] += a.bias[n0 + i];
-            if (a.relu)
-                for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
-            if (a.mask) {
-                const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + p * N + n0);
-                uint4 mv[2] = {mp[0], mp[1]};
-                const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(mv);
-                for (int i = 0; i < 16; ++i)
-                    if (!(__bfloat162float(mb[i]) > 0.f)) v[i] = 0.f;
-            }
-            if (a.out) {
-                uint4 ov[2];
-                __nv_bfloat16 *ob = reinterpret_cast<__nv_bfloat16 *>(ov);
-                for (int i = 0; i < 16; ++i) ob[i] = __float2bfloat16_rn(v[i]);
-                uint4 *op = reinterpret_cast<uint4 *>(a.out + p * N + n0);
-                op[0] = ov[0];
-                op[1] = ov[1];
-            }
-            if (a.out_f32) {
-                float4 *op = reinterpret_cast<float4 *>(a.out_f32 + p * N + n0);
-                for (int i = 0; i < 4; ++i) op[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-            }
-        }
-        tc::fence_before_sync();
-        __syncthreads();  // this slot's TMEM reads are done before it is reused
-        return true;
-    };
-
-    for (int s = 0; s < total + kConvStages - 1 && !failed; ++s) {
-        bool ok = true;
-        if (s < total) {
-            const int st = s % kConvStages;
-            if (s >= kConvStages) ok = tc::mbar_wait(&bars[st], ((s / kConvStages) - 1) & 1);
-            unsigned char *sa = stages + st * stage_bytes, *sb = sa + a_bytes;
-            const int tile = blockIdx.x + (s / chunks) * gridDim.x, c0 = (s % chunks) * KC;
-            const int t0 = qbeg + tile * kBM;
-            // halo: one pixel per (region, row), its KC channels as KG vectors
-            for (int pr = tid; pr < 3 * kHalo; pr += kConvThreads) {
-                const int r = pr / kHalo, j = pr - r * kHalo;
-                const int p = padded_to_pixel(t0 + (r - 1) * Wp + j - 1, W, H, NR);
-                const __nv_bfloat16 *src = p >= 0 ? a.in + (size_t)p * C + c0 : a.in;
-                unsigned char *dst = sa + r * region_bytes + j * 16;
-                for (int kg = 0; kg < KG; ++kg)
-                    tc::cp_async16(dst + kg * lbo_a, p >= 0 ? src + kg * 8 : src, p >= 0 ? 16u : 0u);
-            }
-            // weights: one (tap, output channel) row per iteration
-            for (int pr = tid; pr < (kResident ? 0 : 9 * N); pr += kConvThreads) {
-                const int t = pr / N, n = pr - t * N;
-                const __nv_bfloat16 *src = a.wgt + ((size_t)t * N + n) * C + c0;
-                unsigned char *dst = sb + t * tap_bytes + n * 16;
-                for (int kg = 0; kg < KG; ++kg) tc::cp_async16(dst + kg * lbo_b, src + kg * 8, 16u);
-            }
-        }
-        tc::cp_async_commit();
-        const int c = s - (kConvStages - 1);
-        if (c < 0) {
-            if (__syncthreads_or(!ok)) failed = true;
-            continue;
-        }
-        tc::cp_async_wait<kConvStages - 1>();
-        tc::fence_proxy_async();
-        if (__syncthreads_or(!ok)) {
-            failed = true;
-            break;
-        }
-        const int tl = c / chunks, chunk = c % chunks, slot = tl & 1, st = c % kConvStages;
-        if (tid == 0) {
-            const uint32_t sa = tc::smem_addr(stages + st * stage_bytes);
-            const uint32_t sb = kResident ? tc::smem_addr(wres + chunk * b_bytes) : sa + a_bytes;
-            tc::fence_after_sync();
-            for (int tap = 0; tap < 9; ++tap) {
-                int sy = tap / 3 - 1, sx = tap % 3 - 1;
-                if (a.flip) {
-                    sy = -sy;
-                    sx = -sx;
-                }
-                for (int jj = 0; jj < KG / 2; ++jj)
-                    tc::mma_bf16(tmem + slot * N,
-                                 tc::smem_desc(sa + (sy + 1) * region_bytes + 2 * jj * lbo_a + (sx + 1) * 16, lbo_a, 128),
-                                 tc::smem_desc(sb + tap * tap_bytes + 2 * jj * lbo_b, lbo_b, 128), idesc,
-                                 chunk > 0 || tap > 0 || jj > 0);
-            }
-            tc::mma_commit(tc::smem_addr(&bars[st]));
-            if (chunk == chunks - 1) tc::mma_commit(tc::smem_addr(&bars[kConvStages + slot]));
-        }
-        if (chunk == 0 && tl > 0 && !epilogue(tl - 1)) failed = true;
-    }
-    if (!failed && my_tiles > 0 && !epilogue(my_tiles - 1)) failed = true;
-    if (failed && tid == 0) atomicExch(a.err, 1);
-    tc::cp_async_wait_all();
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp < kEpi0) {
+        // ---- producers ----
+        const int ptid = tid;
+        int s = 0;
+        for (int tl = 0; tl < my_tiles; ++tl) {
+            const int t0 = qbeg + (blockIdx.x + tl * gridDim.x) * kBM;
+            tc::named_sync(1, kProd);  // the previous tile's rows are no longer read
+            for (int pr = ptid; pr < 3 * kHalo; pr += kProd) {
+                const int r = pr / kHalo, j = pr - r * kHalo;
+                hpix[pr] = padded_to_pixel(t0 + (r - 1) * Wp + j - 1, W, H, NR);
+            }
+            tc::named_sync(1, kProd);
+            for (int chunk = 0; chunk < chunks; ++chunk, ++s) {
+                const int st = s % kS, c0 = chunk * KC;
+                if (s >= kS && !tc::mbar_wait_or_abort(&empty[st], ((s / kS) - 1) & 1, abort)) {
+                    // another role gave up: keep the loop (and its named
+                    // barriers) uniform over the producer warps, copy nothing
+                } else if (!*abort) {
+                    unsigned char *sa = stages + st * stage_bytes;
+                    // halo: consecutive threads copy consecutive 16 B of one pixel
+                    for (int it = ptid; it < 3 * kHalo * KG; it += kProd) {
+                        const int kg = it & (KG - 1), pr = it >> kg_shift;
+                        const int r = pr / kHalo, j = pr - r * kHalo, p = hpix[pr];
+                        const __nv_bfloat16 *src = p >= 0 ? a.in + (size_t)p * C + c0 + kg * 8 : a.in;
+                        tc::cp_async16(sa + r * region_bytes + kg * lbo_a + j * 16, src, p >= 0 ? 16u : 0u);
+                    }
+                    if (!kResident) {
+                        unsigned char *sb = sa + a_bytes;
+                        for (int it = ptid; it < 9 * N * KG; it += kProd) {
+                            const int kg = it & (KG - 1), row = it >> kg_shift, t = row / N, n = row - t * N;
+                            tc::cp_async16(sb + t * tap_bytes + kg * lbo_b + n * 16,
+                                           a.wgt + ((size_t)t * N + n) * C + c0 + kg * 8, 16u);
+                        }
+                    }
+                }
+                tc::cp_async_commit();
+                if (s >= kLag) {
+                    tc::cp_async_wait<kLag>();
+                    tc::fence_proxy_async();
+                    tc::mbar_arrive(&full[(s - kLag) % kS]);
+                }
+            }
+        }
+        tc::cp_async_wait_all();
+        tc::fence_proxy_async();
+        for (int s2 = s > kLag ? s - kLag : 0; s2 < s; ++s2) tc::mbar_arrive(&full[s2 % kS]);
+    } else if (warp < kMmaWarp) {
+        // ---- epilogue ----
+        const int etid = tid - kEpi0 * 32;  // = 32 * (warp % 4) + lane: this thread's TMEM lane
+        for (int tl = 0; tl < my_tiles; ++tl) {
+            const int slot = tl & 1;
+            if (!tc::mbar_wait_or_abort(&tfull[slot], (tl >> 1) & 1, abort)) break;
+            tc::fence_after_sync();
+            const int64_t p = padded_to_pixel(qbeg + (blockIdx.x + tl * gridDim.x) * kBM + etid, W, H, NR);
+            const uint32_t lane_base = tmem + ((uint32_t)(etid & ~31) << 16) + slot * N;
+            for (int n0 = 0; n0 < N; n0 += 16) {
+                float v[16];
+                tc::tmem_ld16(lane_base + n0, v);
+                if (p < 0) continue;
+                for (int i = 0; i < 16; ++i) v[i] += sbias[n0 + i];
+                if (a.relu)
+                    for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
+                if (a.mask) {
+                    const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + p * N + n0);
+                    uint4 mv[2] = {mp[0], mp[1]};
+                    const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(mv);
+                    for (int i = 0; i < 16; ++i)
+                        if (!(__bfloat162float(mb[i]) > 0.f)) v[i] = 0.f;
+                }
+                if (a.out) {
+                    uint4 ov[2];
+                    __nv_bfloat16 *ob = reinterpret_cast<__nv_bfloat16 *>(ov);
+                    for (int i = 0; i < 16; ++i) ob[i] = __float2bfloat16_rn(v[i]);
+                    uint4 *op = reinterpret_cast<uint4 *>(a.out + p * N + n0);
+                    op[0] = ov[0];
+                    op[1] = ov[1];
+                }
+                if (a.out_f32) {
+                    float4 *op = reinterpret_cast<float4 *>(a.out_f32 + p * N + n0);
+                    for (int i = 0; i < 4; ++i) op[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                }
+            }
+            tc::fence_before_sync();
+            tc::mbar_arrive(&tempty[slot]);  // this slot's TMEM reads are done
+        }
+    } else if ((tid & 31) == 0) {
+        // ---- MMA issuer ----
+        const uint32_t idesc = tc::idesc_bf16(kBM, N, false, false);
+        int s = 0;
+        for (int tl = 0; tl < my_tiles && !*abort; ++tl) {
+            const int slot = tl & 1;
+            if (tl >= 2 && !tc::mbar_wait_or_abort(&tempty[slot], ((tl >> 1) - 1) & 1, abort)) break;
+            tc::fence_after_sync();
+            bool ok = true;
+            for (int chunk = 0; chunk < chunks; ++chunk, ++s) {
+                const int st = s % kS;
+                if (!tc::mbar_wait_or_abort(&full[st], (s / kS) & 1, abort)) {
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t sa = tc::smem_addr(stages + st * stage_bytes);
+                const uint32_t sb = kResident ? tc::smem_addr(wres + chunk * b_bytes) : sa + a_bytes;
+                for (int tap = 0; tap < 9; ++tap) {
+                    int sy = tap / 3 - 1, sx = tap % 3 - 1;
+                    if (a.flip) {
+                        sy = -sy;
+                        sx = -sx;
+                    }
+                    for (int jj = 0; jj < KG / 2; ++jj)
+                        tc::mma_bf16(tmem + slot * N,
+                                     tc::smem_desc(sa + (sy + 1) * region_bytes + 2 * jj * lbo_a + (sx + 1) * 16, lbo_a, 128),
+                                     tc::smem_desc(sb + tap * tap_bytes + 2 * jj * lbo_b, lbo_b, 128), idesc,
+                                     chunk > 0 || tap > 0 || jj > 0);
+                }
+                tc::mma_commit(tc::smem_addr(&empty[st]));
+                if (chunk == chunks - 1) tc::mma_commit(tc::smem_addr(&tfull[slot]));
+            }
+            if (!ok) break;
+        }
+        // every MMA issued has finished before TMEM is released
+        tc::mma_commit(tc::smem_addr(&mma_done));
+        tc::mbar_wait(&mma_done, 0);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (tid == 0 && abort_flag) atomicExch(a.err, 1);
+    if (warp == kMmaWarp) tc::tmem_dealloc(tmem, ncols);
 }
 
 struct WgradArgs {
@@ -407,29 +450,33 @@ void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const flo
     a.N = N;
     a.flip = flip ? 1 : 0;
     a.relu = relu ? 1 : 0;
-    // Weights resident in shared memory when they fit next to 5 halo
-    // stages, else streamed per stage with 3 stages; the channel chunk KC is
-    // the largest of 64, 32, 16 dividing C that fits.
+    // Weights resident in shared memory when they fit next to 4 or 5 halo
+    // stages, else streamed per stage with 3 or 4 stages; the largest
+    // channel chunk KC of 64, 32, 16 dividing C that fits wins, then the
+    // deeper pipeline.
     const size_t kSmemCap = 220 * 1024;
     const size_t wbytes = (size_t)9 * N * C * 2;
     auto a_stage = [&](int kc) { return (size_t)kc * 3 * kHalo * 2; };
     bool resident = false;
+    int stages = 0;
     a.KC = 0;
     for (int kc : {64, 32, 16})
-        if (C % kc == 0 && wbytes + 5 * a_stage(kc) <= kSmemCap) {
-            a.KC = kc;
-            resident = true;
-            break;
-        }
-    if (!resident)
-        for (int kc : {64, 32, 16})
-            if (C % kc == 0 && 3 * (a_stage(kc) + (size_t)18 * N * kc) <= kSmemCap) {
+        for (int ns : {5, 4})
+            if (!a.KC && C % kc == 0 && wbytes + ns * a_stage(kc) <= kSmemCap) {
                 a.KC = kc;
-                break;
+                stages = ns;
+                resident = true;
+            }
+    for (int kc : {64, 32, 16})
+        for (int ns : {4, 3})
+            if (!a.KC && C % kc == 0 && ns * (a_stage(kc) + (size_t)18 * N * kc) <= kSmemCap) {
+                a.KC = kc;
+                stages = ns;
             }
     CRT_CHECK(a.KC > 0, CRT_ERR_INVALID, "conv3x3: tile does not fit shared memory");
-    const size_t smem = resident ? wbytes + 5 * a_stage(a.KC) : 3 * (a_stage(a.KC) + (size_t)18 * N * a.KC);
-    const void *kfn = resident ? (const void *)k_conv3x3<5, true> : (const void *)k_conv3x3<3, false>;
+    const size_t smem = resident ? wbytes + stages * a_stage(a.KC) : stages * (a_stage(a.KC) + (size_t)18 * N * a.KC);
+    const void *kfn = resident ? (stages == 5 ? (const void *)k_conv3x3<5, true> : (const void *)k_conv3x3<4, true>)
+                               : (stages == 4 ? (const void *)k_conv3x3<4, false> : (const void *)k_conv3x3<3, false>);
     CRT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kConvThreads, smem));
@@ -438,10 +485,8 @@ void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const flo
     CRT_CHECK(padded < (1LL << 31) - 4 * kBM, CRT_ERR_INVALID, "conv3x3: image too large");
     const int64_t tiles = ((int64_t)(w + 2) * (nimg * (int64_t)(h + 1) - 1) + kBM - 1) / kBM;
     const int grid = (int)std::min<int64_t>(tiles, (int64_t)sm_count() * per_sm);
-    if (resident)
-        k_conv3x3<5, true><<<grid, kConvThreads, smem, s>>>(a);
-    else
-        k_conv3x3<3, false><<<grid, kConvThreads, smem, s>>>(a);
+    void *args[] = {&a};
+    CRT_CUDA(cudaLaunchKernel(kfn, dim3(grid), dim3(kConvThreads), args, smem, s));
     CRT_CUDA(cudaGetLastError());
 }
 

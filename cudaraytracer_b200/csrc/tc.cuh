@@ -125,6 +125,33 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
     return false;
 }
 
+// Same, but also gives up as soon as *abort is set by another thread of the
+// block (which then stops waiting on this block's other barriers too); on a
+// timeout it sets *abort itself.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, uint32_t parity, volatile int *abort) {
+    for (int round = 0; round < 256; ++round) {
+        if (*abort) return false;
+        if (mbar_wait(bar, parity, 1u << 16)) return true;
+    }
+    *abort = 1;
+    return false;
+}
+
+// Plain arrive (release at CTA scope) by this thread.
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile(
+        "{\n\t"
+        ".reg .b64 st;\n\t"
+        "mbarrier.arrive.shared::cta.b64 st, [%0];\n\t"
+        "}\n" ::"r"(smem_addr(bar))
+        : "memory");
+}
+
+// Named barrier `id` (1..15) over `nthreads` threads (a multiple of 32).
+__device__ __forceinline__ void named_sync(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
 // 16 B global -> shared copy; src_bytes = 0 fills zeros (src must still be
 // a valid address).
 __device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t src_bytes) {
