@@ -25,26 +25,32 @@
 #include "api_internal.h"
 #include "tc.cuh"
 #include <algorithm>
+#include <cudaTypedefs.h>
+#include <type_traits>
 
 namespace crt {
 namespace {
 
 constexpr int kBM = 128;      // pixels (or (tap, c) rows) per tile
 constexpr int kThreads = 128;      // weight-gradient kernel
-constexpr int kConvThreads = 288;  // forward / data-gradient kernel: 4 producer, 4 epilogue, 1 MMA warp
+constexpr int kFwdThreads = 320;  // forward / data gradient: TMA warp, MMA warp, 8 epilogue warps
+constexpr int kMaxStages = 5;
 constexpr int kStages = 4;
 constexpr int kWgradBK = 64;  // pixels per weight-gradient K step
 
 struct ConvArgs {
-    const __nv_bfloat16 *in;    // [P][C]
-    const __nv_bfloat16 *wgt;   // [9][N][C]
     const float *bias;          // [N] or null
     const __nv_bfloat16 *mask;  // [P][N] or null: out *= (mask > 0)
     __nv_bfloat16 *out;         // [P][N] or null
     float *out_f32;             // [P][N] or null
     int *err;
-    int nimg, h, wd, C, N, KC;
-    int flip, relu;
+    int nimg, h, wd, C, N;
+    int KC, RB;                 // channel chunk and its row bytes in shared memory (2 KC, the swizzle span)
+    int NP, MB, M;              // pixels per tile (the MMA's N), 128-row blocks of output channels, MMA M
+    int stages, resident, flip, relu;
+    uint32_t region_bytes;      // one halo row: NP + 2 pixels x RB, rounded up to 1 KB
+    uint32_t wchunk_bytes;      // weights of one channel chunk: [KC / 8][9][N][16 B]
+    uint32_t stage_bytes, wres_bytes;
 };
 
 __device__ __forceinline__ uint32_t tmem_cols(int n) {
@@ -53,233 +59,248 @@ __device__ __forceinline__ uint32_t tmem_cols(int n) {
     return c;
 }
 
-constexpr int kHalo = kBM + 2;  // rows of one halo region
-
-// Position q of the padded linear image space (rows of W + 2: columns W and
-// W + 1 are zero padding, column W + 1 doubling as column -1 of the next
-// row; row 0 and one row after every image are zero rows) -> NHWC pixel
-// index, or -1 for padding.
-// (32-bit arithmetic: the host refuses images whose padded space reaches 2^31.)
-__device__ __forceinline__ int padded_to_pixel(int q, int W, int H, int NR) {
-    if (q < 0) return -1;
-    const int Wp = W + 2;
-    const int R = q / Wp;
-    const int x = q - R * Wp;
-    if (x >= W || R < 1 || R > NR - 2) return -1;
-    const int rr = R - 1;
-    const int b = rr / (H + 1);
-    const int r = rr - b * (H + 1);
-    if (r >= H) return -1;
-    return (b * H + r) * W + x;
-}
-
-// One CTA walks its tiles of 128 consecutive padded positions. Per tile and
-// channel chunk of KC, a stage holds three halo regions (input rows shifted
-// by -1, 0, +1; 130 positions each: the tile plus one on either side) and,
-// unless the weights are resident, the chunk of all 9 taps' weights. Tap
-// (dy, dx) is then the MMA whose A operand starts dx + 1 rows (16 B each)
-// into region dy + 1: no per-tap gather.
+// Forward and data gradient with the output channels on the MMA's M side
+// (M = 64 for up to 64 channels, else 128-row blocks; rows past N read
+// neighbouring weights and their results are never read back) and NP = 256
+// (or 128) pixels of one image row on its N side. One tcgen05.mma costs
+// about the same issue time whatever its shape, so the wide N = 256 tile is
+// what keeps the tensor core busy.
+//
+// A tile is pixels x0 .. x0 + NP - 1 of row y of image b. Per channel chunk
+// of KC a stage holds the three input rows y - 1, y, y + 1, columns
+// x0 - 1 .. x0 + NP, each written by TMA (an NP-wide box and a 2-wide edge
+// box, zero-filled outside the image) in the swizzled K-major layout with
+// RB = 2 KC bytes per pixel row. Tap (dy, dx) is the MMA whose B operand
+// starts dx + 1 rows into row buffer dy + 1: no gather (the swizzle is a
+// function of the absolute shared-memory address, so shifted starts read
+// the rows TMA wrote). The weights (A, [chunk][k group][tap][n][16 B], no
+// swizzle) are loaded by TMA once per CTA when they fit next to the stages,
+// else per stage.
 // Warp roles (no block-wide barrier inside the tile loop):
-//   warps 0-3  producers: cp.async the halo (and streamed weights) of step s
-//              into stage s % kS; once a step's copies have landed they
-//              make them visible to the tensor core (proxy fence) and
-//              arrive on full[stage]. kS - 2 steps stay in flight.
-//   warp 8     one thread issues the step's 9 taps x KC/16 MMAs into one of
-//              two TMEM accumulator slots and commits them to empty[stage]
-//              (the stage may be refilled) and, after a tile's last chunk,
-//              to tfull[slot].
-//   warps 4-7  epilogue: TMEM lane quarter (warp % 4), one pixel per thread:
-//              bias / ReLU / mask, BF16 or FP32 NHWC stores; then arrive on
-//              tempty[slot] so the MMAs of tile + 2 may overwrite the slot.
+//   warp 0     one thread issues the TMA loads of step s into stage s % S
+//              (after the MMAs of step s - S released it) with the bytes
+//              it expects on full[stage].
+//   warp 1     the whole warp runs the MMA loop, one elected lane issues the
+//              step's 9 taps x KC / 16 x MB MMAs into one of two TMEM
+//              accumulator slots and commits them to empty[stage] and,
+//              after a tile's last chunk, to tfull[slot].
+//   warps 2-9  epilogue: TMEM lane quarter warp % 4, half (warp - 2) / 4 of
+//              the tile's pixels; bias / ReLU in FP32, BF16 staged through
+//              shared memory into 16 B stores (ReLU mask applied there).
+//              Then arrive on tempty[slot].
 // Every wait is bounded and also ends when another role has given up.
-// kResident: the layer's weights (all taps, all channel chunks) are loaded
-// into shared memory once per CTA; stages then hold only halo regions.
-template <int kS, bool kResident>
-__global__ void __launch_bounds__(kConvThreads, 1) k_conv3x3(ConvArgs a) {
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ uint64_t full[kS], empty[kS], tfull[2], tempty[2], mma_done;
+// kKS = KC / 16 (K steps per tap) and kMB are compile-time so that the MMA
+// warp's loop unrolls into base descriptors plus precomputed offsets: the
+// issue loop, not the tensor core, is otherwise the bottleneck.
+template <int kKS, int kMB>
+__global__ void __launch_bounds__(kFwdThreads, 1)
+    k_conv3x3(const __grid_constant__ CUtensorMap map_in, const __grid_constant__ CUtensorMap map_edge,
+              const __grid_constant__ CUtensorMap map_w, ConvArgs a) {
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ uint64_t full[kMaxStages], empty[kMaxStages], tfull[2], tempty[2], wbar, mma_done;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
-    __shared__ int hpix[3 * kHalo];  // pixel index (or -1) of each halo row of the producers' tile
-    __shared__ float sbias[256];
-    constexpr int kLag = kS - 2;     // producer steps in flight before a step is signalled
-    constexpr int kProd = 128, kEpi0 = 4, kMmaWarp = 8;
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int C = a.C, N = a.N, KC = a.KC, W = a.wd, H = a.h;
-    const int Wp = W + 2, NR = a.nimg * (H + 1) + 1;
-    const int qbeg = Wp, qend = Wp * (NR - 1);
-    const int ntiles = (qend - qbeg + kBM - 1) / kBM;
-    const int chunks = C / KC, KG = KC / 8, kg_shift = KG == 8 ? 3 : KG == 4 ? 2 : 1;
-    const uint32_t lbo_a = kHalo * 16, region_bytes = KG * lbo_a, a_bytes = 3 * region_bytes;
-    const uint32_t lbo_b = (uint32_t)N * 16, tap_bytes = KG * lbo_b, b_bytes = 9 * tap_bytes;
-    const uint32_t stage_bytes = kResident ? a_bytes : a_bytes + b_bytes;
-    // resident weights: [chunk][tap][k group][n], then the stages
-    unsigned char *const wres = smem_raw;
-    unsigned char *const stages = smem_raw + (kResident ? (size_t)chunks * b_bytes : 0);
-    const uint32_t ncols = tmem_cols(2 * N);
+    __shared__ __align__(16) __nv_bfloat16 ostage[8][16 * 32];  // per epilogue warp: 16 pixels x 32 channels
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr int KC = 16 * kKS, RB = 2 * KC, KG = KC / 8, MB = kMB;
+    const int C = a.C, N = a.N, W = a.wd, H = a.h, NP = a.NP, S = a.stages;
+    const int chunks = C / KC;
+    const int ntx = (W + NP - 1) / NP, ntiles = a.nimg * H * ntx;
+    const uint32_t region_bytes = a.region_bytes, stage_bytes = a.stage_bytes, wchunk_bytes = a.wchunk_bytes;
+    const uint32_t tap_bytes = (uint32_t)N * 16, wkg_bytes = 9 * tap_bytes;
+    // 1 KB aligned: TMA swizzle atoms and the descriptors' address phase
+    unsigned char *const base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    unsigned char *const wres = base;
+    unsigned char *const stages = base + a.wres_bytes;
+    const uint32_t slot_cols = (uint32_t)(MB * NP), ncols = tmem_cols(2 * MB * NP);
     const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     volatile int *abort = &abort_flag;
 
     if (tid == 0) {
-        for (int i = 0; i < kS; ++i) {
-            tc::mbar_init(&full[i], kProd);
+        for (int i = 0; i < S; ++i) {
+            tc::mbar_init(&full[i], 1);
             tc::mbar_init(&empty[i], 1);
         }
         for (int i = 0; i < 2; ++i) {
             tc::mbar_init(&tfull[i], 1);
-            tc::mbar_init(&tempty[i], 128);
+            tc::mbar_init(&tempty[i], 256);
         }
+        tc::mbar_init(&wbar, 1);
         tc::mbar_init(&mma_done, 1);
         abort_flag = 0;
         tc::fence_mbar_init();
     }
-    for (int n = tid; n < N; n += kConvThreads) sbias[n] = a.bias ? a.bias[n] : 0.f;
-    if (warp == kMmaWarp) tc::tmem_alloc(&tmem_slot, ncols);
-    if (kResident) {
-        for (int pr = tid; pr < chunks * 9 * N * KG; pr += kConvThreads) {
-            const int kg = pr & (KG - 1), row = pr >> kg_shift;
-            const int ch = row / (9 * N), rest = row - ch * 9 * N, t = rest / N, n = rest - t * N;
-            tc::cp_async16(wres + ch * b_bytes + t * tap_bytes + kg * lbo_b + n * 16,
-                           a.wgt + ((size_t)t * N + n) * C + ch * KC + kg * 8, 16u);
-        }
-        tc::cp_async_commit();
-        tc::cp_async_wait_all();
-        tc::fence_proxy_async();
-    }
+    if (warp == 1) tc::tmem_alloc(&tmem_slot, ncols);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
 
-    if (warp < kEpi0) {
-        // ---- producers ----
-        const int ptid = tid;
-        int s = 0;
-        for (int tl = 0; tl < my_tiles; ++tl) {
-            const int t0 = qbeg + (blockIdx.x + tl * gridDim.x) * kBM;
-            tc::named_sync(1, kProd);  // the previous tile's rows are no longer read
-            for (int pr = ptid; pr < 3 * kHalo; pr += kProd) {
-                const int r = pr / kHalo, j = pr - r * kHalo;
-                hpix[pr] = padded_to_pixel(t0 + (r - 1) * Wp + j - 1, W, H, NR);
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer ----
+            if (a.resident) {
+                tc::mbar_arrive_expect_tx(&wbar, chunks * wchunk_bytes);
+                for (int ch = 0; ch < chunks; ++ch)
+                    for (int kg = 0; kg < KG; ++kg)
+                        tc::tma_load_3d(wres + ch * wchunk_bytes + kg * wkg_bytes, &map_w, ch * KC + kg * 8, 0, 0,
+                                        &wbar);
             }
-            tc::named_sync(1, kProd);
-            for (int chunk = 0; chunk < chunks; ++chunk, ++s) {
-                const int st = s % kS, c0 = chunk * KC;
-                if (s >= kS && !tc::mbar_wait_or_abort(&empty[st], ((s / kS) - 1) & 1, abort)) {
-                    // another role gave up: keep the loop (and its named
-                    // barriers) uniform over the producer warps, copy nothing
-                } else if (!*abort) {
+            const uint32_t tx = 3u * (NP + 2) * RB + (a.resident ? 0u : wchunk_bytes);
+            int s = 0;
+            for (int tl = 0; tl < my_tiles && !*abort; ++tl) {
+                const int tile = blockIdx.x + tl * gridDim.x, xt = tile % ntx, by = tile / ntx;
+                const int y = by % H, b = by / H, x0 = xt * NP;
+                bool ok = true;
+                for (int ch = 0; ch < chunks; ++ch, ++s) {
+                    const int st = s % S;
+                    if (s >= S && !tc::mbar_wait_or_abort(&empty[st], ((s / S) - 1) & 1, abort)) {
+                        ok = false;
+                        break;
+                    }
                     unsigned char *sa = stages + st * stage_bytes;
-                    // halo: consecutive threads copy consecutive 16 B of one pixel
-                    for (int it = ptid; it < 3 * kHalo * KG; it += kProd) {
-                        const int kg = it & (KG - 1), pr = it >> kg_shift;
-                        const int r = pr / kHalo, j = pr - r * kHalo, p = hpix[pr];
-                        const __nv_bfloat16 *src = p >= 0 ? a.in + (size_t)p * C + c0 + kg * 8 : a.in;
-                        tc::cp_async16(sa + r * region_bytes + kg * lbo_a + j * 16, src, p >= 0 ? 16u : 0u);
+                    tc::mbar_arrive_expect_tx(&full[st], tx);
+                    for (int r = 0; r < 3; ++r) {
+                        tc::tma_load_4d(sa + r * region_bytes, &map_in, ch * KC, x0 - 1, y + r - 1, b, &full[st]);
+                        tc::tma_load_4d(sa + r * region_bytes + NP * RB, &map_edge, ch * KC, x0 - 1 + NP, y + r - 1,
+                                        b, &full[st]);
                     }
-                    if (!kResident) {
-                        unsigned char *sb = sa + a_bytes;
-                        for (int it = ptid; it < 9 * N * KG; it += kProd) {
-                            const int kg = it & (KG - 1), row = it >> kg_shift, t = row / N, n = row - t * N;
-                            tc::cp_async16(sb + t * tap_bytes + kg * lbo_b + n * 16,
-                                           a.wgt + ((size_t)t * N + n) * C + c0 + kg * 8, 16u);
-                        }
-                    }
+                    if (!a.resident)
+                        for (int kg = 0; kg < KG; ++kg)
+                            tc::tma_load_3d(sa + 3 * region_bytes + kg * wkg_bytes, &map_w, ch * KC + kg * 8, 0, 0,
+                                            &full[st]);
                 }
-                tc::cp_async_commit();
-                if (s >= kLag) {
-                    tc::cp_async_wait<kLag>();
-                    tc::fence_proxy_async();
-                    tc::mbar_arrive(&full[(s - kLag) % kS]);
+                if (!ok) break;
+            }
+            // no TMA write may land after the CTA has exited: wait for the
+            // last phase issued on every stage (immediate when consumed)
+            for (int st = 0; st < S && st < s; ++st) {
+                const int last = s - 1 - ((s - 1 - st) % S);
+                tc::mbar_wait(&full[st], (last / S) & 1);
+            }
+            if (a.resident) tc::mbar_wait(&wbar, 0);
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer: the whole warp runs the loop, one lane issues ----
+        // Descriptor offsets (16 B units in the start-address field, which
+        // never carries: shared addresses stay below 256 KB) of the 9 taps:
+        // B = row buffer r shifted by c rows; A = the tap's weight slice
+        // (mirrored taps for the data gradient).
+        const uint32_t idesc = tc::idesc_bf16(a.M, NP, false, false);
+        uint32_t boff[9], aoff[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            const int r = t / 3, c = t % 3, tap = a.flip ? 8 - t : t;
+            boff[t] = (r * region_bytes + c * RB) >> 4;
+            aoff[t] = (tap * tap_bytes) >> 4;
+        }
+        const uint64_t bdesc0 = tc::smem_desc_sw(tc::smem_addr(stages), RB);
+        const uint64_t adesc0 = tc::smem_desc(tc::smem_addr(a.resident ? wres : stages + 3 * region_bytes), wkg_bytes, 128);
+        const uint32_t stage16 = stage_bytes >> 4, wchunk16 = wchunk_bytes >> 4, kstep_a16 = (2 * wkg_bytes) >> 4;
+        int s = 0;
+        bool run = !a.resident || tc::mbar_wait_or_abort_warp(&wbar, 0, abort);
+        for (int tl = 0; tl < my_tiles && run; ++tl) {
+            const int slot = tl & 1;
+            if (tl >= 2 && !tc::mbar_wait_or_abort_warp(&tempty[slot], ((tl >> 1) - 1) & 1, abort)) break;
+            tc::fence_after_sync();
+            const uint32_t d = tmem + slot * slot_cols;
+            for (int ch = 0; ch < chunks; ++ch, ++s) {
+                const int st = s % S;
+                if (!tc::mbar_wait_or_abort_warp(&full[st], (s / S) & 1, abort)) {
+                    run = false;
+                    break;
                 }
+                tc::fence_after_sync();
+                const uint64_t bd = bdesc0 + st * stage16;
+                const uint64_t ad = adesc0 + (a.resident ? ch * wchunk16 : st * stage16);
+#pragma unroll
+                for (int t = 0; t < 9; ++t)
+#pragma unroll
+                    for (int kk = 0; kk < kKS; ++kk)
+#pragma unroll
+                        for (int mb = 0; mb < kMB; ++mb)
+                            tc::mma_bf16_warp(d + mb * NP, ad + aoff[t] + kk * kstep_a16 + mb * 128, bd + boff[t] + kk * 2,
+                                              idesc, ch > 0 || t > 0 || kk > 0);
+                tc::mma_commit_warp(tc::smem_addr(&empty[st]));
+                if (ch == chunks - 1) tc::mma_commit_warp(tc::smem_addr(&tfull[slot]));
             }
         }
-        tc::cp_async_wait_all();
-        tc::fence_proxy_async();
-        for (int s2 = s > kLag ? s - kLag : 0; s2 < s; ++s2) tc::mbar_arrive(&full[s2 % kS]);
-    } else if (warp < kMmaWarp) {
+        // every MMA issued has finished before TMEM is released
+        tc::mma_commit_warp(tc::smem_addr(&mma_done));
+        if (lane == 0) tc::mbar_wait(&mma_done, 0);
+        __syncwarp();
+    } else {
         // ---- epilogue ----
-        const int etid = tid - kEpi0 * 32;  // = 32 * (warp % 4) + lane: this thread's TMEM lane
+        // TMEM lane quarter q holds channels q * cpq .. + cpq - 1 of each
+        // 128-row block in its first cpq lanes (M = 128: 32 per quarter;
+        // M = 64: rows 16 q .. 16 q + 15 sit in lanes 32 q .. 32 q + 15).
+        // Per 16-pixel chunk the warp converts its channels to BF16 (bias,
+        // ReLU), stages them as [pixel][channel] in shared memory and writes
+        // 16 B pieces (8 channels of one pixel; the ReLU mask applied there).
+        const int q = warp & 3, half = (warp - 2) >> 2;
+        const int cpq = a.M == 64 ? 16 : 32, pieces = 16 * cpq / 8;
+        const int cbeg = half * (NP / 2), cend = cbeg + NP / 2;
+        __nv_bfloat16 *const os = ostage[warp - 2];
         for (int tl = 0; tl < my_tiles; ++tl) {
             const int slot = tl & 1;
             if (!tc::mbar_wait_or_abort(&tfull[slot], (tl >> 1) & 1, abort)) break;
             tc::fence_after_sync();
-            const int64_t p = padded_to_pixel(qbeg + (blockIdx.x + tl * gridDim.x) * kBM + etid, W, H, NR);
-            const uint32_t lane_base = tmem + ((uint32_t)(etid & ~31) << 16) + slot * N;
-            for (int n0 = 0; n0 < N; n0 += 16) {
-                float v[16];
-                tc::tmem_ld16(lane_base + n0, v);
-                if (p < 0) continue;
-                for (int i = 0; i < 16; ++i) v[i] += sbias[n0 + i];
-                if (a.relu)
-                    for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.f);
-                if (a.mask) {
-                    const uint4 *mp = reinterpret_cast<const uint4 *>(a.mask + p * N + n0);
-                    uint4 mv[2] = {mp[0], mp[1]};
-                    const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(mv);
-                    for (int i = 0; i < 16; ++i)
-                        if (!(__bfloat162float(mb[i]) > 0.f)) v[i] = 0.f;
-                }
-                if (a.out) {
-                    uint4 ov[2];
-                    __nv_bfloat16 *ob = reinterpret_cast<__nv_bfloat16 *>(ov);
-                    for (int i = 0; i < 16; ++i) ob[i] = __float2bfloat16_rn(v[i]);
-                    uint4 *op = reinterpret_cast<uint4 *>(a.out + p * N + n0);
-                    op[0] = ov[0];
-                    op[1] = ov[1];
-                }
-                if (a.out_f32) {
-                    float4 *op = reinterpret_cast<float4 *>(a.out_f32 + p * N + n0);
-                    for (int i = 0; i < 4; ++i) op[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            const int tile = blockIdx.x + tl * gridDim.x, xt = tile % ntx, by = tile / ntx;
+            const int x0 = xt * NP;
+            const size_t row_pix = (size_t)by * W;  // (b * H + y) * W
+            for (int mb = 0; mb < MB; ++mb) {
+                const int cq = mb * 128 + q * cpq;  // first channel of this quarter
+                if (cq >= N) continue;             // warp-uniform: no channels here
+                const int co = cq + lane;
+                const bool cvalid = lane < cpq && co < N;
+                const float bias = (a.bias && cvalid) ? a.bias[co] : 0.f;
+                const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + slot * slot_cols + mb * NP;
+                for (int col = cbeg; col < cend && x0 + col < W; col += 16) {
+                    float v[16];
+                    tc::tmem_ld16(taddr + col, v);
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        v[i] += bias;
+                        if (a.relu) v[i] = fmaxf(v[i], 0.f);
+                    }
+                    if (a.out_f32 && cvalid)
+#pragma unroll
+                        for (int i = 0; i < 16; ++i)
+                            if (x0 + col + i < W) a.out_f32[(row_pix + x0 + col + i) * N + co] = v[i];
+                    if (!a.out) continue;
+                    if (lane < cpq)
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) os[i * cpq + lane] = __float2bfloat16_rn(v[i]);
+                    __syncwarp();
+                    for (int j = lane; j < pieces; j += 32) {
+                        const int px = j / (cpq / 8), part = j - px * (cpq / 8);
+                        const int c8 = cq + part * 8;
+                        if (x0 + col + px < W && c8 < N) {
+                            uint4 val = *reinterpret_cast<const uint4 *>(os + px * cpq + part * 8);
+                            const size_t o = (row_pix + x0 + col + px) * N + c8;
+                            if (a.mask) {
+                                const uint4 mv = *reinterpret_cast<const uint4 *>(a.mask + o);
+                                const __nv_bfloat16 *mb16 = reinterpret_cast<const __nv_bfloat16 *>(&mv);
+                                __nv_bfloat16 *vb = reinterpret_cast<__nv_bfloat16 *>(&val);
+                                for (int e = 0; e < 8; ++e)
+                                    if (!(__bfloat162float(mb16[e]) > 0.f)) vb[e] = __float2bfloat16_rn(0.f);
+                            }
+                            *reinterpret_cast<uint4 *>(a.out + o) = val;
+                        }
+                    }
+                    __syncwarp();
                 }
             }
             tc::fence_before_sync();
             tc::mbar_arrive(&tempty[slot]);  // this slot's TMEM reads are done
         }
-    } else if ((tid & 31) == 0) {
-        // ---- MMA issuer ----
-        const uint32_t idesc = tc::idesc_bf16(kBM, N, false, false);
-        int s = 0;
-        for (int tl = 0; tl < my_tiles && !*abort; ++tl) {
-            const int slot = tl & 1;
-            if (tl >= 2 && !tc::mbar_wait_or_abort(&tempty[slot], ((tl >> 1) - 1) & 1, abort)) break;
-            tc::fence_after_sync();
-            bool ok = true;
-            for (int chunk = 0; chunk < chunks; ++chunk, ++s) {
-                const int st = s % kS;
-                if (!tc::mbar_wait_or_abort(&full[st], (s / kS) & 1, abort)) {
-                    ok = false;
-                    break;
-                }
-                tc::fence_after_sync();
-                const uint32_t sa = tc::smem_addr(stages + st * stage_bytes);
-                const uint32_t sb = kResident ? tc::smem_addr(wres + chunk * b_bytes) : sa + a_bytes;
-                for (int tap = 0; tap < 9; ++tap) {
-                    int sy = tap / 3 - 1, sx = tap % 3 - 1;
-                    if (a.flip) {
-                        sy = -sy;
-                        sx = -sx;
-                    }
-                    for (int jj = 0; jj < KG / 2; ++jj)
-                        tc::mma_bf16(tmem + slot * N,
-                                     tc::smem_desc(sa + (sy + 1) * region_bytes + 2 * jj * lbo_a + (sx + 1) * 16, lbo_a, 128),
-                                     tc::smem_desc(sb + tap * tap_bytes + 2 * jj * lbo_b, lbo_b, 128), idesc,
-                                     chunk > 0 || tap > 0 || jj > 0);
-                }
-                tc::mma_commit(tc::smem_addr(&empty[st]));
-                if (chunk == chunks - 1) tc::mma_commit(tc::smem_addr(&tfull[slot]));
-            }
-            if (!ok) break;
-        }
-        // every MMA issued has finished before TMEM is released
-        tc::mma_commit(tc::smem_addr(&mma_done));
-        tc::mbar_wait(&mma_done, 0);
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     if (tid == 0 && abort_flag) atomicExch(a.err, 1);
-    if (warp == kMmaWarp) tc::tmem_dealloc(tmem, ncols);
+    if (warp == 1) tc::tmem_dealloc(tmem, ncols);
 }
 
 struct WgradArgs {
@@ -419,6 +440,31 @@ int host_tmem_cols(int n) {
     return c;
 }
 
+// cuTensorMapEncodeTiled from the driver, found once through the runtime
+// (the library links no driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        CRT_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q));
+        CRT_CHECK(f && q == cudaDriverEntryPointSuccess, CRT_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    return fn;
+}
+
+void encode_map(CUtensorMap *m, const void *ptr, cuuint32_t rank, const cuuint64_t *dims,
+                const cuuint64_t *strides_bytes, const cuuint32_t *box, CUtensorMapSwizzle swz) {
+    const cuuint32_t ones[5] = {1, 1, 1, 1, 1};
+    const CUresult r = tensor_map_encoder()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void *>(ptr), dims,
+                                            strides_bytes, box, ones, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CRT_CHECK(r == CUDA_SUCCESS, CRT_ERR_CUDA, "conv3x3: tensor map encoding failed");
+}
+
+size_t round1k(size_t v) { return (v + 1023) & ~(size_t)1023; }
+
 }  // namespace
 
 void conv3x3_check(int C, int N) {
@@ -434,10 +480,14 @@ void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const flo
                     bool relu, cudaStream_t s) {
     conv3x3_check(C, N);
     const int64_t P = (int64_t)nimg * h * w;
-    CRT_CHECK(P > 0 && P < (1LL << 31) - kBM, CRT_ERR_INVALID, "conv3x3: bad image size");
+    CRT_CHECK(nimg > 0 && h > 0 && w > 0 && P < (1LL << 31), CRT_ERR_INVALID, "conv3x3: bad image size");
+    CRT_CHECK((reinterpret_cast<uintptr_t>(in) & 15) == 0 && (reinterpret_cast<uintptr_t>(wgt) & 15) == 0,
+              CRT_ERR_INVALID, "conv3x3: input and weights must be 16-byte aligned");
+    CRT_CHECK((!out || (reinterpret_cast<uintptr_t>(out) & 15) == 0) &&
+                  (!out_f32 || (reinterpret_cast<uintptr_t>(out_f32) & 3) == 0) &&
+                  (!mask || (reinterpret_cast<uintptr_t>(mask) & 15) == 0),
+              CRT_ERR_INVALID, "conv3x3: output and mask must be 16-byte aligned");
     ConvArgs a;
-    a.in = in;
-    a.wgt = wgt;
     a.bias = bias;
     a.mask = mask;
     a.out = out;
@@ -450,43 +500,71 @@ void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const flo
     a.N = N;
     a.flip = flip ? 1 : 0;
     a.relu = relu ? 1 : 0;
-    // Weights resident in shared memory when they fit next to 4 or 5 halo
-    // stages, else streamed per stage with 3 or 4 stages; the largest
-    // channel chunk KC of 64, 32, 16 dividing C that fits wins, then the
-    // deeper pipeline.
-    const size_t kSmemCap = 220 * 1024;
-    const size_t wbytes = (size_t)9 * N * C * 2;
-    auto a_stage = [&](int kc) { return (size_t)kc * 3 * kHalo * 2; };
-    bool resident = false;
-    int stages = 0;
+    // Tile: 256 pixels (one MMA of N = 256) unless the image is at most 128
+    // wide or there are more than 128 output channels (two 128-row M
+    // blocks; the TMEM then holds 2 slots x 2 x 128 columns).
+    a.MB = N > 128 ? 2 : 1;
+    a.M = N <= 64 ? 64 : 128;  // M = 64 spreads the channels over all four TMEM lane quarters
+    a.NP = (a.MB == 2 || w <= 128) ? 128 : 256;
+    // Channel chunk: row bytes RB = 2 KC of 128, 64 or 32 (the TMA swizzle
+    // span). Weights resident in shared memory when they fit next to at
+    // least 3 stages (widest chunk first, then the deepest pipeline), else
+    // streamed with every stage.
+    const size_t kCap = 220 * 1024 - 1024 - 2048 - 8192;  // minus base alignment, over-read pad, epilogue staging
+    const size_t wbytes = round1k((size_t)9 * N * C * 2);
+    auto region = [&](int rb) { return round1k((size_t)(a.NP + 2) * rb); };
     a.KC = 0;
-    for (int kc : {64, 32, 16})
-        for (int ns : {5, 4})
-            if (!a.KC && C % kc == 0 && wbytes + ns * a_stage(kc) <= kSmemCap) {
-                a.KC = kc;
-                stages = ns;
-                resident = true;
+    a.stages = 0;
+    a.resident = 0;
+    for (int rb : {128, 64, 32})
+        for (int ns : {5, 4, 3})
+            if (!a.KC && C % (rb / 2) == 0 && wbytes + ns * 3 * region(rb) <= kCap) {
+                a.KC = rb / 2;
+                a.stages = ns;
+                a.resident = 1;
             }
-    for (int kc : {64, 32, 16})
+    for (int rb : {128, 64, 32})
         for (int ns : {4, 3})
-            if (!a.KC && C % kc == 0 && ns * (a_stage(kc) + (size_t)18 * N * kc) <= kSmemCap) {
-                a.KC = kc;
-                stages = ns;
+            if (!a.KC && C % (rb / 2) == 0 &&
+                ns * (3 * region(rb) + round1k((size_t)(rb / 16) * 9 * N * 16)) <= kCap) {
+                a.KC = rb / 2;
+                a.stages = ns;
             }
     CRT_CHECK(a.KC > 0, CRT_ERR_INVALID, "conv3x3: tile does not fit shared memory");
-    const size_t smem = resident ? wbytes + stages * a_stage(a.KC) : stages * (a_stage(a.KC) + (size_t)18 * N * a.KC);
-    const void *kfn = resident ? (stages == 5 ? (const void *)k_conv3x3<5, true> : (const void *)k_conv3x3<4, true>)
-                               : (stages == 4 ? (const void *)k_conv3x3<4, false> : (const void *)k_conv3x3<3, false>);
+    a.RB = 2 * a.KC;
+    a.region_bytes = (uint32_t)region(a.RB);
+    a.wchunk_bytes = (uint32_t)((a.KC / 8) * 9 * N * 16);
+    a.stage_bytes = (uint32_t)(3 * a.region_bytes + (a.resident ? 0 : round1k(a.wchunk_bytes)));
+    a.wres_bytes = a.resident ? (uint32_t)round1k((size_t)(C / a.KC) * a.wchunk_bytes) : 0u;
+    const size_t smem = 1024 + a.wres_bytes + (size_t)a.stages * a.stage_bytes + 2048;
+
+    // input [nimg][h][w][C] as 4D (C, w, h, nimg); weights [9][N][C] as 3D (C, N, 9)
+    CUtensorMap map_in, map_edge, map_w;
+    const CUtensorMapSwizzle swz = a.RB == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                   : a.RB == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                                : CU_TENSOR_MAP_SWIZZLE_32B;
+    const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)nimg};
+    const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)w * C * 2, (cuuint64_t)h * w * C * 2};
+    const cuuint32_t box[4] = {(cuuint32_t)a.KC, (cuuint32_t)a.NP, 1, 1};
+    const cuuint32_t box_edge[4] = {(cuuint32_t)a.KC, 2, 1, 1};
+    encode_map(&map_in, in, 4, dims, strides, box, swz);
+    encode_map(&map_edge, in, 4, dims, strides, box_edge, swz);
+    const cuuint64_t wdims[3] = {(cuuint64_t)C, (cuuint64_t)N, 9};
+    const cuuint64_t wstrides[2] = {(cuuint64_t)C * 2, (cuuint64_t)N * C * 2};
+    const cuuint32_t wbox[3] = {8, (cuuint32_t)N, 9};
+    encode_map(&map_w, wgt, 3, wdims, wstrides, wbox, CU_TENSOR_MAP_SWIZZLE_NONE);
+
+    using Kfn = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, ConvArgs);
+    const Kfn kfns[2][3] = {{k_conv3x3<1, 1>, k_conv3x3<2, 1>, k_conv3x3<4, 1>},
+                            {k_conv3x3<1, 2>, k_conv3x3<2, 2>, k_conv3x3<4, 2>}};
+    const Kfn kfn = kfns[a.MB - 1][a.KC == 16 ? 0 : a.KC == 32 ? 1 : 2];
     CRT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kConvThreads, smem));
-    per_sm = std::max(1, std::min(per_sm, 512 / host_tmem_cols(2 * N)));
-    const int64_t padded = (int64_t)(w + 2) * (nimg * (int64_t)(h + 1) + 1);
-    CRT_CHECK(padded < (1LL << 31) - 4 * kBM, CRT_ERR_INVALID, "conv3x3: image too large");
-    const int64_t tiles = ((int64_t)(w + 2) * (nimg * (int64_t)(h + 1) - 1) + kBM - 1) / kBM;
+    CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kFwdThreads, smem));
+    per_sm = std::max(1, std::min(per_sm, 512 / host_tmem_cols(2 * a.MB * a.NP)));
+    const int64_t tiles = (int64_t)nimg * h * ((w + a.NP - 1) / a.NP);
     const int grid = (int)std::min<int64_t>(tiles, (int64_t)sm_count() * per_sm);
-    void *args[] = {&a};
-    CRT_CUDA(cudaLaunchKernel(kfn, dim3(grid), dim3(kConvThreads), args, smem, s));
+    kfn<<<grid, kFwdThreads, smem, s>>>(map_in, map_edge, map_w, a);
     CRT_CUDA(cudaGetLastError());
 }
 

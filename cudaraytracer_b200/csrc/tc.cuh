@@ -14,6 +14,7 @@
 // byte stride between groups of 8 K values; one K=16 MMA reads two K groups.
 #pragma once
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 namespace crt {
@@ -33,6 +34,22 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes,
     d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
     d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
     d |= (uint64_t)1u << 46;  // descriptor version
+    return d;
+}
+
+// Descriptor of a K-major operand in one of the swizzled layouts that TMA
+// writes (rows of `row_bytes` = 32, 64 or 128 B, 16 B chunks XOR-permuted
+// by address bits 7.. of the row): SBO = 8 rows, LBO unused, base offset 0.
+// The hardware swizzles on absolute shared-memory addresses, so the start
+// may sit any whole number of rows (and 32 B K-steps) into a swizzle atom.
+__device__ __forceinline__ uint64_t smem_desc_sw(uint32_t addr, uint32_t row_bytes) {
+    const uint64_t layout = row_bytes == 128 ? 2 : row_bytes == 64 ? 4 : 6;
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1u << 16;
+    d |= (uint64_t)(((8 * row_bytes) >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= layout << 61;
     return d;
 }
 
@@ -59,6 +76,33 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
         "}\n" ::"r"(tmem_d),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+
+// The same, executed by a whole converged warp: one lane (elect.sync)
+// issues. Running the issue loop warp-uniformly lets the compiler keep the
+// descriptors in uniform registers; a loop under `if (lane == 0)` pays
+// register moves per MMA and issues far slower.
+__device__ __forceinline__ void mma_bf16_warp(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                              bool accumulate) {
+    const uint32_t acc = accumulate ? 1u : 0u, z = 0u;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p, e;\n\t"
+        "elect.sync _|e, 0xffffffff;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit_warp(uint32_t mbar) {
+    asm volatile(
+        "{\n\t"
+        ".reg .pred e;\n\t"
+        "elect.sync _|e, 0xffffffff;\n\t"
+        "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t"
+        "}\n" ::"r"(mbar)
         : "memory");
 }
 
@@ -137,6 +181,14 @@ __device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, uint32_t parit
     return false;
 }
 
+// Warp-uniform form of mbar_wait_or_abort for a converged warp: lane 0's
+// outcome is everyone's.
+__device__ __forceinline__ bool mbar_wait_or_abort_warp(uint64_t *bar, uint32_t parity, volatile int *abort) {
+    bool ok = false;
+    if ((threadIdx.x & 31) == 0) ok = mbar_wait_or_abort(bar, parity, abort);
+    return __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+}
+
 // Plain arrive (release at CTA scope) by this thread.
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile(
@@ -144,6 +196,37 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
         ".reg .b64 st;\n\t"
         "mbarrier.arrive.shared::cta.b64 st, [%0];\n\t"
         "}\n" ::"r"(smem_addr(bar))
+        : "memory");
+}
+
+// Arrive and add `bytes` to the transaction count the phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile(
+        "{\n\t"
+        ".reg .b64 st;\n\t"
+        "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t"
+        "}\n" ::"r"(smem_addr(bar)),
+        "r"(bytes)
+        : "memory");
+}
+
+// TMA tiled loads (no multicast) into this CTA's shared memory; completion
+// is signalled as transaction bytes on the mbarrier. Coordinates are
+// elements, innermost first; out-of-bounds elements are filled with zeros.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
         : "memory");
 }
 
