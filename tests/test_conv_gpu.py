@@ -16,6 +16,10 @@ CASES = [  # n, h, w, cin, cout
     (1, 12, 13, 160, 64),
     (1, 9, 11, 64, 16),
     (3, 7, 5, 32, 160),
+    # wider than 256: 256-pixel tiles, the last x tile partial
+    (1, 6, 300, 64, 64),    # row ring, one 128 B channel chunk
+    (2, 5, 520, 32, 96),    # row ring, two images, three x tiles
+    (1, 4, 280, 96, 64),    # three-row stages with resident weights
 ]
 
 
