@@ -405,6 +405,203 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
     if (warp == 1) tc::tmem_dealloc(tmem, ncols);
 }
 
+// ---- weight gradient on the row ring ----
+//
+// dW[t][n][c] += sum_p in[p + off(t)][c] * g[p][n] as one GEMM per CTA with
+// rows (tap, channel), columns n and K = the CTA's pixels, accumulated in
+// TMEM over its whole contiguous range of row tiles (same order as the
+// forward's ring mode: consecutive rows of one column strip).
+// A = the input rows of the ring, read MN-major: a 128-row block is the
+// channel chunk (KC channels per 2 KC-byte swizzled row) of 128 / KC
+// dx-adjacent taps of one input row; consecutive taps are the same rows
+// shifted by one pixel, i.e. MN groups one row apart (LBO = one row). Taps
+// past the third and channels past C fill the block's spare rows; their
+// results are not read. B = the output gradient tile (NP pixels x N
+// channels, TMA-loaded, MN-major). Blocks of one CTA group: TMEM holds
+// (blocks per group) x N columns; with more blocks than fit, the grid is
+// split into groups that each accumulate a subset and read all inputs.
+struct WgradRingArgs {
+    float *dw;  // [9][N][C], accumulated
+    int *err;
+    int nimg, h, wd, C, N;
+    int NP, R;  // pixels per tile, ring rows
+    int G, blocks_per_group, total_blocks;
+    uint32_t region_bytes, row_bytes;     // input: one channel chunk of a ring row, one ring row
+    uint32_t gregion_bytes, gtile_bytes;  // gradient: one channel group of a tile, one tile
+};
+
+template <int kKS, int kGS>  // input chunk KC = 16 kKS, gradient channel group 16 kGS
+__global__ void __launch_bounds__(kFwdThreads, 1)
+    k_conv3x3_wgrad_ring(const __grid_constant__ CUtensorMap map_in, const __grid_constant__ CUtensorMap map_edge,
+                         const __grid_constant__ CUtensorMap map_g, WgradRingArgs a) {
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ uint64_t full[kMaxStages], empty[kMaxStages], gfull[2], gempty[2], mma_done;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag, mma_pace;
+    constexpr int KC = 16 * kKS, RB = 2 * KC, GKC = 16 * kGS, RBG = 2 * GKC;
+    constexpr int TPB = KC == 64 ? 2 : 3;  // valid taps (dx) per 128-row block
+    constexpr int BPD = KC == 64 ? 2 : 1;  // blocks per (input row, channel chunk)
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int C = a.C, N = a.N, W = a.wd, H = a.h, NP = a.NP, S = a.R;
+    const int chunks = C / KC, ggroups = N / GKC;
+    const int ntx = (W + NP - 1) / NP, ntiles = a.nimg * H * ntx;
+    const int grp = blockIdx.x % a.G, ctas = gridDim.x / a.G, ci = blockIdx.x / a.G;
+    const int b_beg = grp * a.blocks_per_group, b_end = min(a.total_blocks, b_beg + a.blocks_per_group);
+    const int t_beg = (int)((int64_t)ntiles * ci / ctas);
+    const int my_tiles = (int)((int64_t)ntiles * (ci + 1) / ctas) - t_beg;
+    const uint32_t ncols = tmem_cols(a.blocks_per_group * N);
+    unsigned char *const base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    unsigned char *const ring = base;
+    unsigned char *const gbuf = base + (size_t)S * a.row_bytes;
+    auto tile_of = [&](int tl, int &b, int &y, int &x0) {
+        const int t = t_beg + tl, r2 = t / H;
+        y = t - r2 * H;
+        x0 = (r2 % ntx) * NP;
+        b = r2 / ntx;
+    };
+    volatile int *abort = &abort_flag;
+
+    if (tid == 0) {
+        for (int i = 0; i < S; ++i) {
+            tc::mbar_init(&full[i], 1);
+            tc::mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&gfull[i], 1);
+            tc::mbar_init(&gempty[i], 1);
+        }
+        tc::mbar_init(&mma_done, 1);
+        abort_flag = 0;
+        mma_pace = 0;
+        tc::fence_mbar_init();
+    }
+    if (warp == 1) tc::tmem_alloc(&tmem_slot, ncols);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer: ring rows (as the forward's ring mode) and
+            // one gradient tile per row tile (two buffers) ----
+            const uint32_t tx_row = (uint32_t)chunks * (NP + 2) * RB, tx_g = (uint32_t)ggroups * NP * RBG;
+            int s = 0, tl = 0;
+            for (; tl < my_tiles && !*abort; ++tl) {
+                int b, y, x0;
+                tile_of(tl, b, y, x0);
+                const bool seg = tl == 0 || y == 0;
+                bool ok = true;
+                for (int yy = seg ? y - 1 : y + 1; yy <= y + 1; ++yy, ++s) {
+                    const int st = s % S;
+                    if (s >= S && !tc::mbar_wait_or_abort(&empty[st], ((s / S) - 1) & 1, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char *sa = ring + (size_t)st * a.row_bytes;
+                    tc::mbar_arrive_expect_tx(&full[st], tx_row);
+                    for (int ch = 0; ch < chunks; ++ch) {
+                        tc::tma_load_4d(sa + ch * a.region_bytes, &map_in, ch * KC, x0 - 1, yy, b, &full[st]);
+                        tc::tma_load_4d(sa + ch * a.region_bytes + NP * RB, &map_edge, ch * KC, x0 - 1 + NP, yy, b,
+                                        &full[st]);
+                    }
+                }
+                if (!ok) break;
+                const int gs = tl & 1;
+                if (tl >= 2 && !tc::mbar_wait_or_abort(&gempty[gs], ((tl >> 1) - 1) & 1, abort)) break;
+                unsigned char *gb = gbuf + (size_t)gs * a.gtile_bytes;
+                tc::mbar_arrive_expect_tx(&gfull[gs], tx_g);
+                for (int gg = 0; gg < ggroups; ++gg)
+                    tc::tma_load_4d(gb + gg * a.gregion_bytes, &map_g, gg * GKC, x0, y, b, &gfull[gs]);
+                // (a break above leaves this tile's gradient unissued: tl is
+                // then not counted below)
+            }
+            // no TMA write may land after the CTA has exited
+            for (int st = 0; st < S && st < s; ++st) {
+                const int last = s - 1 - ((s - 1 - st) % S);
+                tc::mbar_wait(&full[st], (last / S) & 1);
+            }
+            for (int t2 = tl > 2 ? tl - 2 : 0; t2 < tl; ++t2) tc::mbar_wait(&gfull[t2 & 1], (t2 >> 1) & 1);
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer (whole warp, one elected lane issues) ----
+        const uint32_t idesc = tc::idesc_bf16(128, N, true, true);
+        const uint32_t ring_addr = tc::smem_addr(ring), gbuf_addr = tc::smem_addr(gbuf);
+        const int ksteps = NP / 16;
+        int s = 0, top = 0;
+        bool run = true;
+        for (int tl = 0; tl < my_tiles && run; ++tl) {
+            int b, y, x0;
+            tile_of(tl, b, y, x0);
+            if (tl == 0 || y == 0) {
+                top = s;
+                s += 3;
+            } else {
+                top += 1;
+                s += 1;
+            }
+            const int gs = tl & 1;
+            if (!tc::mbar_wait_or_abort_warp(&gfull[gs], (tl >> 1) & 1, abort)) break;
+            tc::fence_after_sync();
+            const uint64_t bd0 = tc::smem_desc_sw(gbuf_addr + gs * a.gtile_bytes, RBG, a.gregion_bytes);
+            for (int ri = 0; ri < 3 && run; ++ri) {
+                const int ld = top + ri, st = ld % S;
+                if (!tc::mbar_wait_or_abort_warp(&full[st], (ld / S) & 1, abort)) {
+                    run = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                for (int ch = 0; ch < chunks; ++ch)
+#pragma unroll
+                    for (int bb = 0; bb < BPD; ++bb) {
+                        const int blk = (ri * chunks + ch) * BPD + bb;
+                        if (blk < b_beg || blk >= b_end) continue;
+                        const uint32_t d = tmem + (uint32_t)(blk - b_beg) * N;
+                        const uint64_t ad0 = tc::smem_desc_sw(
+                            ring_addr + st * a.row_bytes + ch * a.region_bytes + bb * TPB * RB, RB, RB);
+                        for (int kk = 0; kk < ksteps; ++kk)
+                            tc::mma_bf16_warp(d, ad0 + ((kk * 16 * RB) >> 4), bd0 + ((kk * 16 * RBG) >> 4), idesc,
+                                              tl > 0 || kk > 0);
+                    }
+                if (lane == 0) atomicAdd(&mma_pace, 1);  // see k_conv3x3's ring loop
+            }
+            if (!run) break;
+            const bool strip_ends = tl + 1 == my_tiles || y + 1 == H;
+            for (int r = 0; r < (strip_ends ? 3 : 1); ++r) tc::mma_commit_warp(tc::smem_addr(&empty[(top + r) % S]));
+            tc::mma_commit_warp(tc::smem_addr(&gempty[gs]));
+        }
+        tc::mma_commit_warp(tc::smem_addr(&mma_done));
+        if (lane == 0) tc::mbar_wait(&mma_done, 0);
+        __syncwarp();
+    } else {
+        // ---- epilogue: add the accumulators into dW ----
+        const int q = warp & 3, half = (warp - 2) >> 2, r = q * 32 + lane;
+        const bool ok = tc::mbar_wait_or_abort(&mma_done, 0, abort);
+        tc::fence_after_sync();
+        if (ok && my_tiles > 0 && !*abort)
+            for (int blk = b_beg + half; blk < b_end; blk += 2) {
+                const int bb = blk % BPD, rc = blk / BPD, ch = rc % chunks, ri = rc / chunks;
+                const int gtap = bb * TPB + r / KC, c = ch * KC + r % KC;
+                const bool valid = r / KC < TPB && gtap < 3;
+                const int t = ri * 3 + gtap;
+                const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(blk - b_beg) * N;
+                for (int n0 = 0; n0 < N; n0 += 16) {
+                    float v[16];
+                    tc::tmem_ld16(taddr + n0, v);
+                    if (valid)
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) atomicAdd(a.dw + ((size_t)t * N + n0 + i) * C + c, v[i]);
+                }
+            }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (tid == 0 && abort_flag) atomicExch(a.err, 1);
+    if (warp == 1) tc::tmem_dealloc(tmem, ncols);
+}
+
 struct WgradArgs {
     const __nv_bfloat16 *in;   // [P][C] layer input
     const __nv_bfloat16 *g;    // [P][N] gradient of the layer's pre-activation output
@@ -690,11 +887,76 @@ void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const flo
 
 // dw[9][N][C] += weight gradient of a 3x3 conv with input `in` [P][C] and
 // pre-activation output gradient `g` [P][N].
+namespace {
+// Weight gradient on the row ring when the ring and two gradient tiles fit
+// in shared memory; returns false (nothing launched) otherwise.
+bool wgrad_ring_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *g, float *dw, int *err, int nimg, int h, int w,
+                       int C, int N, cudaStream_t s) {
+    if ((reinterpret_cast<uintptr_t>(in) & 15) || (reinterpret_cast<uintptr_t>(g) & 15)) return false;
+    const int KC = C % 64 == 0 ? 64 : C % 32 == 0 ? 32 : 16, GKC = N % 64 == 0 ? 64 : N % 32 == 0 ? 32 : 16;
+    const int RB = 2 * KC, RBG = 2 * GKC;
+    WgradRingArgs a;
+    a.dw = dw;
+    a.err = err;
+    a.nimg = nimg;
+    a.h = h;
+    a.wd = w;
+    a.C = C;
+    a.N = N;
+    a.total_blocks = 3 * (C / KC) * (KC == 64 ? 2 : 1);
+    a.blocks_per_group = std::min(a.total_blocks, 512 / N);
+    a.G = (a.total_blocks + a.blocks_per_group - 1) / a.blocks_per_group;
+    const size_t kCap = 220 * 1024 - 1024;
+    a.NP = 0;
+    for (int np : {256, 128}) {
+        if (a.NP || (np == 256 && w <= 128)) continue;
+        const size_t region = round1k((size_t)(np + 2) * RB), row = (size_t)(C / KC) * region;
+        const size_t gregion = round1k((size_t)np * RBG), gtile = (size_t)(N / GKC) * gregion;
+        for (int ns : {5, 4})
+            if (!a.NP && ns * row + 2 * gtile <= kCap) {
+                a.NP = np;
+                a.R = ns;
+                a.region_bytes = (uint32_t)region;
+                a.row_bytes = (uint32_t)row;
+                a.gregion_bytes = (uint32_t)gregion;
+                a.gtile_bytes = (uint32_t)gtile;
+            }
+    }
+    if (!a.NP) return false;
+    const size_t smem = 1024 + (size_t)a.R * a.row_bytes + 2 * (size_t)a.gtile_bytes;
+    CUtensorMap map_in, map_edge, map_g;
+    auto swz = [](int rb) {
+        return rb == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : rb == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
+    };
+    const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)nimg};
+    const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)w * C * 2, (cuuint64_t)h * w * C * 2};
+    const cuuint32_t box[4] = {(cuuint32_t)KC, (cuuint32_t)a.NP, 1, 1}, box_edge[4] = {(cuuint32_t)KC, 2, 1, 1};
+    encode_map(&map_in, in, 4, dims, strides, box, swz(RB));
+    encode_map(&map_edge, in, 4, dims, strides, box_edge, swz(RB));
+    const cuuint64_t gdims[4] = {(cuuint64_t)N, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)nimg};
+    const cuuint64_t gstrides[3] = {(cuuint64_t)N * 2, (cuuint64_t)w * N * 2, (cuuint64_t)h * w * N * 2};
+    const cuuint32_t gbox[4] = {(cuuint32_t)GKC, (cuuint32_t)a.NP, 1, 1};
+    encode_map(&map_g, g, 4, gdims, gstrides, gbox, swz(RBG));
+    using Kfn = void (*)(CUtensorMap, CUtensorMap, CUtensorMap, WgradRingArgs);
+    const Kfn kfns[3][3] = {{k_conv3x3_wgrad_ring<1, 1>, k_conv3x3_wgrad_ring<1, 2>, k_conv3x3_wgrad_ring<1, 4>},
+                            {k_conv3x3_wgrad_ring<2, 1>, k_conv3x3_wgrad_ring<2, 2>, k_conv3x3_wgrad_ring<2, 4>},
+                            {k_conv3x3_wgrad_ring<4, 1>, k_conv3x3_wgrad_ring<4, 2>, k_conv3x3_wgrad_ring<4, 4>}};
+    const Kfn kfn = kfns[KC == 16 ? 0 : KC == 32 ? 1 : 2][GKC == 16 ? 0 : GKC == 32 ? 1 : 2];
+    CRT_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t tiles = (int64_t)nimg * h * ((w + a.NP - 1) / a.NP);
+    const int ctas = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, sm_count() / a.G > 0 ? sm_count() / a.G : 1));
+    kfn<<<ctas * a.G, kFwdThreads, smem, s>>>(map_in, map_edge, map_g, a);
+    CRT_CUDA(cudaGetLastError());
+    return true;
+}
+}  // namespace
+
 void conv3x3_wgrad_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *g, float *dw, int *err, int nimg, int h, int w,
                           int C, int N, cudaStream_t s) {
     conv3x3_check(C, N);
     const int64_t P = (int64_t)nimg * h * w;
     CRT_CHECK(P > 0 && P < (1LL << 31) - kWgradBK, CRT_ERR_INVALID, "conv3x3_wgrad: bad image size");
+    if (wgrad_ring_launch(in, g, dw, err, nimg, h, w, C, N, s)) return;
     WgradArgs a;
     a.in = in;
     a.g = g;

@@ -42,11 +42,14 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes,
 // by address bits 7.. of the row): SBO = 8 rows, LBO unused, base offset 0.
 // The hardware swizzles on absolute shared-memory addresses, so the start
 // may sit any whole number of rows (and 32 B K-steps) into a swizzle atom.
-__device__ __forceinline__ uint64_t smem_desc_sw(uint32_t addr, uint32_t row_bytes) {
+// For an MN-major operand in the same layouts (rows of the K dimension, each
+// holding row_bytes of consecutive M or N elements), lbo_bytes is the stride
+// between such groups of M / N elements.
+__device__ __forceinline__ uint64_t smem_desc_sw(uint32_t addr, uint32_t row_bytes, uint32_t lbo_bytes = 16) {
     const uint64_t layout = row_bytes == 128 ? 2 : row_bytes == 64 ? 4 : 6;
     uint64_t d = 0;
     d |= (uint64_t)((addr >> 4) & 0x3FFFu);
-    d |= (uint64_t)1u << 16;
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
     d |= (uint64_t)(((8 * row_bytes) >> 4) & 0x3FFFu) << 32;
     d |= (uint64_t)1u << 46;
     d |= layout << 61;
