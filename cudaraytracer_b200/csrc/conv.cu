@@ -838,7 +838,7 @@ void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const flo
                 a.resident = 1;
             }
     for (int rb : {128, 64, 32})
-        for (int ns : {4, 3})
+        for (int ns : {4, 3, 2})  // two stages only for the widest layers (256 output channels)
             if (!a.KC && C % (rb / 2) == 0 &&
                 ns * (3 * region(rb) + round1k((size_t)(rb / 16) * 9 * N * 16)) <= kCap) {
                 a.KC = rb / 2;

@@ -20,6 +20,10 @@ CASES = [  # n, h, w, cin, cout
     (1, 6, 300, 64, 64),    # row ring, one 128 B channel chunk
     (2, 5, 520, 32, 96),    # row ring, two images, three x tiles
     (1, 4, 280, 96, 64),    # three-row stages with resident weights
+    # smallest images and the channel limits
+    (1, 1, 1, 16, 16),
+    (4, 2, 3, 16, 32),
+    (1, 3, 20, 256, 256),   # weights streamed with the stages, two 128-row M blocks
 ]
 
 
@@ -73,6 +77,19 @@ def test_conv3x3_forward_and_gradients(crt_ctx, n, h, w, cin, cout):
     ref_gw = K.conv3x3_backward_weights(x, g)
     bound_gw = K.conv3x3_backward_weights(np.abs(x), np.abs(g))
     assert np.all(np.abs(from_dev(gw) - ref_gw) <= 2e-5 * bound_gw + 1e-6)
+
+
+def test_forward_512_input_channels(crt_ctx):
+    """The widest input accepted (512 channels): streamed weights, two-stage pipeline."""
+    from cudaraytracer_b200 import kpcn
+
+    rng = np.random.default_rng(512)
+    x = K.bf16_round(rng.normal(size=(1, 3, 20, 512)).astype(np.float32))
+    wt = K.bf16_round((rng.normal(size=(9, 256, 512)) / np.sqrt(9 * 512)).astype(np.float32))
+    out = kpcn.conv3x3_forward(crt_ctx, to_dev(x, "bf16"), to_dev(wt, "bf16"))
+    ref = K.conv3x3_forward(x, wt)
+    bound = K.conv3x3_forward(np.abs(x), np.abs(wt))
+    assert np.all(np.abs(from_dev(out) - ref) <= 2e-5 * bound + 1e-6 + np.abs(ref) * 2.0 ** -8)
 
 
 def test_weight_gradient_accumulates(crt_ctx):
