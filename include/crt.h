@@ -416,9 +416,14 @@ crt_status crt_trace_shadow_device(crt_scene *scene, const crt_shadow_query *d_q
 /* No reference counterpart: the dense contractions of the kernel-predicting
  * denoiser, as BF16 x BF16 -> FP32 implicit GEMMs on the sm_100a tensor cores
  * (tcgen05). Activations are NHWC BF16 (bit patterns as uint16), n images of
- * h x w pixels; channel counts are multiples of 16 (cout in [16, 256]);
- * stride 1, zero padding 1; tap t = 3 * (dy + 1) + (dx + 1). All
- * asynchronous on `stream` (NULL = the context stream). */
+ * h x w pixels; channel counts are multiples of 16 (input channels up to
+ * 512, output channels in [16, 256]; the data gradient's output is the
+ * forward's input, so it takes cin <= 256); stride 1, zero padding 1; tap
+ * t = 3 * (dy + 1) + (dx + 1). Activation, weight, mask and BF16 output
+ * buffers are 16-byte aligned (the kernels read them with TMA and store
+ * 16 B vectors); FP32 outputs 4-byte aligned; other alignments are refused
+ * with CRT_ERR_INVALID. All asynchronous on `stream` (NULL = the context
+ * stream). */
 /* out[p, o] = bias[o] + sum_{t, c} in[p + off(t), c] * w[t][o][c], ReLU if
  * relu != 0; written as BF16 (d_out_bf16) and/or FP32 (d_out_f32). */
 crt_status crt_conv3x3_forward(crt_ctx *ctx, const void *d_in, int32_t n, int32_t h, int32_t w, int32_t cin,
