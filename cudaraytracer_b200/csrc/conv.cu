@@ -837,9 +837,11 @@ void conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *wgt, const flo
                 a.stages = ns;
                 a.resident = 1;
             }
-    for (int rb : {128, 64, 32})
-        for (int ns : {4, 3, 2})  // two stages only for the widest layers (256 output channels)
-            if (!a.KC && C % (rb / 2) == 0 &&
+    // (a pipeline of 3 or 4 stages at any chunk width first: the streamed
+    // weights dominate a stage; two stages only for the widest layers)
+    for (int ns : {4, 3, 2})
+        for (int rb : {128, 64, 32})
+            if (!a.KC && (ns >= 3 || rb == 32) && C % (rb / 2) == 0 &&
                 ns * (3 * region(rb) + round1k((size_t)(rb / 16) * 9 * N * 16)) <= kCap) {
                 a.KC = rb / 2;
                 a.stages = ns;
