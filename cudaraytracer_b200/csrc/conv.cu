@@ -3,25 +3,26 @@
 // BF16 -> FP32 in TMEM). These are the dense contractions of the learned
 // kernel-predicting denoiser (kpcn.cu); the reference has no learned part.
 //
-// Forward and data gradient share one kernel: output pixel tile (M = 128
-// pixels) x all output channels (N), K = 9 taps x C input channels.
 //   forward : out[p, n] = sum_{t, c} in[p + off(t), c] * w[t][n][c]
 //   data grad: out[p, n] = sum_{t, c} g[p - off(t), c] * wt[t][n][c]
 //             (wt = w transposed per tap, flip = 1)
-// The input is staged per (tile, channel chunk) as three halo regions with
-// 16 B cp.async copies (zero-filled outside the image) in the K-major
-// core-matrix layout of tc.cuh; every tap's A operand is a shifted
-// descriptor into them, B the tap's weight slice (resident in shared memory
-// when the layer's weights fit). Producer warps, one MMA-issuing thread and
-// epilogue warps hand stages and the two TMEM accumulator slots to each
-// other through mbarriers, so copies, MMAs and the epilogue of the previous
-// tile overlap. The epilogue reads the FP32 accumulators from TMEM (one
-// pixel per thread) and applies bias + ReLU (forward) or the ReLU mask of
-// the layer below (data gradient), writing BF16 (or FP32) NHWC.
+//   weights  : dW[t][n][c] += sum_p in[p + off(t), c] * g[p, n]
 //
-// The weight gradient is a second kernel: rows M = (tap, c) (9C rows in
-// 128-row tiles), columns N = output channels, K = pixels split across
-// CTAs; both operands MN-major, partial sums added to FP32 dW with atomics.
+// Three kernels:
+//   k_conv3x3             forward and data gradient: output channels as the
+//                         MMA's M, 256 (or 128) pixels of one image row as
+//                         its N; input rows TMA-loaded in swizzled layouts,
+//                         the 9 taps as row-shifted descriptors; a ring of
+//                         input rows per column strip (ring mode) or
+//                         three-row stages per tile (step mode, weights
+//                         resident or streamed).
+//   k_conv3x3_wgrad_ring  weight gradient on the same row ring, MN-major,
+//                         accumulators resident in TMEM over each CTA's
+//                         pixel range.
+//   k_conv3x3_wgrad       weight gradient for layers whose ring does not fit
+//                         shared memory: (tap, channel) row tiles x output
+//                         channels, pixels split over CTAs, cp.async-staged
+//                         MN-major operands, FP32 atomics into dW.
 #include "api_internal.h"
 #include "tc.cuh"
 #include <algorithm>
@@ -31,12 +32,12 @@
 namespace crt {
 namespace {
 
-constexpr int kBM = 128;      // pixels (or (tap, c) rows) per tile
-constexpr int kThreads = 128;      // weight-gradient kernel
+constexpr int kBM = 128;           // k_conv3x3_wgrad: (tap, c) rows per tile
+constexpr int kThreads = 128;      // k_conv3x3_wgrad
 constexpr int kFwdThreads = 320;  // forward / data gradient: TMA warp, MMA warp, 8 epilogue warps
 constexpr int kMaxStages = 5;
-constexpr int kStages = 4;
-constexpr int kWgradBK = 64;  // pixels per weight-gradient K step
+constexpr int kStages = 4;         // k_conv3x3_wgrad pipeline depth
+constexpr int kWgradBK = 64;       // k_conv3x3_wgrad: pixels per K step
 
 struct ConvArgs {
     const float *bias;          // [N] or null
