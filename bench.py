@@ -227,7 +227,7 @@ def batch_leg(ctx, stream):
     """Batched persistent wavefront (survey config C3): 64 orbit views of
     the Cornell box (radius 3, elevation U[-30, 30] deg, seeded), 512x512,
     16 spp, depth 12, all views in shared wavefronts with a CUDA graph per
-    pass and an autotuned wavefront size, against 64 sequential single-view
+    pass and an autotuned wavefront size and stage block size, against 64 sequential single-view
     renders of the same cameras."""
     import tempfile
 
@@ -266,7 +266,8 @@ def batch_leg(ctx, stream):
             "sequential_ms": round(sms, 2), "speedup": round(sms / bms, 3),
             "batched_msamples_per_s": round(samples / (bms * 1e-3) / 1e6, 1),
             "sequential_msamples_per_s": round(samples / (sms * 1e-3) / 1e6, 1),
-            "paths_per_pass": tune["paths_per_pass"], "autotune_ms": tune.get("timings_ms")}
+            "paths_per_pass": tune["paths_per_pass"], "stage_block": tune["stage_block"],
+            "autotune_ms": tune.get("timings_ms"), "autotune_block_ms": tune.get("block_timings_ms")}
 
 
 def serve_leg(ctx, quick=False):

@@ -68,6 +68,7 @@ class RenderParams(C.Structure):
         ("seed", C.c_uint64),
         ("spp_per_pass", C.c_int32),
         ("paths_per_pass", C.c_int32),
+        ("stage_block", C.c_int32),
     ]
 
 

@@ -1,9 +1,12 @@
 """Autotuner for the batched renderer: picks the wavefront size (paths per
-pass) of Scene.render_views by timing a short probe render of each
-candidate with CUDA events, and caches the choice in a JSON file keyed by
-GPU name, scene triangle count (power-of-two bucket), image size and view
-count. No counterpart in the reference (its wavefront is one frame of one
-view)."""
+pass, the queue capacity) and then the thread-block size of the
+extend/shade/shadow stage kernels for Scene.render_views, by timing a short
+probe render of each candidate with CUDA events, and caches the choice in a
+JSON file keyed by GPU name, scene triangle count (power-of-two bucket),
+image size and view count. The traversal stack depth (a compile-time array
+of 64 entries; only the entries a ray uses are touched) and the BVH node
+width (binary; a 4-wide collapse measured slower) are not tuned. No
+counterpart in the reference (its wavefront is one frame of one view)."""
 from __future__ import annotations
 
 import json
@@ -11,6 +14,7 @@ import math
 import os
 
 DEFAULT_CANDIDATES = (1 << 20, 2 << 20, 4 << 20, 8 << 20, 16 << 20)
+BLOCK_CANDIDATES = (64, 128, 256)
 
 
 def cache_key(scene, n_views: int) -> str:
@@ -24,10 +28,12 @@ def cache_key(scene, n_views: int) -> str:
 
 
 def autotune_paths_per_pass(scene, cameras, probe_spp: int = 1, candidates=DEFAULT_CANDIDATES,
-                            cache_path: str | None = None) -> dict:
+                            cache_path: str | None = None, blocks=BLOCK_CANDIDATES) -> dict:
     """Times render_views(cameras, probe_spp) for each candidate wavefront
-    size, sets the fastest on the scene and returns {"paths_per_pass",
-    "timings_ms", "cached"}."""
+    size (at the scene's current stage block size), then for each stage
+    block size at the fastest wavefront size; sets the winners on the scene
+    and returns {"paths_per_pass", "stage_block", "timings_ms",
+    "block_timings_ms", "cached"}."""
     import torch
 
     key = cache_key(scene, len(cameras))
@@ -35,19 +41,16 @@ def autotune_paths_per_pass(scene, cameras, probe_spp: int = 1, candidates=DEFAU
         with open(cache_path) as f:
             cache = json.load(f)
         if key in cache:
-            scene.set_render_params(paths_per_pass=int(cache[key]["paths_per_pass"]))
+            scene.set_render_params(paths_per_pass=int(cache[key]["paths_per_pass"]),
+                                    stage_block=int(cache[key].get("stage_block", 0)))
             return {**cache[key], "cached": True}
     rp = scene.render_params()
     shape = (len(cameras), rp["height"], rp["width"], 4)
     d = torch.zeros(shape, device="cuda")
     i = torch.zeros(shape, device="cuda")
     total = len(cameras) * rp["height"] * rp["width"] * probe_spp
-    timings = {}
-    for c in candidates:
-        c = int(min(c, max(total, 1)))
-        if c in timings:
-            continue
-        scene.set_render_params(paths_per_pass=c)
+
+    def probe_ms() -> float:
         scene.render_views(cameras, d, i, probe_spp)  # warm-up (allocation, capture)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -55,10 +58,26 @@ def autotune_paths_per_pass(scene, cameras, probe_spp: int = 1, candidates=DEFAU
         scene.render_views(cameras, d, i, probe_spp, first_sample=probe_spp)
         e1.record()
         torch.cuda.synchronize()
-        timings[c] = e0.elapsed_time(e1)
+        return e0.elapsed_time(e1)
+
+    timings = {}
+    for c in candidates:
+        c = int(min(c, max(total, 1)))
+        if c in timings:
+            continue
+        scene.set_render_params(paths_per_pass=c)
+        timings[c] = probe_ms()
     best = min(timings, key=timings.get)
     scene.set_render_params(paths_per_pass=best)
-    entry = {"paths_per_pass": best, "timings_ms": {str(k): round(v, 3) for k, v in timings.items()}}
+    block_timings = {}
+    for b in blocks:
+        scene.set_render_params(stage_block=int(b))
+        block_timings[int(b)] = probe_ms()
+    best_block = min(block_timings, key=block_timings.get)
+    scene.set_render_params(stage_block=best_block)
+    entry = {"paths_per_pass": best, "stage_block": best_block,
+             "timings_ms": {str(k): round(v, 3) for k, v in timings.items()},
+             "block_timings_ms": {str(k): round(v, 3) for k, v in block_timings.items()}}
     if cache_path:
         cache = {}
         if os.path.exists(cache_path):

@@ -445,6 +445,7 @@ crt_status crt_get_render_params(const crt_scene *scene, crt_render_params *p) {
         p->seed = scene->rp.seed;
         p->spp_per_pass = scene->rp.spp_per_pass;
         p->paths_per_pass = scene->rp.paths_per_pass;
+        p->stage_block = scene->rp.stage_block;
     });
 }
 
@@ -455,6 +456,8 @@ crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p) {
                   "crt_set_render_params: bad resolution");
         CRT_CHECK(p->spp >= 0 && p->max_bounces >= 0 && p->spp_per_pass >= 0 && p->paths_per_pass >= 0,
                   CRT_ERR_INVALID, "crt_set_render_params: negative count");
+        CRT_CHECK(p->stage_block == 0 || p->stage_block == 64 || p->stage_block == 128 || p->stage_block == 256,
+                  CRT_ERR_INVALID, "crt_set_render_params: stage_block must be 0, 64, 128 or 256");
         bool resized = p->width != scene->rp.width || p->height != scene->rp.height;
         scene->rp.width = p->width;
         scene->rp.height = p->height;
@@ -465,6 +468,7 @@ crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p) {
         scene->rp.seed = p->seed;
         scene->rp.spp_per_pass = p->spp_per_pass;
         scene->rp.paths_per_pass = p->paths_per_pass;
+        scene->rp.stage_block = p->stage_block;
         if (resized) {
             scene->cam.width = p->width;
             scene->cam.height = p->height;

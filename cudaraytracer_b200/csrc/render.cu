@@ -362,7 +362,7 @@ __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *co
 
 // Extend: closest hit of every live path (TraceRay, renderer.cuh:124-130:
 // tMin 0, closest starts at 1e8). Also clears the next bounce's counters.
-__global__ void __launch_bounds__(128) k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters,
+__global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters,
                                                 int out_idx) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         counters[out_idx] = 0;
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(128) k_extend(BvhView bvh, QueueView q, const 
     }
 }
 
-__global__ void __launch_bounds__(128) k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits,
+__global__ void __launch_bounds__(256) k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits,
                                                const int *n_in, QueueView qout, int *counters, int out_idx,
                                                ShadowView sh, float4 *term0, float4 *term1, AccumView acc) {
     const int n = *n_in;
@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(128) k_shade(SceneView s, StepParams sp, Queue
 // Shadow: Light::Visible for each deferred NEE sample; a visible sample's
 // contribution joins its path's direct or indirect radiance; a path that
 // already terminated is then added to its pixel.
-__global__ void __launch_bounds__(128) k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueView qout,
+__global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueView qout,
                                                 float4 *term0, float4 *term1, AccumView acc) {
     const int n = counters[2];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -507,9 +507,10 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
     for (int j = 0; j < 2; ++j)
         for (int k = 0; k < 5; ++k) q[j].p[k] = wf.q[j][k];
     ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
-    const int g_ext = persistent_grid((const void *)k_extend, 128);
-    const int g_sh = persistent_grid((const void *)k_shade, 128);
-    const int g_sd = persistent_grid((const void *)k_shadow, 128);
+    const int blk = rp.block();
+    const int g_ext = persistent_grid((const void *)k_extend, blk);
+    const int g_sh = persistent_grid((const void *)k_shade, blk);
+    const int g_sd = persistent_grid((const void *)k_shadow, blk);
     int launches = 0;
     for (int done = 0; done < spp; done += per_pass) {
         int s_here = std::min(per_pass, spp - done);
@@ -526,10 +527,10 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
         for (int b = 0; b < rp.max_bounces; ++b) {
             int in = b & 1, out = 1 - in;
             sp.bounce = b;
-            k_extend<<<g_ext, 128, 0, stream>>>(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out);
-            k_shade<<<g_sh, 128, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out], wf.counters, out, sh,
+            k_extend<<<g_ext, blk, 0, stream>>>(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out);
+            k_shade<<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out], wf.counters, out, sh,
                                               wf.term[0], wf.term[1], av);
-            k_shadow<<<g_sd, 128, 0, stream>>>(view.bvh, sh, wf.counters, q[out], wf.term[0], wf.term[1], av);
+            k_shadow<<<g_sd, blk, 0, stream>>>(view.bvh, sh, wf.counters, q[out], wf.term[0], wf.term[1], av);
             launches += 3;
         }
         CRT_CUDA(cudaGetLastError());

@@ -15,6 +15,8 @@ struct RenderParams {
     uint64_t seed = 1;
     int spp_per_pass = 0;     // samples per wavefront; 0 = automatic
     int paths_per_pass = 0;   // paths per wavefront of multi-view batches; 0 = 8M
+    int stage_block = 0;      // threads per block of the wavefront stage kernels; 0 = 128
+    int block() const { return stage_block ? stage_block : 128; }
 };
 
 // Device-resident render data of a scene (everything but the BVH).

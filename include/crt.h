@@ -198,6 +198,8 @@ typedef struct crt_render_params {
     uint64_t seed;            /* PCG32 seed of the per-path streams */
     int32_t spp_per_pass;     /* samples per wavefront of crt_render*; 0 = automatic */
     int32_t paths_per_pass;   /* paths per wavefront of crt_render_views; 0 = 8M */
+    int32_t stage_block;      /* threads per block of the extend/shade/shadow wavefront stages
+                                 (64, 128 or 256); 0 = 128 */
 } crt_render_params;
 
 crt_status crt_get_render_params(const crt_scene *scene, crt_render_params *p);

@@ -81,5 +81,27 @@ def test_autotuner_picks_and_caches(cornell, tmp_path):
     r = autotune_paths_per_pass(cornell, views, candidates=(1 << 14, 1 << 16), cache_path=cache)
     assert not r["cached"] and r["paths_per_pass"] in (1 << 14, 1 << 16)
     assert cornell.render_params()["paths_per_pass"] == r["paths_per_pass"]
+    assert r["stage_block"] in (64, 128, 256) and cornell.render_params()["stage_block"] == r["stage_block"]
     r2 = autotune_paths_per_pass(cornell, views, candidates=(1 << 14, 1 << 16), cache_path=cache)
     assert r2["cached"] and r2["paths_per_pass"] == r["paths_per_pass"]
+    assert r2["stage_block"] == r["stage_block"]
+
+
+def test_stage_block_size_does_not_change_the_image(cornell):
+    """The stage kernels' block size only changes scheduling: per-path work
+    is keyed by (seed, pixel, sample), so the frame is the same up to the
+    order of the accumulators' float additions."""
+    import pytest
+
+    from cudaraytracer_b200 import CrtError
+
+    frames = []
+    for b in (64, 256):
+        cornell.set_render_params(stage_block=b, seed=23)
+        d, i = cornell.render(4)
+        frames.append((d, i))
+    cornell.set_render_params(stage_block=0)
+    for a, b in zip(frames[0], frames[1]):
+        np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6)
+    with pytest.raises(CrtError):
+        cornell.set_render_params(stage_block=96)
