@@ -224,7 +224,7 @@ def render_leg(ctx, steps, stream, with_reference=True):
 
 
 def batch_leg(ctx, stream):
-    """Batched persistent wavefront (survey config C3): 64 orbit views of
+    """Batched persistent wavefront (the multi-view batch workload): 64 orbit views of
     the Cornell box (radius 3, elevation U[-30, 30] deg, seeded), 512x512,
     16 spp, depth 12, all views in shared wavefronts with a CUDA graph per
     pass and an autotuned wavefront size and stage block size, against 64 sequential single-view
@@ -271,7 +271,7 @@ def batch_leg(ctx, stream):
 
 
 def serve_leg(ctx, quick=False):
-    """Serving (survey config C4) on a bounded sample. 8 resident scenes of
+    """Serving (the multi-scene request workload) on a bounded sample. 8 resident scenes of
     the icosphere-field generator with {1, 4, 8, 16, 32, 64, 128, 256}
     level-5 spheres (20k to 5.2M triangles, 2048x1024 env each). Requests
     draw resolution from {256^2, 512^2, 1280x720, 1920x1080}, spp from
@@ -366,7 +366,7 @@ def conv_leg(ctx, h=1080, w=1920, cin=64, cout=64, reps=10):
 
 
 def denoise_leg(ctx):
-    """Learned denoiser (survey config C5 on a bounded sample): the KPCN is
+    """Learned denoiser (the learned-denoiser workload on a bounded sample): the KPCN is
     trained on the GPU on 64 views of seeded Cornell variants (scene seeds
     100-131, 256x256, 1-16 spp inputs, 1024-spp references) for 1500 Adam
     steps of 8 random 128x128 crops, then evaluated on unseen scenes (seeds
