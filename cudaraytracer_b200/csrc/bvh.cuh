@@ -97,6 +97,21 @@ __device__ __forceinline__ bool slab(float lox, float hix, float loy, float hiy,
 // accepted on [0, 1e8] with closest initialised to tmax. When t_exit > 0 the
 // traversal stops at the first accepted hit with t < t_exit (used by the
 // shadow predicate, whose answer is fixed once such a hit exists).
+// One 64 B interior node (child boxes n0, n1 and n2.xy / n2.zw, child links
+// n3.xy) as two 32 B read-only loads: nodes sit 64 B apart from a 256 B-
+// aligned allocation. Measured 1.3-1.5% faster than four 16 B loads in the
+// standalone extend and shadow kernels (traverse.cuh), with identical
+// results; in the renderer's stages (closest_hit below) it measured 0.5-1%
+// slower per frame, so closest_hit keeps the 16 B loads.
+__device__ __forceinline__ void load_node(const float4 *nd, float4 &n0, float4 &n1, float4 &n2, int4 &n3) {
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(n0.x), "=f"(n0.y), "=f"(n0.z), "=f"(n0.w), "=f"(n1.x), "=f"(n1.y), "=f"(n1.z), "=f"(n1.w)
+        : "l"(nd));
+    asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(n2.x), "=f"(n2.y), "=f"(n2.z), "=f"(n2.w), "=r"(n3.x), "=r"(n3.y), "=r"(n3.z), "=r"(n3.w)
+        : "l"(nd + 2));
+}
+
 template <bool kEarlyExit, bool kCull = true>
 __device__ __forceinline__ Hit closest_hit(const BvhView &bvh, V3 o, V3 d, float tmin, float tmax,
                                            float t_exit = 0.f) {

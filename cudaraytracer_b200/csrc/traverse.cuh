@@ -76,18 +76,9 @@ __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
         if (idx < 0) continue;
         // one while-while iteration of closest_hit
         while (link >= 0) {
-            // the 64 B node as two 32 B read-only loads (nodes are 64 B
-            // apart from a 256 B-aligned base); measured 1.3-1.5% faster than
-            // four 16 B loads on the extend and shadow batches, same results
-            const float4 *nd = bvh.nodes + 4 * (size_t)link;
             float4 n0, n1, n2;
             int4 n3;
-            asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                : "=f"(n0.x), "=f"(n0.y), "=f"(n0.z), "=f"(n0.w), "=f"(n1.x), "=f"(n1.y), "=f"(n1.z), "=f"(n1.w)
-                : "l"(nd));
-            asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                : "=f"(n2.x), "=f"(n2.y), "=f"(n2.z), "=f"(n2.w), "=r"(n3.x), "=r"(n3.y), "=r"(n3.z), "=r"(n3.w)
-                : "l"(nd + 2));
+            load_node(bvh.nodes + 4 * (size_t)link, n0, n1, n2, n3);
             float t0, t1;
             bool h0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, tmin, hit.t, t0);
             bool h1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, tmin, hit.t, t1);
