@@ -8,9 +8,11 @@ python bench.py [--gpus N] [--steps K] [--warmup W] [--impl crt|reference]
             inputs, CUDA events on the launching stream, max over ranks.
 * e2e     : the same through the public host-buffer API (crt_trace_closest
             / crt_trace_shadow on pinned host arrays; copies inside).
-* roofline: the extend kernel (the dominant launch), 48 algorithmic bytes
-            per ray (32 B ray in + 16 B hit out) over its event-timed
-            duration, against the measured HBM copy bandwidth.
+* roofline: the dominant launch of the step (the shadow kernel on this
+            workload; the extend kernel if it ever takes longer), its
+            algorithmic bytes (shadow 49 B per query: 48 B in + 1 B out;
+            extend 48 B per ray: 32 B ray in + 16 B hit out) over its
+            event-timed duration, against the measured HBM copy bandwidth.
 * cpu_baseline: the reference's own BVH traversal and visibility test
             (oracle/_ref, host-compiled) on the host cores, bounded sample.
 --impl reference runs that reference CPU implementation as the timed arm.
@@ -22,7 +24,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -52,16 +53,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per 16M-ray
+# launch of each trace kernel, from one ncu capture of an 8M-ray launch of
+# the same kernel build on the same batch distribution, scaled x2 (ray bytes
+# scale exactly, node visits linearly for uniform random rays). The capture
+# and its command are summarised in profiles/ (traversal summary).
+TRAFFIC_PER_16M = {"extend": 1698088448, "shadow": 5904843776}
+
+
 def profiled_traffic(kernel: str):
     """Per-launch DRAM bytes (16M-ray launch) of `kernel` ("extend" or
-    "shadow") from the committed ncu summary
-    (profiles/extend_icospheres_ncu.md), or None if not captured."""
-    p = os.path.join(ROOT, "profiles", "extend_icospheres_ncu.md")
-    if not os.path.exists(p):
-        return None
-    key = "traffic_bytes_per_launch_16M" if kernel == "extend" else "shadow_traffic_bytes_per_launch_16M"
-    m = re.search(r"^" + key + r":\s*([0-9.eE+]+)", open(p).read(), re.M)
-    return float(m.group(1)) if m else None
+    "shadow"), or None if not captured."""
+    return TRAFFIC_PER_16M.get(kernel)
 
 
 class ClockSampler:
@@ -169,6 +172,54 @@ def reference_cuda(tris, rays, qs, hits_mine, occ_mine, steps, stream):
            "build": "reference sources, nvcc -O3 -rdc -arch sm_100a, BVH built on the host"}
     ref.close()
     return res
+
+
+def cornell_trace_leg(ctx, stream, reps=20, with_reference=True):
+    """Traversal on the Cornell box (36 triangles): 1M fixed closest-hit rays
+    (seed 1: origins uniform in the scene box, directions uniform on the
+    sphere) + 1M Light::Visible queries (seed 2), device-resident, CUDA
+    events over `reps` launches of each after a warm-up; then the reference's
+    own traversal built for the GPU on the same device batch, with its hit
+    records compared to ours. Returns a dict (Mrays/s of both, their ratio)."""
+    import torch
+
+    from cudaraytracer_b200 import Scene, scenes
+
+    n = 1 << 20
+    tris = scenes.cornell_box().triangles()
+    dev = torch.device("cuda", ctx.device)
+    rays = torch.from_numpy(scenes.random_rays(tris, n, seed=1)).to(dev)
+    qs = torch.from_numpy(scenes.random_shadow_queries(tris, n, seed=2)).to(dev)
+    hits = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    occ = torch.empty((n,), dtype=torch.uint8, device=dev)
+    sc = Scene.from_triangles(ctx, tris)
+    for _ in range(5):
+        sc.trace_closest(rays, hits)
+        sc.trace_shadow(qs, occ)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    for _ in range(reps):
+        sc.trace_closest(rays, hits)
+    ev[1].record(stream)
+    for _ in range(reps):
+        sc.trace_shadow(qs, occ)
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    ext = ev[0].elapsed_time(ev[1]) / reps
+    sh = ev[1].elapsed_time(ev[2]) / reps
+    out = {"workload": "Cornell box 36 tris; 1M closest-hit rays (seed 1) + 1M shadow queries (seed 2)",
+           "value": round(2 * n / ((ext + sh) * 1e-3) / 1e6, 1), "unit": "Mrays/s",
+           "extend_ms_per_launch": round(ext, 4), "shadow_ms_per_launch": round(sh, 4),
+           "hit_rate": float((hits[:, 1].view(torch.int32) >= 0).float().mean().item()),
+           "occluded_frac": float(occ.float().mean().item())}
+    if with_reference:
+        ref = reference_cuda(tris, rays, qs, hits, occ, reps, stream)
+        if ref is not None:
+            out["reference_cuda"] = ref
+            out["ratio_vs_reference_cuda"] = round(out["value"] / ref["value"], 2)
+    sc.close()
+    return out
 
 
 def render_leg(ctx, steps, stream, with_reference=True):
@@ -408,6 +459,15 @@ def denoise_leg(ctx):
             "throughput": thr}
 
 
+def bench_config(world):
+    """The workload description both arms print (the same dict, so the two
+    lines name one configuration)."""
+    return {"workload": "icosphere field (64 x level-5 icospheres, 1,310,720 tris); per GPU and step "
+                        "16M closest-hit rays + 16M shadow queries (1:1 extend:shadow)",
+            "l2": "inputs 1.28 GB per step > 126 MB L2 (no flush needed)",
+            "parallelism": f"replicas x{world}"}
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU implementation of the path
     (rank 0 only), on the same scene, metric and unit."""
@@ -421,9 +481,11 @@ def run_reference(args, rank, world):
         return
     threads = os.cpu_count() or 1
     tris = scenes.icosphere_field(with_env=False).triangles()
-    n_ext, n_sh = 4 << 20, 1 << 20
-    rays = scenes.random_rays(tris, n_ext, seed=5)
-    q = scenes.random_shadow_queries(tris, n_sh, seed=6)
+    # the same 1:1 extend:shadow mix as the GPU arm, on the first rays and
+    # queries of the GPU arm's rank-0 batch
+    n_ext = n_sh = 2 << 20
+    rays = scenes.random_rays(tris, N_RAYS, seed=5)[:n_ext]
+    q = scenes.random_shadow_queries(tris, N_RAYS, seed=1005)[:n_sh]
     ref = oracle.RefScene(tris)
     for _ in range(args.warmup):
         ref.trace_closest(rays[: 1 << 18], threads)
@@ -437,12 +499,13 @@ def run_reference(args, rank, world):
     ref.close()
     dt = sum(times)
     value = args.steps * (n_ext + n_sh) / dt / 1e6
-    sample = f"{n_ext} extend rays + {n_sh} shadow queries per step (bounded sample of the 16M+16M batch)"
+    sample = (f"{n_ext} extend rays + {n_sh} shadow queries per step: the first rays and queries of the "
+              f"16M+16M batch, same 1:1 mix")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "icosphere field 1.31M tris; extend + shadow rays", "threads": threads},
+        "config": bench_config(world), "threads": threads,
         "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -459,6 +522,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA traversal")
+    ap.add_argument("--no-cornell", action="store_true", help="skip the Cornell-box 1M+1M traversal leg")
     ap.add_argument("--no-render", action="store_true", help="skip the full-frame render leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the multi-scene serving leg")
@@ -546,6 +610,9 @@ def main():
     ref_cuda = None
     if rank == 0 and not args.no_ref_cuda:
         ref_cuda = reference_cuda(tris, rays, qs, hits, occ, max(1, min(args.steps, 3)), stream)
+    cornell = None
+    if rank == 0 and not args.no_cornell:
+        cornell = cornell_trace_leg(ctx, stream, with_reference=not args.no_ref_cuda)
     render = None
     if rank == 0 and not args.no_render:
         render = render_leg(ctx, max(2, min(args.steps, 8)), stream, with_reference=not args.no_ref_cuda)
@@ -601,7 +668,7 @@ def main():
         cpu = None
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            n_ext, n_sh = 4 << 20, 1 << 20
+            n_ext = n_sh = 2 << 20  # the step's 1:1 extend:shadow mix
             r = reference_cpu(tris, rays_np[:n_ext], q_np[:n_sh], threads)
             if r is not None:
                 cpu = {"value": round(r[0], 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
@@ -611,11 +678,9 @@ def main():
             "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "icosphere field (64 x level-5 icospheres, 1,310,720 tris); per GPU and step "
-                                   "16M closest-hit rays + 16M shadow queries",
-                       "l2": "inputs 1.28 GB per step > 126 MB L2 (no flush needed)",
-                       "bvh_nodes": info["num_bvh_nodes"], "bvh_depth": info["bvh_depth"],
-                       "bvh_build_ms": round(info["build_ms"], 2), "parallelism": f"replicas x{world}"},
+            "config": bench_config(world),
+            "bvh": {"nodes": info["num_bvh_nodes"], "depth": info["bvh_depth"],
+                    "build_ms": round(info["build_ms"], 2)},
             "kernels": kern,
             "roofline": {"bound": "hbm", "achieved": kern[dom]["achieved"], "peak": peak, "unit": "GB/s",
                          "frac": kern[dom]["frac"], "traffic": kern[dom]["traffic"],
@@ -627,6 +692,7 @@ def main():
             "e2e": {"value": round(e2e_val, 2), "unit": "Mrays/s",
                     "h2d_bytes_per_step": N_RAYS * (32 + 48), "d2h_bytes_per_step": N_RAYS * (16 + 1)},
             "reference_cuda": ref_cuda,
+            "cornell_trace": cornell,
             "render": render,
             "batch": batch,
             "serve": serve,

@@ -54,6 +54,9 @@ class SceneInfo(C.Structure):
         ("fovy", C.c_float),
         ("denoise", C.c_int32),
         ("has_env", C.c_int32),
+        ("num_wide_nodes", C.c_int64),
+        ("wide_depth", C.c_int32),
+        ("wide_build_ms", C.c_float),
     ]
 
 
@@ -265,6 +268,8 @@ _SIGS = {
     "crt_trace_closest_device": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
     "crt_trace_shadow": (C.c_int, [_VP, _VP, C.c_int64, _VP]),
     "crt_trace_shadow_device": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
+    "crt_scene_ray_counts": (C.c_int, [_VP, _VP, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "crt_bvh8_collapse": (C.c_int, [_VP, C.c_int64, _VP, _VP, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
 }
 
 

@@ -135,6 +135,9 @@ crt_status crt_scene_info(const crt_scene *scene, crt_scene_info_t *info) {
             info->bounds_max[k] = scene->bvh.bounds_max[k];
         }
         info->build_ms = scene->bvh.build_ms;
+        info->num_wide_nodes = scene->bvh.num_wide_nodes;
+        info->wide_depth = scene->bvh.wide_depth;
+        info->wide_build_ms = scene->bvh.wide_build_ms;
         scene->fill_info(*info);
     });
 }
@@ -184,6 +187,40 @@ crt_status crt_trace_shadow_device(crt_scene *scene, const crt_shadow_query *d_q
                   "crt_trace_shadow_device: queries must be 16-byte aligned");
         cudaStream_t s = stream ? (cudaStream_t)stream : scene->ctx->stream;
         launch_trace_shadow(scene->bvh.view(), reinterpret_cast<const float *>(d_q), n, d_occ, s);
+    });
+}
+
+crt_status crt_scene_ray_counts(crt_scene *scene, void *stream, int64_t *extend_rays, int64_t *shadow_rays) {
+    return guard([&] {
+        CRT_CHECK(scene && extend_rays && shadow_rays, CRT_ERR_INVALID, "crt_scene_ray_counts: null argument");
+        CRT_CUDA(cudaSetDevice(scene->ctx->device));
+        *extend_rays = *shadow_rays = 0;
+        if (!scene->wf.counters) return;
+        if (stream) CRT_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+        CRT_CUDA(cudaStreamSynchronize(scene->ctx->stream));
+        unsigned long long c[2];
+        CRT_CUDA(cudaMemcpy(&c[0], scene->wf.counters + kExtendRaysCounter, 8, cudaMemcpyDeviceToHost));
+        CRT_CUDA(cudaMemcpy(&c[1], scene->wf.counters + kShadowRaysCounter, 8, cudaMemcpyDeviceToHost));
+        *extend_rays = (int64_t)c[0];
+        *shadow_rays = (int64_t)c[1];
+    });
+}
+
+crt_status crt_bvh8_collapse(const float *bin_nodes, int64_t num_bin_nodes, float *wide_nodes, int32_t *wide_links,
+                             int64_t *num_wide, int32_t *wide_depth) {
+    return guard([&] {
+        CRT_CHECK(bin_nodes && num_bin_nodes > 0 && num_wide, CRT_ERR_INVALID, "crt_bvh8_collapse: bad argument");
+        std::vector<float4> nodes;
+        std::vector<int> links;
+        const int depth = collapse_bvh8(reinterpret_cast<const float4 *>(bin_nodes), num_bin_nodes, nodes, links);
+        const int64_t count = (int64_t)(nodes.size() / 4);
+        if (wide_nodes && wide_links) {
+            CRT_CHECK(*num_wide >= count, CRT_ERR_CAPACITY, "crt_bvh8_collapse: output arrays too small");
+            std::memcpy(wide_nodes, nodes.data(), nodes.size() * sizeof(float4));
+            std::memcpy(wide_links, links.data(), links.size() * sizeof(int));
+        }
+        *num_wide = count;
+        if (wide_depth) *wide_depth = depth;
     });
 }
 

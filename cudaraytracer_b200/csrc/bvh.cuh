@@ -28,9 +28,11 @@ constexpr int kSentinel = INT_MIN;  // never a valid link: first < 2^27 - 1
 constexpr float kTriTMax = 1e8f;    // Triangle::IsIntersect default tMax
 
 struct BvhView {
-    const float4 *nodes;  // 4 float4 per node
-    const float4 *tris;   // 3 float4 per triangle
+    const float4 *nodes;   // 4 float4 per node
+    const float4 *tris;    // 3 float4 per triangle
     int num_tris;
+    const float4 *wnodes;  // 8-wide quantised nodes, 4 float4 each (bvh8.cuh)
+    const int *wlinks;     // 8 child links per wide node
 };
 
 __host__ __device__ __forceinline__ int leaf_link(int first, int count) { return ~((first << 4) | count); }

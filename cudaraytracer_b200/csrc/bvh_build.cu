@@ -21,6 +21,7 @@
 #include <vector>
 #include <algorithm>
 #include <cstring>
+#include <chrono>
 
 namespace crt {
 namespace {
@@ -786,12 +787,17 @@ void build_bvh(const float *d_verts, int n, cudaStream_t stream, BvhBuffers &out
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     out.num_tris = n;
+    const auto w0 = std::chrono::steady_clock::now();
+    build_bvh8(out, stream);
+    out.wide_build_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - w0).count();
 }
 
 void free_bvh(BvhBuffers &b) {
     if (b.nodes) cudaFree(b.nodes);
     if (b.tris) cudaFree(b.tris);
     if (b.slot_of_prim) cudaFree(b.slot_of_prim);
+    if (b.wnodes) cudaFree(b.wnodes);
+    if (b.wlinks) cudaFree(b.wlinks);
     b = BvhBuffers();
 }
 

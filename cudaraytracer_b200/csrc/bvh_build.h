@@ -1,6 +1,7 @@
 // Device BVH build interface (see bvh_build.cu).
 #pragma once
 #include "bvh.cuh"
+#include "bvh8.cuh"
 
 namespace crt {
 
@@ -14,7 +15,13 @@ struct BvhBuffers {
     float bounds_min[3] = {0, 0, 0};
     float bounds_max[3] = {0, 0, 0};
     float build_ms = 0.f;
-    BvhView view() const { return BvhView{nodes, tris, num_tris}; }
+    // 8-wide quantised tree collapsed from `nodes` (bvh8.cuh)
+    float4 *wnodes = nullptr;
+    int *wlinks = nullptr;
+    int64_t num_wide_nodes = 0;
+    int wide_depth = 0;
+    float wide_build_ms = 0.f;
+    BvhView view() const { return BvhView{nodes, tris, num_tris, wnodes, wlinks}; }
 };
 
 // Builds the BVH of n triangles given as n x 9 floats (v0, v1, v2) on the

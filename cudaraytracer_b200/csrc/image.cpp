@@ -4,8 +4,9 @@
 // uchar4 CUDA array (Texture::Load, Src/Core/texture.cu:207-240, through
 // stbi_load with 4 requested channels): 16-bit samples keep their high byte,
 // low-bit-depth grey is scaled to 0..255, palette entries expand with their
-// tRNS alpha, absent alpha is 255. Interlaced PNGs and other formats are
-// refused with a message (the scene loader then keeps the basecolor).
+// tRNS alpha, absent alpha is 255. JPEG is decoded in jpeg.cpp. Interlaced
+// PNGs and other formats are refused with a message (the scene loader then
+// keeps the basecolor).
 #include "scene_data.h"
 #include "common.cuh"
 #include <algorithm>
@@ -318,6 +319,8 @@ void decode_ppm(const std::vector<uint8_t> &f, HostTexture &t) {
 
 }  // namespace
 
+void decode_jpeg(const std::vector<uint8_t> &f, HostTexture &t);  // jpeg.cpp
+
 void load_texture_image(const std::string &path, HostTexture &t) {
     std::ifstream in(path, std::ios::binary);
     if (!in) throw Error(CRT_ERR_IO, "cannot open texture " + path);
@@ -326,8 +329,10 @@ void load_texture_image(const std::string &path, HostTexture &t) {
         decode_png(f, t);
     else if (f.size() >= 2 && f[0] == 'P' && f[1] == '6')
         decode_ppm(f, t);
+    else if (f.size() >= 3 && f[0] == 0xFF && f[1] == 0xD8 && f[2] == 0xFF)
+        decode_jpeg(f, t);
     else
-        throw Error(CRT_ERR_PARSE, "unsupported texture format (PNG and binary PPM are decoded): " + path);
+        throw Error(CRT_ERR_PARSE, "unsupported texture format (PNG, JPEG and binary PPM are decoded): " + path);
 }
 
 }  // namespace crt

@@ -306,19 +306,27 @@ void init_camera(CameraState &c, const float bmin[3], const float bmax[3], const
 // wavefront buffers
 // ---------------------------------------------------------------------------
 void Wavefront::reserve(size_t paths) {
+    if (!counters) {
+        // kept across growth: [0..3] queue counts, [8..11] two 64-bit ray counters
+        CRT_CUDA(cudaMalloc(&counters, kWavefrontCounters * sizeof(int)));
+        CRT_CUDA(cudaMemset(counters, 0, kWavefrontCounters * sizeof(int)));
+    }
     if (paths <= cap) return;
-    release();
+    release_paths();
     for (int q = 0; q < 2; ++q)
         for (int k = 0; k < 5; ++k) CRT_CUDA(cudaMalloc(&this->q[q][k], paths * sizeof(float4)));
     CRT_CUDA(cudaMalloc(&hits, paths * sizeof(float4)));
     for (int k = 0; k < 4; ++k) CRT_CUDA(cudaMalloc(&shadow[k], paths * sizeof(float4)));
     for (int k = 0; k < 2; ++k) CRT_CUDA(cudaMalloc(&term[k], paths * sizeof(float4)));
-    CRT_CUDA(cudaMalloc(&counters, 8 * sizeof(int)));
-    CRT_CUDA(cudaMemset(counters, 0, 8 * sizeof(int)));
     cap = paths;
 }
 
 void Wavefront::release() {
+    release_paths();
+    if (counters) cudaFree(counters), counters = nullptr;
+}
+
+void Wavefront::release_paths() {
     for (int q = 0; q < 2; ++q)
         for (int k = 0; k < 5; ++k)
             if (this->q[q][k]) cudaFree(this->q[q][k]), this->q[q][k] = nullptr;
@@ -327,7 +335,6 @@ void Wavefront::release() {
         if (shadow[k]) cudaFree(shadow[k]), shadow[k] = nullptr;
     for (int k = 0; k < 2; ++k)
         if (term[k]) cudaFree(term[k]), term[k] = nullptr;
-    if (counters) cudaFree(counters), counters = nullptr;
     cap = 0;
 }
 
@@ -364,12 +371,13 @@ __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *co
 // tMin 0, closest starts at 1e8). Also clears the next bounce's counters.
 __global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters,
                                                 int out_idx) {
+    const int n = *n_in;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         counters[out_idx] = 0;
         counters[2] = 0;
         counters[3] = 0;
+        atomicAdd(reinterpret_cast<unsigned long long *>(counters + kExtendRaysCounter), (unsigned long long)n);
     }
-    const int n = *n_in;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = q.p[0][i], b = q.p[1][i];
         Hit h = closest_hit<false>(bvh, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, 0.f, kTriTMax);
@@ -435,6 +443,9 @@ __global__ void __launch_bounds__(256) k_shade(SceneView s, StepParams sp, Queue
 __global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueView qout,
                                                 float4 *term0, float4 *term1, AccumView acc) {
     const int n = counters[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        atomicAdd(reinterpret_cast<unsigned long long *>(const_cast<int *>(counters) + kShadowRaysCounter),
+                  (unsigned long long)n);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = sh.r[0][i], b = sh.r[1][i], c = sh.r[2][i], d = sh.r[3][i];
         bool vis = visible(bvh, V3{a.x, a.y, a.z}, V3{a.w, b.x, b.y}, V3{b.z, b.w, c.x}, V3{c.y, c.z, c.w});

@@ -22,10 +22,17 @@
 // The array's device address is looked up with cudaGetSymbolAddress the
 // first time the entry point runs on a device (with that device current),
 // so that first call must come before any stream capture on that device.
-// All calls share the one array and it keeps the previous call's contents:
-// the counters are cleared at the start of every call, and calls whose GPU
-// work overlaps (two streams, two host threads, two scenes) race on it, so
-// they must be ordered by the caller.
+// All calls share the one array and it keeps the previous call's contents.
+// Nothing stale is read: the stage kernels set every queue counter before
+// it is used (k_raygen the input count, k_extend the next bounce's output,
+// shadow and terminal counts), and the counter block is also zeroed at the
+// start of every call as a defensive measure. Calls whose GPU work overlaps
+// (two streams, two host threads, two scenes) race on the array, so they
+// must be ordered by the caller.
+//
+// Block size and samples per wavefront follow the scene's render params as
+// crt_render_device does (stage_block; spp_per_pass, capped at
+// 65,536 / pixels so one wavefront fits the scratch).
 #include "api_internal.h"
 #include "render_kernels.cuh"
 #include <algorithm>
@@ -93,7 +100,7 @@ extern "C" crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_
         float4 *hits = plane[10];
         ShadowView sh{{plane[11], plane[12], plane[13], plane[14]}};
         float4 *term0 = plane[15], *term1 = plane[16];
-        CRT_CUDA(cudaMemsetAsync(counters, 0, kCounterBytes, s));
+        CRT_CUDA(cudaMemsetAsync(counters, 0, kCounterBytes, s));  // defensive; see the header comment
         if (spp == 0) return;
 
         const SceneView view = make_view(scene->bvh, scene->rd);
@@ -109,10 +116,12 @@ extern "C" crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_
         cv.w = w;
         cv.h = h;
         AccumView av{(float4 *)d_direct, (float4 *)d_indirect, (float4 *)d_sumsq};
-        const int per_pass = std::max(1, std::min(spp, (int)(kNoAllocMaxPaths / pixels)));
-        const int g_ext = persistent_grid((const void *)k_extend, 128);
-        const int g_sh = persistent_grid((const void *)k_shade, 128);
-        const int g_sd = persistent_grid((const void *)k_shadow, 128);
+        const int fit = (int)(kNoAllocMaxPaths / pixels);
+        const int per_pass = std::max(1, std::min(spp, rp.spp_per_pass > 0 ? std::min(rp.spp_per_pass, fit) : fit));
+        const int blk = rp.block();
+        const int g_ext = persistent_grid((const void *)k_extend, blk);
+        const int g_sh = persistent_grid((const void *)k_shade, blk);
+        const int g_sd = persistent_grid((const void *)k_shadow, blk);
         for (int done = 0; done < spp; done += per_pass) {
             const int n = (int)pixels * std::min(per_pass, spp - done);
             StepParams sp;
@@ -126,10 +135,10 @@ extern "C" crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_
             for (int b = 0; b < rp.max_bounces; ++b) {
                 const int in = b & 1, out = 1 - in;
                 sp.bounce = b;
-                k_extend<<<g_ext, 128, 0, s>>>(view.bvh, q[in], counters + in, hits, counters, out);
-                k_shade<<<g_sh, 128, 0, s>>>(view, sp, q[in], hits, counters + in, q[out], counters, out, sh, term0,
+                k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], counters + in, hits, counters, out);
+                k_shade<<<g_sh, blk, 0, s>>>(view, sp, q[in], hits, counters + in, q[out], counters, out, sh, term0,
                                             term1, av);
-                k_shadow<<<g_sd, 128, 0, s>>>(view.bvh, sh, counters, q[out], term0, term1, av);
+                k_shadow<<<g_sd, blk, 0, s>>>(view.bvh, sh, counters, q[out], term0, term1, av);
             }
             CRT_CUDA(cudaGetLastError());
         }

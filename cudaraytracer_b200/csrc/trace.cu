@@ -8,6 +8,7 @@
 #include "trace.cuh"
 #include "traverse.cuh"
 #include "render_kernels.cuh"  // persistent_grid
+#include <cstdlib>
 
 namespace crt {
 
@@ -68,6 +69,32 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow(BvhView bvh, const
     trace_dynamic<true>(job, n);
 }
 
+// The same over the 8-wide quantised tree with the shared-memory short
+// stack (kShort entries per lane, kShort x 128 words per block).
+template <int kShort>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_closest8(BvhView bvh, const float4 *__restrict__ rays, int n,
+                                                                float4 *__restrict__ hits) {
+    __shared__ unsigned s_stack[kShort * kTraceBlock];
+    ClosestJob job{bvh, rays, hits};
+    trace_dynamic8<true, kShort>(job, n, s_stack);
+}
+
+template <int kShort>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8(BvhView bvh, const float4 *__restrict__ q, int n,
+                                                               uint8_t *__restrict__ occ) {
+    __shared__ unsigned s_stack[kShort * kTraceBlock];
+    ShadowJob job{bvh, q, occ, {}};
+    trace_dynamic8<true, kShort>(job, n, s_stack);
+}
+
+// Traversal variant: 8 = the 8-wide tree with a 16-entry shared-memory
+// stack (default), 82 = the same with 8 entries, 2 = the binary tree with
+// a local-memory stack. CRT_TRAVERSAL overrides the default.
+static int traversal_variant() {
+    const char *e = getenv("CRT_TRAVERSAL");
+    return e ? atoi(e) : 8;
+}
+
 // Persistent grid (all SMs at full occupancy), fewer blocks for small
 // batches so every warp gets rays.
 static int trace_grid(const void *kernel, int64_t n) {
@@ -79,15 +106,32 @@ static int trace_grid(const void *kernel, int64_t n) {
 void launch_trace_closest(const BvhView &bvh, const float4 *d_rays, int64_t n, float4 *d_hits, cudaStream_t s) {
     if (n <= 0) return;
     CRT_CHECK(n < (int64_t)1 << 31, CRT_ERR_CAPACITY, "trace batch larger than 2^31 rays");
-    k_trace_closest<<<trace_grid((const void *)k_trace_closest, n), kTraceBlock, 0, s>>>(bvh, d_rays, (int)n, d_hits);
+    const int v = bvh.wnodes ? traversal_variant() : 2;
+    if (v == 8)
+        k_trace_closest8<16><<<trace_grid((const void *)k_trace_closest8<16>, n), kTraceBlock, 0, s>>>(
+            bvh, d_rays, (int)n, d_hits);
+    else if (v == 82)
+        k_trace_closest8<8><<<trace_grid((const void *)k_trace_closest8<8>, n), kTraceBlock, 0, s>>>(
+            bvh, d_rays, (int)n, d_hits);
+    else
+        k_trace_closest<<<trace_grid((const void *)k_trace_closest, n), kTraceBlock, 0, s>>>(bvh, d_rays, (int)n,
+                                                                                            d_hits);
     CRT_CUDA(cudaGetLastError());
 }
 
 void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_t *d_occ, cudaStream_t s) {
     if (n <= 0) return;
     CRT_CHECK(n < (int64_t)1 << 31, CRT_ERR_CAPACITY, "trace batch larger than 2^31 queries");
-    k_trace_shadow<<<trace_grid((const void *)k_trace_shadow, n), kTraceBlock, 0, s>>>(
-        bvh, reinterpret_cast<const float4 *>(d_q), (int)n, d_occ);
+    const float4 *q = reinterpret_cast<const float4 *>(d_q);
+    const int v = bvh.wnodes ? traversal_variant() : 2;
+    if (v == 8)
+        k_trace_shadow8<16><<<trace_grid((const void *)k_trace_shadow8<16>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
+                                                                                                    d_occ);
+    else if (v == 82)
+        k_trace_shadow8<8><<<trace_grid((const void *)k_trace_shadow8<8>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
+                                                                                                  d_occ);
+    else
+        k_trace_shadow<<<trace_grid((const void *)k_trace_shadow, n), kTraceBlock, 0, s>>>(bvh, q, (int)n, d_occ);
     CRT_CUDA(cudaGetLastError());
 }
 

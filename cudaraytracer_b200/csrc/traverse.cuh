@@ -24,6 +24,7 @@
 // early exit; t_exit = 0 never fires).
 #pragma once
 #include "bvh.cuh"
+#include "bvh8.cuh"
 
 namespace crt {
 
@@ -40,7 +41,7 @@ __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
     int cleft = (int)((w + 1) * n / warps) - cbase;
     // per-lane ray state
     int idx = -1;
-    BvhView bvh{nullptr, nullptr, 0};
+    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr};
     V3 o{0.f, 0.f, 0.f}, d{0.f, 0.f, 0.f}, inv{0.f, 0.f, 0.f};
     float tmin = 0.f, t_exit = 0.f;
     Hit hit;
@@ -116,6 +117,81 @@ __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
                 link = stack[--sp];
                 finished = link == kSentinel;
             }
+        }
+        if (finished) {
+            job.finish(idx, bvh, hit);
+            idx = -1;
+        }
+    }
+}
+
+// trace_dynamic over the 8-wide quantised tree (bvh8.cuh) with the
+// per-lane short stack in shared memory: `s_stack` is the block's
+// kShort x blockDim.x word array. One loop turn finds the next leaf
+// (visiting wide nodes on the way) and tests its triangles; lanes whose ray
+// finished take new rays as above. Hit records equal closest_hit's (same
+// triangle test, conservative boxes); only the order in which equal-t
+// triangles are met may differ.
+template <bool kCull, int kShort, class Job>
+__device__ __forceinline__ void trace_dynamic8(Job &job, int n, unsigned *s_stack) {
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int cbase = (int)(w * n / warps);
+    int cleft = (int)((w + 1) * n / warps) - cbase;
+    int idx = -1;
+    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr};
+    V3 o{0.f, 0.f, 0.f}, d{0.f, 0.f, 0.f}, inv{0.f, 0.f, 0.f};
+    float tmin = 0.f, t_exit = 0.f;
+    unsigned oct = 0, cur = 0;
+    Hit hit;
+    hit.t = 0.f;
+    hit.slot = -1;
+    hit.b1 = hit.b2 = 0.f;
+    ShortStack<kShort> st;
+    st.col = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
+    st.sp = 0;
+
+    while (true) {
+        const unsigned idle = __ballot_sync(0xffffffffu, idx < 0);
+        if (idle && cleft > 0) {
+            const int take = min(__popc(idle), cleft);
+            const int rank = __popc(idle & lt);
+            if (idx < 0 && rank < take) {
+                idx = cbase + rank;
+                float tmax;
+                job.setup(idx, bvh, o, d, tmin, tmax, t_exit);
+                inv = v3(rrcp(d.x), rrcp(d.y), rrcp(d.z));
+                oct = ray_octant(d);
+                hit.t = tmax;
+                hit.slot = -1;
+                hit.b1 = hit.b2 = 0.f;
+                st.reset();
+                cur = visit8(bvh.wnodes, 0, o, inv, tmin, hit.t, oct);
+            }
+            cbase += take;
+            cleft -= take;
+        }
+        if (__ballot_sync(0xffffffffu, idx >= 0) == 0) break;
+        if (idx < 0) continue;
+        const int leaf = next_leaf8(bvh, cur, st, o, inv, tmin, hit.t, oct);
+        bool finished = leaf == 0;
+        if (!finished) {
+            const int code = ~leaf;
+            const int first = code >> 4, count = code & 15;
+            for (int k = 0; k < count; ++k) {
+                const int slot = first + k;
+                const float4 *tp = bvh.tris + 3 * (size_t)slot;
+                const float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                const bool acc = intersect_triangle<kCull>(o, d, a, b, c, slot, hit);
+                if (acc && hit.t < t_exit) {
+                    finished = true;
+                    break;
+                }
+            }
+            if (!finished && (cur & 0xffu) == 0 && st.empty()) finished = true;
         }
         if (finished) {
             job.finish(idx, bvh, hit);

@@ -81,9 +81,11 @@ class SceneSpec:
     def triangles(self) -> np.ndarray:
         return np.concatenate([m.tris for m in self.meshes]).astype(np.float32)
 
-    def write(self, directory: str, name: str = "scene") -> str:
+    def write(self, directory: str, name: str = "scene", texture_format: str = "png") -> str:
         """Writes OBJ / HDR / JSON in the reference's schema; returns the
-        JSON path. Asset paths are absolute, as in the reference's scenes."""
+        JSON path. Asset paths are absolute, as in the reference's scenes.
+        Textures are written as PNG, or as baseline JPEG (quality 95, 4:4:4
+        chroma, through Pillow) with texture_format="jpg"."""
         os.makedirs(directory, exist_ok=True)
         directory = os.path.abspath(directory)
         objects = []
@@ -93,8 +95,15 @@ class SceneSpec:
             objects.append({"name": m.name, "path": path, "material": m.material})
         textures = []
         for tname, img in self.textures.items():
-            path = os.path.join(directory, f"{name}_tex_{tname}.png")
-            write_png(path, img)
+            if texture_format == "jpg":
+                from PIL import Image
+
+                path = os.path.join(directory, f"{name}_tex_{tname}.jpg")
+                Image.fromarray(np.ascontiguousarray(img[..., :3], dtype=np.uint8)).save(path, quality=95,
+                                                                                         subsampling=0)
+            else:
+                path = os.path.join(directory, f"{name}_tex_{tname}.png")
+                write_png(path, img)
             textures.append({"name": tname, "path": path})
         lights = []
         for l in self.lights:

@@ -265,6 +265,14 @@ class Scene:
         _lib.call("crt_render_device", self._h, int(first_sample), int(spp), direct.data_ptr(), indirect.data_ptr(),
                   sumsq.data_ptr() if sumsq is not None else None, C.c_void_p(s))
 
+    def ray_counts(self, stream=None) -> tuple:
+        """(extend rays, shadow rays) traced by this scene's wavefront
+        renders since it was created (path vertices and Light::Visible
+        tests; subsurface probe rays are not counted)."""
+        e, s = C.c_int64(0), C.c_int64(0)
+        _lib.call("crt_scene_ray_counts", self._h, C.c_void_p(stream or 0), C.byref(e), C.byref(s))
+        return e.value, s.value
+
     def render_device_noalloc(self, direct, indirect, spp: int, first_sample: int = 0, sumsq=None, stream=None):
         """render_device without device allocation: the library's fixed
         scratch holds the path queues (at most 65,536 pixels; calls must not
@@ -418,6 +426,22 @@ class Scene:
         out = np.empty((q.shape[0],), dtype=np.uint8) if occluded is None else occluded
         _lib.call("crt_trace_shadow", self._h, q.ctypes.data, int(q.shape[0]), out.ctypes.data)
         return out
+
+
+def bvh8_collapse(bin_nodes: np.ndarray):
+    """Collapses a binary node array ((n, 16) float32 in this library's
+    two-child layout, root at 0) into the 8-wide quantised layout on the
+    host. Returns (wide_nodes (m, 16) float32, wide_links (m, 8) int32,
+    depth)."""
+    b = np.ascontiguousarray(bin_nodes, dtype=np.float32).reshape(-1, 16)
+    cnt = C.c_int64(0)
+    dep = C.c_int32(0)
+    _lib.call("crt_bvh8_collapse", b.ctypes.data, b.shape[0], None, None, C.byref(cnt), C.byref(dep))
+    nodes = np.zeros((cnt.value, 16), np.float32)
+    links = np.zeros((cnt.value, 8), np.int32)
+    _lib.call("crt_bvh8_collapse", b.ctypes.data, b.shape[0], nodes.ctypes.data, links.ctypes.data, C.byref(cnt),
+              C.byref(dep))
+    return nodes, links, dep.value
 
 
 def hit_prims(hits: np.ndarray) -> np.ndarray:

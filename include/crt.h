@@ -85,6 +85,9 @@ typedef struct crt_scene_info_t {
     float rr, fovy;
     int32_t denoise;
     int32_t has_env;
+    int64_t num_wide_nodes;  /* nodes of the 8-wide quantised tree the traversal kernels use */
+    int32_t wide_depth;
+    float wide_build_ms;     /* collapse of the binary tree into it (host clock) */
 } crt_scene_info_t;
 
 /* ---- context ---------------------------------------------------------- */
@@ -231,13 +234,23 @@ crt_status crt_render(crt_scene *scene, int32_t spp, float *direct, float *indir
 crt_status crt_render_device(crt_scene *scene, int32_t first_sample, int32_t spp, float *d_direct,
                              float *d_indirect, float *d_sumsq, void *stream);
 
+/* Running totals of the rays the scene's wavefront renders have traced
+ * since it was created (crt_render, crt_render_device, crt_render_views):
+ * closest-hit extend rays (path vertices) and shadow rays (Light::Visible
+ * tests). Subsurface probe rays, traced inside the shade stage, are not
+ * counted. Waits for the scene's work on the context stream and `stream`.
+ * No counterpart in the reference. */
+crt_status crt_scene_ray_counts(crt_scene *scene, void *stream, int64_t *extend_rays, int64_t *shadow_rays);
+
 /* Same as crt_render_device but allocates no device memory: the path queues
  * live in a fixed scratch area inside the library's device image (17.8 MB
  * per GPU that loads the library, held until exit), for hosts that own the
  * GPU memory pool and forbid foreign cudaMalloc/cudaFree during a frame
  * (engines, viewport plugins, real-time services). At most 65,536 paths per
- * wavefront: images with more than 65,536 pixels return CRT_ERR_CAPACITY.
- * The first call on a device looks up the scratch address and must come
+ * wavefront: images with more than 65,536 pixels return CRT_ERR_CAPACITY;
+ * smaller images run ceil(spp / per_pass) wavefronts of per_pass samples,
+ * per_pass = min(65,536 / pixels, spp_per_pass when set). The stage block
+ * size follows stage_block as in crt_render_device. The first call on a device looks up the scratch address and must come
  * before any stream capture on that device. All calls share the scratch,
  * so calls whose GPU work overlaps race; the caller must order them.
  * No counterpart in the reference (its renderer allocates its buffers in
@@ -412,6 +425,17 @@ crt_status crt_trace_shadow(crt_scene *scene, const crt_shadow_query *q,
                             int64_t n, uint8_t *occluded);
 crt_status crt_trace_shadow_device(crt_scene *scene, const crt_shadow_query *d_q,
                                    int64_t n, uint8_t *d_occluded, void *stream);
+
+/* Host-side collapse of a binary node array (this library's 64 B two-child
+ * layout, 16 floats per node, root at 0, as built on the device for every
+ * scene) into the 8-wide quantised layout the trace kernels read: 16 floats
+ * (64 B) per wide node and 8 child links per wide node. With wide_nodes or
+ * wide_links NULL only the counts are returned; otherwise both arrays must
+ * hold *num_wide (in: capacity, out: count) nodes. No counterpart in the
+ * reference, whose traversal reads the binary tree it builds
+ * (BVH::FlattenBVHTree, Src/Core/bvh.cu:186-206). */
+crt_status crt_bvh8_collapse(const float *bin_nodes, int64_t num_bin_nodes, float *wide_nodes,
+                             int32_t *wide_links, int64_t *num_wide, int32_t *wide_depth);
 
 /* ---- tensor-core 3x3 convolutions (learned denoiser) ------------------- */
 

@@ -22,8 +22,16 @@ REF_RENDER_SO = os.path.join(HERE, "_ref", "libcrtref_render.so")
 _VP = C.c_void_p
 
 
+# Where the reference source tree is read from when oracle/_ref is built
+# (CRT_REFERENCE_DIR overrides it). Without the tree only liboracle.so builds.
+DEFAULT_REFERENCE_DIR = "/root/reference"
+
+
 def build() -> None:
-    r = subprocess.run(["make", "-C", HERE, "-j", str(os.cpu_count() or 1)], capture_output=True, text=True)
+    env = dict(os.environ)
+    env.setdefault("CRT_REFERENCE_DIR", DEFAULT_REFERENCE_DIR)
+    r = subprocess.run(["make", "-C", HERE, "-j", str(os.cpu_count() or 1)], capture_output=True, text=True,
+                       env=env)
     if r.returncode != 0:
         raise RuntimeError("building the oracle failed:\n" + r.stdout[-3000:] + r.stderr[-3000:])
 

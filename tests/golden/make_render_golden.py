@@ -22,21 +22,32 @@ sys.path.insert(0, ROOT)
 # name -> (scene factory kwargs, spp)
 SCENES = {
     "cornell": ("cornell_box", dict(width=128, height=128, max_bounces=8), 4096),
+    # the Cornell box at its stated render size: 256x256, depth 8, converged at 4096 spp
+    "cornell_256": ("cornell_box", dict(width=256, height=256, max_bounces=8), 4096),
     "icospheres": ("icosphere_field", dict(n_spheres=8, level=2, width=64, height=64, env_size=(256, 128),
                                            max_bounces=6, sun_peak=40.0, sun_sigma=0.1), 16384),
     # diffuse textures (PNG, on a diffuse and a PBR material) and two area lights
     "cornell_tex2": ("cornell_box", dict(width=96, height=96, max_bounces=8, textured=True, lights=2), 4096),
+    # the same scene with its textures as JPEG files (the reference decodes them with stb_image)
+    "cornell_jpg": ("cornell_box", dict(width=96, height=96, max_bounces=8, textured=True, lights=2), 4096,
+                    dict(texture_format="jpg")),
 }
+
+
+def scene_entry(name):
+    """(factory name, factory kwargs, spp, SceneSpec.write kwargs)."""
+    e = SCENES[name]
+    return e[0], e[1], e[2], (e[3] if len(e) > 3 else {})
 
 
 def render_one(name: str, outdir: str) -> None:
     import oracle
     from cudaraytracer_b200 import scenes
 
-    fn, kw, spp = SCENES[name]
+    fn, kw, spp, wkw = scene_entry(name)
     spec = getattr(scenes, fn)(**kw)
     with tempfile.TemporaryDirectory() as td:
-        path = spec.write(td, name)
+        path = spec.write(td, name, **wkw)
         rr = oracle.RefRenderer(path)
         d, i, q, ms = rr.render(spp, with_sumsq=True)
     np.savez_compressed(os.path.join(outdir, f"render_ref_{name}.npz"), direct=d, indirect=i, sumsq=q,

@@ -78,7 +78,11 @@ def test_cornell_render_matches_oracle(crt_ctx, cornell_json):
     assert np.isfinite(d).all() and np.isfinite(i).all()
     compare(d, od, 1e-3, 0.02)
     compare(i, oi, 1e-3, 0.02)
-    np.testing.assert_array_equal(q[..., 3], oq[..., 3]) if (q[..., 3] == oq[..., 3]).mean() == 1 else None
+    # q[..., 3] counts the sample values added into each pixel; it differs
+    # only where a rounding flip changed a path's random branch, the same
+    # 2% of pixels that the radiance bound above allows
+    cnt_bad = q[..., 3] != oq[..., 3]
+    assert cnt_bad.mean() <= 0.02, f"{cnt_bad.mean():.4f} of pixels differ in sample count"
     assert abs(q[..., 3].mean() - oq[..., 3].mean()) < 0.05
 
 

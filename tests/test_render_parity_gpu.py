@@ -22,6 +22,13 @@ sys.path.insert(0, GOLDEN)
 import make_render_golden as mg  # noqa: E402
 
 
+# relMSE bound per fixture. The Cornell-box renders (4096 spp) are held to
+# the converged-image bar of 1e-3. The icosphere fixture (64x64 at 16384 spp,
+# glass and subsurface spheres lit by a sun lobe) keeps heavier-tailed noise
+# from caustic paths; its bound sits above its measured noise floor.
+ABS_RELMSE = {"cornell": 1e-3, "cornell_256": 1e-3, "cornell_tex2": 1e-3, "cornell_jpg": 1e-3, "icospheres": 1e-3}
+
+
 def stats(sum_a, sq_a, na, sum_b, sq_b, nb):
     ma, mb = sum_a / na, sum_b / nb
     va = np.maximum(sq_a / na - ma * ma, 0)
@@ -37,8 +44,8 @@ def test_converged_render_matches_reference(crt_ctx, tmp_path, name):
     if not os.path.exists(gpath):
         pytest.skip("reference render fixture missing")
     g = np.load(gpath)
-    fn, kw, spp = mg.SCENES[name]
-    sc = Scene.load(crt_ctx, getattr(scenes, fn)(**kw).write(str(tmp_path), name))
+    fn, kw, spp, wkw = mg.scene_entry(name)
+    sc = Scene.load(crt_ctx, getattr(scenes, fn)(**kw).write(str(tmp_path), name, **wkw))
     c = sc.camera()
     np.testing.assert_allclose(np.array(c["position"] + c["left_down"] + c["du"] + c["dv"]), g["camera"], atol=1e-6)
     ref_sum = (g["direct"] + g["indirect"])[..., :3].astype(np.float64)
@@ -52,8 +59,10 @@ def test_converged_render_matches_reference(crt_ctx, tmp_path, name):
     rel_self, _ = stats(runs[0][0], runs[0][1], spp, runs[1][0], runs[1][1], spp)
     # no bias beyond sampling noise: relMSE vs the reference is at the floor
     # set by two independent renders of ours (same spp)
+    print(f"{name}: relMSE vs reference {rel_ref:.3e}, between our two renders {rel_self:.3e}, "
+          f"mean z^2 {np.mean(z * z):.3f}, |z|>4 {np.mean(np.abs(z) > 4):.4f}")
     assert rel_ref <= 1.5 * rel_self + 1e-5, (rel_ref, rel_self)
-    if name == "cornell":
-        assert rel_ref <= 1e-3
+    # absolute bound on the converged images' relMSE against the reference
+    assert rel_ref <= ABS_RELMSE[name], (rel_ref, ABS_RELMSE[name])
     assert np.mean(np.abs(z) > 4) <= 0.005
     assert np.mean(z * z) <= 1.5
