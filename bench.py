@@ -244,6 +244,7 @@ def render_leg(ctx, steps, stream, with_reference=True):
     i = torch.zeros((H, W, 4), device=dev)
     sc.render_device(d, i, step_spp, first_sample=0, stream=stream.cuda_stream)
     torch.cuda.synchronize()
+    ext0, sh0 = sc.ray_counts(stream=stream.cuda_stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for k in range(steps):
@@ -251,11 +252,20 @@ def render_leg(ctx, steps, stream, with_reference=True):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    ext1, sh1 = sc.ray_counts(stream=stream.cuda_stream)
+    vertices, shadow_rays = ext1 - ext0, sh1 - sh0
     spp_total = steps * step_spp
+    peak, kind = measured_peaks()
+    ach = PATH_VERTEX_BYTES * vertices / (ms * 1e-3) / 1e9
     out = {"scene": "icosphere field 1920x1080, depth 16, env 2048x1024", "spp_per_step": step_spp,
            "spp_per_s": round(spp_total / (ms * 1e-3), 2),
            "msamples_per_s": round(W * H * spp_total / (ms * 1e-3) / 1e6, 2),
-           "ms_per_spp": round(ms / spp_total, 3)}
+           "ms_per_spp": round(ms / spp_total, 3),
+           "path_vertices": vertices, "shadow_rays": shadow_rays,
+           "vertices_per_sample": round(vertices / (W * H * spp_total), 3),
+           "mrays_per_s": round((vertices + shadow_rays) / (ms * 1e-3) / 1e6, 1),
+           "roofline": {"bound": "hbm", "bytes_per_vertex": PATH_VERTEX_BYTES, "achieved": round(ach, 1),
+                        "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "peak_kind": kind}}
     t0 = time.perf_counter()
     sc.render(step_spp)
     out["e2e_ms_per_spp_host_api"] = round((time.perf_counter() - t0) * 1e3 / step_spp, 3)
@@ -270,6 +280,91 @@ def render_leg(ctx, steps, stream, with_reference=True):
             out["reference_cuda"] = {"msamples_per_s": round(W * H * frames / (rms * 1e-3) / 1e6, 3),
                                      "ms_per_spp": round(rms / frames, 2),
                                      "build": "reference renderer.cuh + Scene, nvcc -O3 -rdc sm_100a, headless"}
+    sc.close()
+    return out
+
+
+# Algorithmic bytes per path vertex of the wavefront render: extend 48
+# (ray in, hit out) + shade (hit 16 + path state 64 in, new ray 32 + path
+# state 64 out, shadow record 44) + shadow 36 + accumulation 16.
+PATH_VERTEX_BYTES = 48 + 16 + 64 + 32 + 64 + 44 + 36 + 16
+SVGF_BYTES_PER_PIXEL = 176 + 112 + 5 * 100  # temporal, variance, 5 a-trous passes (planes read + written once)
+
+
+def svgf_leg(ctx, stream, frames=4, with_reference=True):
+    """SVGF at 1920x1080 on the icosphere field: an orbiting camera
+    (0.5 deg per frame), 1-spp noisy direct/indirect and the primary-hit
+    G-buffer per frame, then one SVGF frame (temporal reprojection,
+    variance, 5 a-trous passes), timed with CUDA events. The reference's
+    own SVGF kernels (headless CUDA build) run on the same inputs, timed
+    per frame the same way. Frames after the first (which skips the
+    a-trous passes) are reported; roofline: 788 B per pixel per frame
+    (temporal 176, variance 112, a-trous 5 x 100) over the frame time."""
+    import tempfile
+
+    import torch
+
+    from cudaraytracer_b200 import Scene, Svgf, scenes
+
+    td = tempfile.mkdtemp(prefix="crt_svgf_")
+    sc = Scene.load(ctx, scenes.icosphere_field().write(td, "icospheres"))
+    rp = sc.render_params()
+    W, H = rp["width"], rp["height"]
+    shape = (H, W, 4)
+    dev = torch.device("cuda", ctx.device)
+    cam0 = sc.camera()
+    sv = Svgf(ctx, W, H)
+    ins, gbs = [], []
+    prev = None
+    for f in range(frames):
+        sc.set_camera_orbit(cam0["target"], cam0["distance"], cam0["theta_deg"], cam0["phi_deg"] + 0.5 * f,
+                            cam0["fovy_deg"])
+        d = torch.zeros(shape, device=dev)
+        i = torch.zeros(shape, device=dev)
+        sc.render_device(d, i, 1, first_sample=f, stream=stream.cuda_stream)
+        g = sc.gbuffer(prev_camera=prev, stream=stream.cuda_stream)
+        prev = sc.camera()
+        ins.append((d, i))
+        gbs.append(g)
+    torch.cuda.synchronize()
+    zero = {k: torch.zeros_like(v) for k, v in gbs[0].items()}
+    outs, ms = [], []
+    for f in range(frames):
+        od = torch.empty(shape, device=dev)
+        oi = torch.empty(shape, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sv.frame(gbs[f], gbs[f - 1] if f else zero, ins[f][0], ins[f][1], od, oi, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        outs.append((od, oi))
+    mine = float(np.median(ms[1:]))
+    px = W * H
+    from_peak, kind = measured_peaks()
+    ach = SVGF_BYTES_PER_PIXEL * px / (mine * 1e-3) / 1e9
+    out = {"workload": "icosphere field 1920x1080, 1 spp per frame, orbit 0.5 deg/frame, 5 a-trous passes",
+           "ms_per_frame": round(mine, 4), "ms_frames": [round(x, 4) for x in ms],
+           "roofline": {"bound": "hbm", "bytes_per_pixel": SVGF_BYTES_PER_PIXEL, "achieved": round(ach, 1),
+                        "peak": from_peak, "unit": "GB/s", "frac": round(ach / from_peak, 4), "peak_kind": kind}}
+    if with_reference:
+        import oracle
+
+        if oracle.ref_render_available():
+            host = lambda t: t.cpu().numpy()
+            nd = np.stack([host(d) for d, _ in ins])
+            ni = np.stack([host(i) for _, i in ins])
+            g = {k: np.stack([host(gb[k]) for gb in gbs]) for k in gbs[0]}
+            rd, ri, rms = oracle.ref_svgf(nd, ni, g["pos_tri"], g["normal_mat"].view(np.uint16),
+                                          g["bary_mesh"].view(np.uint16), g["motion_depth"], timing=True)
+            ref_ms = float(np.median(rms[1:]))
+            diff = max(float(np.abs(host(outs[f][0]) - rd[f]).max()) for f in range(frames))
+            diff = max(diff, max(float(np.abs(host(outs[f][1]) - ri[f]).max()) for f in range(frames)))
+            out["reference_cuda"] = {"ms_per_frame": round(ref_ms, 4), "ms_frames": [round(float(x), 4) for x in rms],
+                                     "build": "reference renderer.cuh SVGF kernels, nvcc -O3 -rdc sm_100a, headless",
+                                     "max_abs_diff_vs_crt": diff}
+            out["speedup_vs_reference_cuda"] = round(ref_ms / mine, 2)
+    sv.close()
     sc.close()
     return out
 
@@ -327,11 +422,14 @@ def serve_leg(ctx, quick=False):
     level-5 spheres (20k to 5.2M triangles, 2048x1024 env each). Requests
     draw resolution from {256^2, 512^2, 1280x720, 1920x1080}, spp from
     {1, 4, 16, 64} and a random orbit pose. Poisson arrivals at 5, 20 and
-    80 per second (40, 120 and 320 requests instead of 2,000 per rate) and a
-    saturated burst (160 requests at t=0), each served by crt_server
-    (continuous batching, HBM budget 150 GiB, 8M-path wavefronts) and by the
-    one-request-at-a-time loop (Scene.render_device per request) over the
-    same requests. Latency = completion - arrival (host clock)."""
+    80 per second (100, 300 and 320 requests instead of 2,000 per rate) and
+    a saturated burst (160 requests at t=0), each served by crt_server
+    (continuous batching, HBM budget 150 GiB, 8M-path wavefronts, passes
+    filled shortest-remaining-first; at 80/s and in the burst also in
+    admission order) and by the one-request-at-a-time loop
+    (Scene.render_device per request) over the same requests. Latency =
+    completion - arrival (host clock), overall and per request class
+    (resolution x spp)."""
     from cudaraytracer_b200 import Scene, scenes
     from cudaraytracer_b200.serve import Server, poisson_requests, run_one_at_a_time, run_served
 
@@ -343,12 +441,16 @@ def serve_leg(ctx, quick=False):
     res = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
     spps = [1, 4, 16, 64]
     srv = Server(ctx, hbm_budget_bytes=150 << 30, paths_per_pass=8 << 20, passes_in_flight=2)
+    fifo = Server(ctx, hbm_budget_bytes=150 << 30, paths_per_pass=8 << 20, passes_in_flight=2,
+                  schedule=Server.ADMISSION_ORDER)
     for sc in scs:
         srv.add_scene(sc)
+        fifo.add_scene(sc)
     warm = poisson_requests(8, 0.0, cams, res, [1, 4], seed=99)
     run_served(srv, warm)
+    run_served(fifo, warm)
     run_one_at_a_time(scs, warm)
-    plan = [(5.0, 40), (20.0, 120), (80.0, 320)] if not quick else [(80.0, 48)]
+    plan = [(5.0, 100), (20.0, 300), (80.0, 320)] if not quick else [(80.0, 48)]
     out = {"workload": "8 resident icosphere-field scenes (1..256 level-5 spheres, 20k-5.2M tris); requests of "
                        "{256^2, 512^2, 1280x720, 1920x1080} x {1, 4, 16, 64} spp, random poses",
            "scenes_tris": [int(sc.info()["num_triangles"]) for sc in scs], "scene_build_s": round(load_s, 2),
@@ -356,15 +458,22 @@ def serve_leg(ctx, quick=False):
     for rate, n in plan:
         reqs = poisson_requests(n, rate, cams, res, spps, seed=int(rate))
         served = run_served(srv, reqs)
-        plain = run_one_at_a_time(scs, reqs)
-        out["rates"][f"{rate:g}/s"] = {"served": served, "one_at_a_time": plain}
+        leg = {"served": served}
+        if rate >= 80.0:
+            leg["served_admission_order"] = run_served(fifo, reqs)
+        leg["one_at_a_time"] = run_one_at_a_time(scs, reqs)
+        out["rates"][f"{rate:g}/s"] = leg
     burst = poisson_requests(160 if not quick else 32, 0.0, cams, res, spps, seed=7)
     served = run_served(srv, burst)
+    served_fifo = run_served(fifo, burst)
     plain = run_one_at_a_time(scs, burst)
-    out["saturated"] = {"served": served, "one_at_a_time": plain,
+    out["saturated"] = {"served": served, "served_admission_order": served_fifo, "one_at_a_time": plain,
                         "req_per_s_ratio": round(served["req_per_s"] / plain["req_per_s"], 3)}
+    out["schedule"] = "served: shortest remaining paths first (oldest request keeps half of each pass); " \
+                      "served_admission_order: first come, first served"
     out["server_stats"] = {k: v for k, v in srv.stats().items() if k in ("passes", "paths")}
     srv.close()
+    fifo.close()
     for sc in scs:
         sc.close()
     return out
@@ -416,56 +525,132 @@ def conv_leg(ctx, h=1080, w=1920, cin=64, cout=64, reps=10):
     return out
 
 
-def denoise_leg(ctx):
-    """Learned denoiser (the learned-denoiser workload on a bounded sample): the KPCN is
-    trained on the GPU on 64 views of seeded Cornell variants (scene seeds
-    100-131, 256x256, 1-16 spp inputs, 1024-spp references) for 1500 Adam
-    steps of 8 random 128x128 crops, then evaluated on unseen scenes (seeds
-    200-207, one 256x256 view each) by relMSE against 4096-spp references:
-    raw and KPCN at 1-32 spp, SVGF at 64 spp. The smallest spp at which the
-    KPCN matches 64 spp + SVGF then sets the learned pipeline of the
-    requests/s comparison: 32 requests at 512x512 served through the
-    multi-scene server at that spp + KPCN, against the one-request-at-a-time
-    loop of 64 spp + SVGF."""
+def kpcn_layers_leg(ctx, reps=10):
+    """The denoiser network at 1920x1080: each of its 11 convolutions
+    timed alone at its own resolution (full, 1/2, 1/4) and channel counts
+    (forward, bias + ReLU), and the whole forward pass of one frame
+    (convolutions, pooling, upsampling, softmax filter). FLOPs per
+    convolution = 2 * 9 * cin * cout * pixels."""
+    import torch
+
+    from cudaraytracer_b200 import kpcn
+    from cudaraytracer_b200.kpcn import Kpcn
+
+    H, W = 1080, 1920
+    scale = {"e0a": 1, "e0b": 1, "e1a": 2, "e1b": 2, "e2a": 4, "e2b": 4, "d1a": 2, "d1b": 2, "d0a": 1, "d0b": 1,
+             "out": 1}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = float(json.load(open(pp))["bf16_tflops"]) if os.path.exists(pp) else 1590.0
+    g = torch.Generator(device="cuda").manual_seed(1)
+    layers, total_ms, total_flop = {}, 0.0, 0.0
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    for name, (cin, cout) in zip(Kpcn.LAYERS, Kpcn.SPEC):
+        h, w = H // scale[name], W // scale[name]
+        x = torch.randn((1, h, w, cin), device="cuda", generator=g).to(torch.bfloat16)
+        wt = (torch.randn((9, cout, cin), device="cuda", generator=g) / 24).to(torch.bfloat16)
+        b = torch.zeros(cout, device="cuda")
+        y = torch.empty((1, h, w, cout), dtype=torch.bfloat16, device="cuda")
+        ms = timed(lambda: kpcn.conv3x3_forward(ctx, x, wt, b, relu=name != "out", out=y))
+        flop = 2.0 * 9 * cin * cout * h * w
+        total_ms += ms
+        total_flop += flop
+        layers[name] = {"shape": f"{w}x{h}, {cin}->{cout}", "ms": round(ms, 4),
+                        "tflops": round(flop / (ms * 1e-3) / 1e12, 1), "frac": round(flop / (ms * 1e-3) / 1e12 / peak, 4)}
+        del x, wt, y
+    net = Kpcn(ctx, seed=0)
+    feat = torch.randn((1, H, W, 16), device="cuda", generator=g).to(torch.bfloat16)
+    noisy = torch.rand((1, H, W, 4), device="cuda", generator=g)
+    out = torch.empty((1, H, W, 4), device="cuda")
+    fwd = timed(lambda: net.forward(feat, noisy, out=out))
+    net.close()
+    kpcn.check_device_errors(ctx)
+    return {"resolution": [W, H], "layers": layers, "conv_ms_sum": round(total_ms, 4),
+            "conv_gflop": round(total_flop / 1e9, 1), "conv_tflops": round(total_flop / (total_ms * 1e-3) / 1e12, 1),
+            "conv_frac": round(total_flop / (total_ms * 1e-3) / 1e12 / peak, 4), "forward_ms_per_frame": round(fwd, 4),
+            "peak_tflops": peak}
+
+
+def denoise_leg(ctx, train_steps=1500):
+    """Learned denoiser against SVGF (the learned-denoiser workload, at
+    256x256 instead of 1920x1080 and 16-frame instead of 60-frame
+    sequences so the 4096-spp references fit the bench): the KPCN is
+    trained on the GPU on 128 views of seeded Cornell variants (scene seeds
+    100-163, two views each, 1-16 spp inputs, 4096-spp references) for
+    1500 Adam steps of 8 random 128x128 crops. Test: one 16-frame orbit
+    sequence (1.5 deg per frame) per unseen scene (seeds 200-207), relMSE
+    of every frame against its 4096-spp reference for raw and KPCN at 1-32
+    spp and for SVGF run temporally over the sequence at 1 and 64 spp.
+    The smallest spp at which KPCN matches 64 spp + temporal SVGF sets the
+    learned pipeline. Serving (same 256x256 frames, same sequences): the
+    plain loop (one request at a time: 64 spp render, G-buffer, SVGF frame
+    with the sequence's state) against the learned pipeline (requests
+    through the multi-scene server at the matching spp, finished requests'
+    KPCN batched), both for a burst of all 128 frames at t = 0
+    (throughput) and for Poisson arrivals at 70% of the plain loop's
+    throughput (latency)."""
     import torch
 
     from cudaraytracer_b200 import denoise as D
     from cudaraytracer_b200.kpcn import Kpcn
 
+    res = 256
     t0 = time.perf_counter()
-    data = D.build_dataset(ctx, range(100, 132), 2, 256, 256, [1, 2, 4, 8, 16], 1024, seed=0)
+    data = D.build_dataset(ctx, range(100, 164), 2, res, res, [1, 2, 4, 8, 16], 4096, seed=0)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     net = Kpcn(ctx, seed=0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    losses = D.train(net, data, 1500, batch=8, crop=128, lr=1e-3)
+    losses = D.train(net, data, train_steps, batch=8, crop=128, lr=1e-3)
     e1.record()
     torch.cuda.synchronize()
     t2 = time.perf_counter()
+    del data
     spp_list = [1, 2, 4, 8, 16, 32]
-    tab = D.evaluate(ctx, net, range(200, 208), 256, 256, spp_list)
-    k = D.matching_spp(tab, spp_list)
-    thr = D.pipeline_throughput(ctx, net, range(200, 208), 512, 512, 32, k or 32)
-    # training throughput: pixels x (forward + backward) per second
-    px = 1500 * 8 * 128 * 128
+    frames = 16
+    tab = D.evaluate_sequences(ctx, net, range(200, 208), res, res, frames, spp_list, svgf_spp_list=(1, 64))
+    t3 = time.perf_counter()
+    k = D.matching_spp(tab, spp_list) or 32
+    scs, burst = D.sequence_requests(ctx, range(200, 208), res, res, frames, 0.0)
+    D.run_plain_svgf_loop(ctx, scs, burst[:8], res, res)  # warm-up
+    D.run_learned_served(ctx, net, scs, burst[:8], res, res, k)
+    plain_b = D.run_plain_svgf_loop(ctx, scs, burst, res, res)
+    learned_b = D.run_learned_served(ctx, net, scs, burst, res, res, k)
+    rate = 0.7 * plain_b["req_per_s"]
+    for sc in scs:
+        sc.close()
+    scs, pois = D.sequence_requests(ctx, range(200, 208), res, res, frames, rate, seed=1)
+    plain_p = D.run_plain_svgf_loop(ctx, scs, pois, res, res)
+    learned_p = D.run_learned_served(ctx, net, scs, pois, res, res, k)
+    for sc in scs:
+        sc.close()
+    px = train_steps * 8 * 128 * 128
     net.close()
-    return {"workload": "Cornell variants: train seeds 100-131 (64 views, 256^2, 1-16 spp, 1024-spp refs), "
-                        "test seeds 200-207 (256^2, 4096-spp refs)",
-            "dataset_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2), "train_steps": 1500,
+    return {"workload": f"Cornell variants at {res}x{res}: train seeds 100-163 (2 views each, 1-16 spp, 4096-spp refs); "
+                        f"test: {frames}-frame orbit sequences of seeds 200-207, 4096-spp refs per frame",
+            "dataset_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2), "eval_s": round(t3 - t2, 2),
+            "train_steps": train_steps,
             "train_mpix_per_s": round(px / (e0.elapsed_time(e1) * 1e-3) / 1e6, 1),
             "loss_first": round(float(sum(losses[:20]) / 20), 5), "loss_last": round(float(sum(losses[-50:]) / 50), 5),
-            "relmse": {k2: round(v, 6) for k2, v in tab.items()}, "kpcn_spp_matching_svgf64": k,
-            "throughput": thr}
-
-
-def bench_config(world):
-    """The workload description both arms print (the same dict, so the two
-    lines name one configuration)."""
-    return {"workload": "icosphere field (64 x level-5 icospheres, 1,310,720 tris); per GPU and step "
-                        "16M closest-hit rays + 16M shadow queries (1:1 extend:shadow)",
-            "l2": "inputs 1.28 GB per step > 126 MB L2 (no flush needed)",
-            "parallelism": f"replicas x{world}"}
+            "relmse": {k2: (round(v, 6) if not isinstance(v, dict) else {a: round(b, 6) for a, b in v.items()})
+                       for k2, v in tab.items()},
+            "kpcn_spp_matching_svgf64": k,
+            "serving": {"resolution": [res, res], "learned_spp": k, "plain_spp": 64,
+                        "burst": {"plain_svgf": plain_b, "learned_kpcn": learned_b,
+                                  "req_per_s_ratio": round(learned_b["req_per_s"] / plain_b["req_per_s"], 2)},
+                        "poisson": {"rate_per_s": round(rate, 1), "plain_svgf": plain_p, "learned_kpcn": learned_p}}}
 
 
 def run_reference(args, rank, world):
@@ -524,11 +709,14 @@ def main():
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA traversal")
     ap.add_argument("--no-cornell", action="store_true", help="skip the Cornell-box 1M+1M traversal leg")
     ap.add_argument("--no-render", action="store_true", help="skip the full-frame render leg")
+    ap.add_argument("--no-svgf", action="store_true", help="skip the 1080p SVGF leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the multi-scene serving leg")
     ap.add_argument("--no-denoise", action="store_true", help="skip the learned-denoiser leg")
-    ap.add_argument("--only", choices=["conv"], default=None,
-                    help="run one micro-benchmark alone (conv: the tensor-core convolutions at 1080p)")
+    ap.add_argument("--only", choices=["conv", "kpcn", "svgf", "render", "cornell", "serve", "denoise"], default=None,
+                    help="run one leg alone: conv (tensor-core convolutions at 1080p), kpcn (the denoiser's "
+                         "layers at 1080p), svgf (1080p SVGF), render (1080p render), cornell (Cornell-box "
+                         "traversal), serve (serving), denoise (learned denoiser vs SVGF)")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays (and shadow queries) per step per GPU")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -538,14 +726,22 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.only == "conv":
+    if args.only is not None:
         import torch
 
         from cudaraytracer_b200 import Context
 
         torch.cuda.set_device(local_rank)
         ctx = Context(local_rank)
-        print(json.dumps({"conv": conv_leg(ctx, reps=args.steps)}))
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        legs = {"conv": lambda: conv_leg(ctx, reps=args.steps), "kpcn": lambda: kpcn_layers_leg(ctx),
+                "svgf": lambda: svgf_leg(ctx, stream, with_reference=not args.no_ref_cuda),
+                "render": lambda: render_leg(ctx, max(2, min(args.steps, 8)), stream,
+                                             with_reference=not args.no_ref_cuda),
+                "cornell": lambda: cornell_trace_leg(ctx, stream, with_reference=not args.no_ref_cuda),
+                "serve": lambda: serve_leg(ctx), "denoise": lambda: denoise_leg(ctx)}
+        print(json.dumps({args.only: legs[args.only]()}))
         ctx.close()
         return
 
@@ -616,6 +812,9 @@ def main():
     render = None
     if rank == 0 and not args.no_render:
         render = render_leg(ctx, max(2, min(args.steps, 8)), stream, with_reference=not args.no_ref_cuda)
+    svgf = None
+    if rank == 0 and not args.no_svgf:
+        svgf = svgf_leg(ctx, stream, with_reference=not args.no_ref_cuda)
     batch = None
     if rank == 0 and not args.no_batch:
         batch = batch_leg(ctx, stream)
@@ -626,6 +825,7 @@ def main():
     if rank == 0 and not args.no_denoise:
         denoise = denoise_leg(ctx)
         denoise["conv"] = conv_leg(ctx)
+        denoise["kpcn_1080p"] = kpcn_layers_leg(ctx)
 
     # e2e through the host-buffer API: pinned host inputs, results back.
     pin_r = torch.from_numpy(rays_np).pin_memory()
@@ -694,6 +894,7 @@ def main():
             "reference_cuda": ref_cuda,
             "cornell_trace": cornell,
             "render": render,
+            "svgf": svgf,
             "batch": batch,
             "serve": serve,
             "denoise": denoise,

@@ -167,6 +167,7 @@ class ServerConfig(C.Structure):
         ("paths_per_pass", C.c_int32),
         ("max_requests", C.c_int32),
         ("passes_in_flight", C.c_int32),
+        ("schedule", C.c_int32),
     ]
 
 

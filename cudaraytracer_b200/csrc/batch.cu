@@ -115,10 +115,12 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
             const int in = b & 1, out = 1 - in;
             StepParams bp = sp;
             bp.bounce = b;
-            k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], sc.wf.counters + in, sc.wf.hits, sc.wf.counters, out);
+            k_extend<<<g_ext, blk, 0, s>>>(stage_bvh(view.bvh), q[in], sc.wf.counters + in, sc.wf.hits, sc.wf.counters,
+                                           out);
             k_shade<<<g_sh, blk, 0, s>>>(view, bp, q[in], sc.wf.hits, sc.wf.counters + in, q[out], sc.wf.counters,
                                          out, sh, sc.wf.term[0], sc.wf.term[1], av);
-            k_shadow<<<g_sd, blk, 0, s>>>(view.bvh, sh, sc.wf.counters, q[out], sc.wf.term[0], sc.wf.term[1], av);
+            k_shadow<<<g_sd, blk, 0, s>>>(stage_bvh(view.bvh), sh, sc.wf.counters, q[out], sc.wf.term[0], sc.wf.term[1],
+                                          av);
         }
         k_advance_pass<<<1, 1, 0, s>>>(d_pass, chunk);
     };

@@ -371,6 +371,10 @@ __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *co
 // tMin 0, closest starts at 1e8). Also clears the next bounce's counters.
 __global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters,
                                                 int out_idx) {
+    __shared__ unsigned s_stack[kStageShort * kStageMaxBlock];
+    ShortStack<kStageShort> st;
+    st.col = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
     const int n = *n_in;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         counters[out_idx] = 0;
@@ -380,7 +384,9 @@ __global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const 
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = q.p[0][i], b = q.p[1][i];
-        Hit h = closest_hit<false>(bvh, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, 0.f, kTriTMax);
+        const V3 o{a.x, a.y, a.z}, d{b.x, b.y, b.z};
+        Hit h = bvh.wnodes ? closest_hit8<false, kStageShort>(bvh, st, o, d, 0.f, kTriTMax)
+                           : closest_hit<false>(bvh, o, d, 0.f, kTriTMax);
         hits[i] = make_float4(h.t, __int_as_float(h.slot), h.b1, h.b2);
     }
 }
@@ -442,13 +448,18 @@ __global__ void __launch_bounds__(256) k_shade(SceneView s, StepParams sp, Queue
 // already terminated is then added to its pixel.
 __global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueView qout,
                                                 float4 *term0, float4 *term1, AccumView acc) {
+    __shared__ unsigned s_stack[kStageShort * kStageMaxBlock];
+    ShortStack<kStageShort> st;
+    st.col = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
     const int n = counters[2];
     if (blockIdx.x == 0 && threadIdx.x == 0)
         atomicAdd(reinterpret_cast<unsigned long long *>(const_cast<int *>(counters) + kShadowRaysCounter),
                   (unsigned long long)n);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = sh.r[0][i], b = sh.r[1][i], c = sh.r[2][i], d = sh.r[3][i];
-        bool vis = visible(bvh, V3{a.x, a.y, a.z}, V3{a.w, b.x, b.y}, V3{b.z, b.w, c.x}, V3{c.y, c.z, c.w});
+        const V3 hp{a.x, a.y, a.z}, hn{a.w, b.x, b.y}, lp{b.z, b.w, c.x}, ln{c.y, c.z, c.w};
+        const bool vis = bvh.wnodes ? visible8<kStageShort>(bvh, st, hp, hn, lp, ln) : visible(bvh, hp, hn, lp, ln);
         uint32_t target = __float_as_uint(d.w);
         uint32_t idx = target & kIndexMask;
         bool direct = (target & kDirectBit) != 0;
@@ -481,6 +492,12 @@ __global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, cons
             }
         }
     }
+}
+
+BvhView stage_bvh(BvhView v) {
+    const char *e = getenv("CRT_TRAVERSAL");
+    if (e && atoi(e) == 2) v.wnodes = nullptr;
+    return v;
 }
 
 int persistent_grid(const void *kernel, int block) {
@@ -519,6 +536,7 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
         for (int k = 0; k < 5; ++k) q[j].p[k] = wf.q[j][k];
     ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
     const int blk = rp.block();
+    const BvhView sbvh = stage_bvh(view.bvh);
     const int g_ext = persistent_grid((const void *)k_extend, blk);
     const int g_sh = persistent_grid((const void *)k_shade, blk);
     const int g_sd = persistent_grid((const void *)k_shadow, blk);
@@ -538,10 +556,10 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
         for (int b = 0; b < rp.max_bounces; ++b) {
             int in = b & 1, out = 1 - in;
             sp.bounce = b;
-            k_extend<<<g_ext, blk, 0, stream>>>(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out);
+            k_extend<<<g_ext, blk, 0, stream>>>(sbvh, q[in], wf.counters + in, wf.hits, wf.counters, out);
             k_shade<<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out], wf.counters, out, sh,
                                               wf.term[0], wf.term[1], av);
-            k_shadow<<<g_sd, blk, 0, stream>>>(view.bvh, sh, wf.counters, q[out], wf.term[0], wf.term[1], av);
+            k_shadow<<<g_sd, blk, 0, stream>>>(sbvh, sh, wf.counters, q[out], wf.term[0], wf.term[1], av);
             launches += 3;
         }
         CRT_CUDA(cudaGetLastError());

@@ -51,4 +51,15 @@ __global__ void k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueV
 // occupancy).
 int persistent_grid(const void *kernel, int block);
 
+// Traversal stack entries per thread kept in shared memory by the extend
+// and shadow stages (8-wide tree; deeper entries spill to local memory),
+// and the largest block those stages are launched with.
+constexpr int kStageShort = 8;
+constexpr int kStageMaxBlock = 256;
+
+// The BVH view the stage kernels get: the 8-wide tree when the scene has
+// one (always, after build_bvh), unless CRT_TRAVERSAL=2 selects the binary
+// tree with its local-memory stack.
+BvhView stage_bvh(BvhView v);
+
 }  // namespace crt

@@ -88,6 +88,10 @@ __global__ void ks_raygen(const ReqDesc *reqs, const Segment *segs, int nseg, in
 
 __global__ void __launch_bounds__(128) ks_extend(const SceneView *scenes, QueueView q, const int *n_in, float4 *hits,
                                                  int *counters, int out_idx) {
+    __shared__ unsigned s_stack[kStageShort * 128];
+    ShortStack<kStageShort> st;
+    st.col = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         counters[out_idx] = 0;
         counters[2] = 0;
@@ -97,7 +101,9 @@ __global__ void __launch_bounds__(128) ks_extend(const SceneView *scenes, QueueV
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = q.p[0][i], b = q.p[1][i];
         const BvhView bvh = scenes[path_tag(q, i) >> kSlotBits].bvh;
-        Hit h = closest_hit<false>(bvh, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, 0.f, kTriTMax);
+        const V3 o{a.x, a.y, a.z}, d{b.x, b.y, b.z};
+        Hit h = bvh.wnodes ? closest_hit8<false, kStageShort>(bvh, st, o, d, 0.f, kTriTMax)
+                           : closest_hit<false>(bvh, o, d, 0.f, kTriTMax);
         hits[i] = make_float4(h.t, __int_as_float(h.slot), h.b1, h.b2);
     }
 }
@@ -173,6 +179,10 @@ __global__ void __launch_bounds__(128) ks_shade(const SceneView *scenes, const R
 // it belongs to; then as k_shadow in render.cu.
 __global__ void __launch_bounds__(128) ks_shadow(const SceneView *scenes, const ReqDesc *reqs, ShadowView sh,
                                                  const int *counters, QueueView qout, float4 *term0, float4 *term1) {
+    __shared__ unsigned s_stack[kStageShort * 128];
+    ShortStack<kStageShort> st;
+    st.col = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
     const int n = counters[2];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 d = sh.r[3][i];
@@ -181,8 +191,9 @@ __global__ void __launch_bounds__(128) ks_shadow(const SceneView *scenes, const 
         const bool term = (target & kTermBit) != 0;
         const uint32_t tag = term ? __float_as_uint(term1[idx].w) : path_tag(qout, idx);
         float4 a = sh.r[0][i], b = sh.r[1][i], c = sh.r[2][i];
-        bool vis = visible(scenes[tag >> kSlotBits].bvh, V3{a.x, a.y, a.z}, V3{a.w, b.x, b.y}, V3{b.z, b.w, c.x},
-                           V3{c.y, c.z, c.w});
+        const BvhView bvh = scenes[tag >> kSlotBits].bvh;
+        const V3 hp{a.x, a.y, a.z}, hn{a.w, b.x, b.y}, lp{b.z, b.w, c.x}, ln{c.y, c.z, c.w};
+        const bool vis = bvh.wnodes ? visible8<kStageShort>(bvh, st, hp, hn, lp, ln) : visible(bvh, hp, hn, lp, ln);
         bool direct = (target & kDirectBit) != 0;
         V3 C{d.x, d.y, d.z};
         if (term) {
@@ -219,6 +230,7 @@ __global__ void __launch_bounds__(128) ks_shadow(const SceneView *scenes, const 
 size_t scene_device_bytes(const Scene &sc) {
     const size_t n = (size_t)sc.bvh.num_tris;
     size_t b = (size_t)sc.bvh.num_nodes * 64 + n * 48 + n * 4;  // nodes, leaf-order triangles, slot_of_prim
+    b += (size_t)sc.bvh.num_wide_nodes * (64 + 32);            // 8-wide nodes and their child links
     b += n * 36;                                              // input vertices
     b += n * 64;                                              // shading attributes
     b += sc.host.meshes.size() * sizeof(DMesh) + sc.host.materials.size() * sizeof(DMaterial) +
@@ -261,12 +273,13 @@ struct crt_server {
     SceneView *d_scenes = nullptr;
     Wavefront wf;
     ReqDesc *d_reqs = nullptr, *h_reqs = nullptr;  // h_reqs: pinned staging, one entry per slot
-    Segment *d_segs = nullptr, *h_segs = nullptr;  // (passes_in_flight + 1) tables of max_requests entries
+    Segment *d_segs = nullptr, *h_segs = nullptr;  // (passes_in_flight + 1) tables of max_requests + 1 entries
     std::vector<cudaEvent_t> events;
     std::deque<Pass> inflight;
     int64_t pass_seq = 0, paths_done = 0, next_id = 1;
     std::deque<Request *> queued;
     std::vector<Request *> active;  // admitted, paths left to enqueue, admission order
+    std::vector<Request *> order;   // scratch: active sorted by paths left
     std::unordered_map<int64_t, Request *> reqs;
     std::vector<int> free_slots;
     std::multimap<size_t, float4 *> pool;  // released accumulator buffers by size
@@ -368,15 +381,18 @@ struct crt_server {
     void enqueue_pass() {
         const int cap = cfg.paths_per_pass;
         const int table = (int)(pass_seq % (cfg.passes_in_flight + 1));
-        Segment *hs = h_segs + (size_t)table * cfg.max_requests;
-        Segment *ds = d_segs + (size_t)table * cfg.max_requests;
+        // a pass holds at most one segment per admitted request, plus the
+        // oldest request's second segment under shortest-first filling
+        Segment *hs = h_segs + (size_t)table * (cfg.max_requests + 1);
+        Segment *ds = d_segs + (size_t)table * (cfg.max_requests + 1);
         int n = 0, nseg = 0, max_b = 0;
         Pass pass;
         pass.ev = events[table];
-        size_t k = 0;
-        for (; k < active.size() && n < cap; ++k) {
-            Request *r = active[k];
-            const int64_t take = std::min<int64_t>(r->total - r->next, cap - n);
+        // one segment: the next `limit` (at most) paths of r
+        auto add = [&](Request *r, int64_t limit) {
+            const int64_t take = std::min<int64_t>(std::min<int64_t>(r->total - r->next, limit), cap - n);
+            if (take <= 0) return;
+            CRT_CHECK(nseg <= cfg.max_requests, CRT_ERR_CAPACITY, "crt_server: pass segment table full");
             hs[nseg].begin = r->next;
             hs[nseg].prefix = n;
             hs[nseg].tag = ((uint32_t)r->scene << kSlotBits) | (uint32_t)r->slot;
@@ -385,6 +401,16 @@ struct crt_server {
             n += (int)take;
             max_b = std::max(max_b, r->desc.max_bounces);
             if (r->next == r->total) pass.finishing.push_back(r->id);
+        };
+        if (cfg.schedule == CRT_SCHED_ADMISSION_ORDER) {
+            for (size_t k = 0; k < active.size() && n < cap; ++k) add(active[k], cap);
+        } else {
+            // the oldest request's guaranteed share, then fewest paths left first
+            add(active[0], cap / 2);
+            order.assign(active.begin(), active.end());
+            std::stable_sort(order.begin(), order.end(),
+                             [](const Request *a, const Request *b) { return a->total - a->next < b->total - b->next; });
+            for (size_t k = 0; k < order.size() && n < cap; ++k) add(order[k], cap);
         }
         active.erase(std::remove_if(active.begin(), active.end(), [](Request *r) { return r->next == r->total; }),
                      active.end());
@@ -442,6 +468,8 @@ extern "C" crt_status crt_server_create(crt_ctx *ctx, const crt_server_config *c
         CRT_CHECK(c.max_requests <= (1 << kSlotBits), CRT_ERR_INVALID, "crt_server_create: max_requests > 2^20");
         CRT_CHECK(c.paths_per_pass <= (int)kIndexMask, CRT_ERR_INVALID, "crt_server_create: paths_per_pass > 2^30");
         CRT_CHECK(c.passes_in_flight <= 64, CRT_ERR_INVALID, "crt_server_create: passes_in_flight > 64");
+        CRT_CHECK(c.schedule == CRT_SCHED_SHORTEST_FIRST || c.schedule == CRT_SCHED_ADMISSION_ORDER, CRT_ERR_INVALID,
+                  "crt_server_create: unknown schedule");
         s->cfg = c;
         s->bytes_wavefront = kWavefrontBytesPerPath * (size_t)c.paths_per_pass;
         CRT_CHECK(s->bytes_wavefront < (size_t)c.hbm_budget_bytes, CRT_ERR_CAPACITY,
@@ -452,7 +480,7 @@ extern "C" crt_status crt_server_create(crt_ctx *ctx, const crt_server_config *c
         CRT_CUDA(cudaMalloc(&s->d_scenes, sizeof(SceneView) * kMaxScenes));
         CRT_CUDA(cudaMalloc(&s->d_reqs, sizeof(ReqDesc) * c.max_requests));
         CRT_CUDA(cudaHostAlloc(&s->h_reqs, sizeof(ReqDesc) * c.max_requests, cudaHostAllocDefault));
-        const size_t nseg = (size_t)(c.passes_in_flight + 1) * c.max_requests;
+        const size_t nseg = (size_t)(c.passes_in_flight + 1) * (c.max_requests + 1);
         CRT_CUDA(cudaMalloc(&s->d_segs, sizeof(Segment) * nseg));
         CRT_CUDA(cudaHostAlloc(&s->h_segs, sizeof(Segment) * nseg, cudaHostAllocDefault));
         s->events.resize(c.passes_in_flight + 1);
@@ -484,6 +512,7 @@ extern "C" crt_status crt_server_add_scene(crt_server *srv, crt_scene *scene, in
                   CRT_ERR_CAPACITY, "crt_server_add_scene: scene does not fit the HBM budget");
         CRT_CUDA(cudaSetDevice(srv->ctx->device));
         SceneView v = make_view(scene->bvh, scene->rd);
+        v.bvh = stage_bvh(v.bvh);
         const int id = (int)srv->scenes.size();
         CRT_CUDA(cudaMemcpy(srv->d_scenes + id, &v, sizeof(v), cudaMemcpyHostToDevice));
         srv->scenes.push_back(scene);

@@ -2,6 +2,7 @@
 // wavefront shade stage.
 #pragma once
 #include "bvh.cuh"
+#include "bvh8.cuh"
 
 namespace crt {
 
@@ -58,6 +59,15 @@ __device__ __forceinline__ bool visible(const BvhView &bvh, V3 hp, V3 hn, V3 lp,
     ShadowRay r;
     shadow_ray_init(r, hp, hn, lp, ln);
     Hit hit = closest_hit<true>(bvh, r.o, r.dir, 1e-6f, 1e8f, r.t_exit);
+    return shadow_ray_visible(r, bvh, hit);
+}
+
+// visible() over the 8-wide tree with a short stack (bvh8.cuh).
+template <int kShort>
+__device__ __forceinline__ bool visible8(const BvhView &bvh, ShortStack<kShort> &st, V3 hp, V3 hn, V3 lp, V3 ln) {
+    ShadowRay r;
+    shadow_ray_init(r, hp, hn, lp, ln);
+    Hit hit = closest_hit8<true, kShort>(bvh, st, r.o, r.dir, 1e-6f, 1e8f, r.t_exit);
     return shadow_ray_visible(r, bvh, hit);
 }
 

@@ -266,6 +266,188 @@ def pipeline_throughput(ctx, net: Kpcn, scene_seeds, width: int, height: int, n_
             "req_per_s_ratio": round(plain_s / learned_s, 3)}
 
 
+def orbit_sequence(scene: Scene, frames: int, seed: int, dphi_deg: float = 1.5):
+    """Cameras of an orbit sequence: a seeded start pose (view_cameras) and
+    an azimuth step of dphi_deg per frame."""
+    c0 = view_cameras(scene, 1, seed)[0]
+    return [dict(c0, phi_deg=c0["phi_deg"] + dphi_deg * f) for f in range(frames)]
+
+
+def evaluate_sequences(ctx, net: Kpcn, scene_seeds, width: int, height: int, frames: int, spp_list,
+                       svgf_spp_list=(1, 64), ref_spp: int = 4096):
+    """relMSE against a ref_spp reference of every frame of an orbit
+    sequence per test scene: raw and KPCN (per frame) at every spp of
+    spp_list, and SVGF run as the reference runs it, temporally over the
+    sequence (one Svgf state per sequence carried from frame to frame,
+    G-buffer motion against the previous frame), at every spp of
+    svgf_spp_list. Returns {method_spp: mean relMSE over all frames} and the
+    same over the frames from the fifth on under "steady"."""
+    import torch
+
+    from . import scenes
+
+    keys = [f"raw_{k}" for k in spp_list] + [f"kpcn_{k}" for k in spp_list]
+    keys += [f"svgf_{k}" for k in svgf_spp_list] + [f"raw_{k}" for k in svgf_spp_list if k not in spp_list]
+    acc = {k: [] for k in keys}
+    steady = {k: [] for k in keys}
+    for s in scene_seeds:
+        sc = Scene.from_spec(ctx, scenes.cornell_box(width=width, height=height, seed=int(s)))
+        cams = orbit_sequence(sc, frames, int(s) * 7 + 3)
+        states = {k: Svgf(ctx, width, height) for k in svgf_spp_list}
+        prev = None
+        for f, cam in enumerate(cams):
+            rd, ri = render_view(sc, cam, width, height, ref_spp, seed=int(s), first_sample=REF_FIRST_SAMPLE)
+            ref = (rd + ri) / ref_spp
+            g_still = sc.gbuffer()
+            g_motion = sc.gbuffer(prev_camera=prev)
+            res = {}
+            for k in sorted(set(list(spp_list) + list(svgf_spp_list))):
+                d, i = render_view(sc, cam, width, height, k, seed=int(s) * 1000 + f)
+                if k in spp_list:
+                    feat, noisy = make_features(sc, g_still, d, i, k, DEPTH_SCALE)
+                    out = net.forward(feat[None].contiguous(), noisy[None].contiguous())[0]
+                    res[f"raw_{k}"] = relmse(noisy, ref)
+                    res[f"kpcn_{k}"] = relmse(out, ref)
+                if k in svgf_spp_list:
+                    nd, ni = (d / k).contiguous(), (i / k).contiguous()
+                    od, oi = torch.empty_like(nd), torch.empty_like(ni)
+                    states[k].frame(g_motion, prev_g if f else g_motion, nd, ni, od, oi)
+                    res[f"svgf_{k}"] = relmse(od + oi, ref)
+                    if k not in spp_list:
+                        res[f"raw_{k}"] = relmse(nd + ni, ref)
+            for k2, v in res.items():
+                acc[k2].append(v)
+                if f >= 4:
+                    steady[k2].append(v)
+            prev = sc.camera()
+            prev_g = g_motion
+        torch.cuda.synchronize()
+        for st in states.values():
+            st.close()
+        sc.close()
+    out = {k: float(np.mean(v)) for k, v in acc.items() if v}
+    out["steady"] = {k: float(np.mean(v)) for k, v in steady.items() if v}
+    return out
+
+
+def sequence_requests(ctx, scene_seeds, width: int, height: int, frames: int, rate_per_s: float, seed: int = 0):
+    """Requests for the frames of one orbit sequence per scene, interleaved
+    by frame (frame f of every sequence before frame f + 1), arriving as a
+    Poisson process at rate_per_s (all at t = 0 when rate_per_s is 0).
+    Returns (scenes, requests) with requests as dicts (scene index,
+    sequence frame, camera, seed, arrival_s)."""
+    from . import scenes
+
+    scs = [Scene.from_spec(ctx, scenes.cornell_box(width=width, height=height, seed=int(s))) for s in scene_seeds]
+    seqs = [orbit_sequence(sc, frames, int(s) * 7 + 3) for sc, s in zip(scs, scene_seeds)]
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    reqs = []
+    for f in range(frames):
+        for si in range(len(scs)):
+            t += rng.exponential(1.0 / rate_per_s) if rate_per_s > 0 else 0.0
+            reqs.append({"scene": si, "frame": f, "camera": seqs[si][f], "seed": 7000 + 100 * si + f, "arrival_s": t})
+    return scs, reqs
+
+
+def _lat_summary(lat, wall, n):
+    a = np.sort(np.asarray(lat))
+    return {"requests": n, "wall_s": round(wall, 4), "req_per_s": round(n / wall, 2),
+            "p50_ms": round(float(np.percentile(a, 50)) * 1e3, 2), "p99_ms": round(float(np.percentile(a, 99)) * 1e3, 2),
+            "mean_ms": round(float(a.mean()) * 1e3, 2)}
+
+
+def run_plain_svgf_loop(ctx, scs, reqs, width: int, height: int, spp: int = 64):
+    """The plain loop, one request at a time in arrival order: render spp
+    samples of the frame, its G-buffer (motion against its sequence's
+    previous frame) and one SVGF frame with its sequence's temporal state;
+    latency = completion - arrival (host clock, GPU synchronised)."""
+    import torch
+
+    states = [Svgf(ctx, width, height) for _ in scs]
+    last = [None] * len(scs)
+    lat = []
+    t0 = time.perf_counter()
+    for r in reqs:
+        now = time.perf_counter() - t0
+        if r["arrival_s"] > now:
+            time.sleep(r["arrival_s"] - now)
+        si = r["scene"]
+        sc = scs[si]
+        d, i = render_view(sc, r["camera"], width, height, spp, r["seed"])
+        prev_cam, prev_g = last[si] if last[si] is not None else (None, None)
+        g = sc.gbuffer(prev_camera=prev_cam)
+        nd, ni = (d / spp).contiguous(), (i / spp).contiguous()
+        od, oi = torch.empty_like(nd), torch.empty_like(ni)
+        states[si].frame(g, prev_g if prev_g is not None else g, nd, ni, od, oi)
+        torch.cuda.synchronize()
+        lat.append(time.perf_counter() - t0 - r["arrival_s"])
+        last[si] = (sc.camera(), g)
+    wall = time.perf_counter() - t0
+    for st in states:
+        st.close()
+    return _lat_summary(lat, wall, len(reqs))
+
+
+def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: int, paths_per_pass: int = 8 << 20):
+    """The learned pipeline, open loop: each request is submitted to the
+    multi-scene server (continuous batching) at spp when it arrives; the
+    requests that finish rendering in a server step get their G-buffer and
+    features and go through one batched KPCN forward together; latency =
+    completion of that forward - arrival."""
+    import torch
+
+    from .serve import DONE, RenderRequest, Server
+
+    srv = Server(ctx, paths_per_pass=paths_per_pass)
+    for sc in scs:
+        srv.add_scene(sc)
+    n = len(reqs)
+    lat = [0.0] * n
+    ids = {}
+    done = 0
+    k = 0
+    t0 = time.perf_counter()
+    while done < n:
+        now = time.perf_counter() - t0
+        while k < n and reqs[k]["arrival_s"] <= now:
+            r = reqs[k]
+            ids[srv.submit(RenderRequest(r["scene"], width, height, spp, r["camera"], seed=r["seed"]))] = k
+            k += 1
+        nd = srv.step(wait=k == n)
+        if nd:
+            fin = [(rid, j) for rid, j in ids.items() if srv.poll(rid) == DONE]
+            feats, noisy = [], []
+            for rid, j in fin:
+                r = reqs[j]
+                dp, ip = srv.result_device(rid)
+                d = torch.empty((height, width, 4), device="cuda")
+                i = torch.empty_like(d)
+                d.view(-1).copy_(_wrap_device(dp, height * width * 4))
+                i.view(-1).copy_(_wrap_device(ip, height * width * 4))
+                sc = scs[r["scene"]]
+                sc.set_render_params(width=width, height=height)
+                c = r["camera"]
+                sc.set_camera_orbit(c["target"], c["distance"], c["theta_deg"], c["phi_deg"], c["fovy_deg"])
+                f, nz = make_features(sc, sc.gbuffer(), d, i, spp, DEPTH_SCALE)
+                feats.append(f)
+                noisy.append(nz)
+                srv.release(rid)
+                del ids[rid]
+            if fin:
+                net.forward(torch.stack(feats).contiguous(), torch.stack(noisy).contiguous())
+                torch.cuda.synchronize()
+                now = time.perf_counter() - t0
+                for _, j in fin:
+                    lat[j] = now - reqs[j]["arrival_s"]
+                done += len(fin)
+        elif k < n and not ids:
+            time.sleep(min(2e-4, max(0.0, reqs[k]["arrival_s"] - (time.perf_counter() - t0))))
+    wall = time.perf_counter() - t0
+    srv.close()
+    return _lat_summary(lat, wall, n)
+
+
 def _wrap_device(ptr: int, count: int):
     """A float32 CUDA tensor view of `count` floats at device address ptr
     (server-owned memory, valid until the request is released)."""

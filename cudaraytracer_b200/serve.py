@@ -41,10 +41,13 @@ class RenderRequest:
 class Server:
     """A crt_server on a Context: add scenes, submit requests, step."""
 
+    SHORTEST_FIRST, ADMISSION_ORDER = 0, 1
+
     def __init__(self, ctx, hbm_budget_bytes: int = 0, paths_per_pass: int = 0, max_requests: int = 0,
-                 passes_in_flight: int = 0):
+                 passes_in_flight: int = 0, schedule: int = 0):
         self.ctx = ctx
-        cfg = _lib.ServerConfig(int(hbm_budget_bytes), int(paths_per_pass), int(max_requests), int(passes_in_flight))
+        cfg = _lib.ServerConfig(int(hbm_budget_bytes), int(paths_per_pass), int(max_requests), int(passes_in_flight),
+                                int(schedule))
         h = C.c_void_p()
         _lib.call("crt_server_create", ctx._h, C.byref(cfg), C.byref(h))
         self._h = h
@@ -160,6 +163,17 @@ def _percentiles(lat):
             "mean_ms": round(float(a.mean()) * 1e3, 2)}
 
 
+def _by_class(requests, lat):
+    """Latency percentiles per request class (resolution x spp)."""
+    groups = {}
+    for r, l in zip(requests, lat):
+        groups.setdefault((r.width * r.height, f"{r.width}x{r.height}@{r.spp}spp"), []).append(l)
+    out = {}
+    for (_, name), ls in sorted(groups.items(), key=lambda kv: (kv[0][0], int(kv[0][1].split("@")[1][:-3]))):
+        out[name] = {"n": len(ls), **_percentiles(ls)}
+    return out
+
+
 def run_served(server: Server, requests, keep_results: bool = False, idle_sleep_s: float = 2e-4):
     """Open-loop run: each request is submitted at its arrival time (wall
     clock from the start), the server is stepped continuously, and a request's
@@ -195,7 +209,7 @@ def run_served(server: Server, requests, keep_results: bool = False, idle_sleep_
     wall = time.perf_counter() - t0
     lat = [done_t[j] - requests[j].arrival_s for j in range(n)]
     out = {"requests": n, "wall_s": round(wall, 3), "req_per_s": round(n / wall, 3), **_percentiles(lat),
-           "samples": int(sum(r.width * r.height * r.spp for r in requests))}
+           "samples": int(sum(r.width * r.height * r.spp for r in requests)), "by_class": _by_class(requests, lat)}
     return (out, results) if keep_results else out
 
 
@@ -231,12 +245,13 @@ def run_one_at_a_time(scenes, requests, keep_results: bool = False):
             results[j] = (d.cpu().numpy(), i.cpu().numpy())
     wall = time.perf_counter() - t0
     out = {"requests": n, "wall_s": round(wall, 3), "req_per_s": round(n / wall, 3), **_percentiles(lat),
-           "samples": int(sum(r.width * r.height * r.spp for r in requests))}
+           "samples": int(sum(r.width * r.height * r.spp for r in requests)), "by_class": _by_class(requests, lat)}
     return (out, results) if keep_results else out
 
 
 def scene_hbm_bytes_estimate(num_tris: int) -> int:
     """Device bytes a loaded scene holds per triangle count (BVH nodes at
     most 2n x 64 B, leaf-order triangles 48 B, vertices 36 B, attributes
-    64 B, slot map 4 B), for sizing budgets before loading."""
-    return int(num_tris * (128 + 48 + 36 + 64 + 4))
+    64 B, slot map 4 B, 8-wide nodes and links about 24 B), for sizing
+    budgets before loading."""
+    return int(num_tris * (128 + 48 + 36 + 64 + 4 + 24))

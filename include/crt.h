@@ -292,7 +292,17 @@ typedef struct crt_server_config {
     int32_t paths_per_pass;   /* shared wavefront size; 0 = 8M paths */
     int32_t max_requests;     /* admitted (unreleased) request slots; 0 = 4096; at most 2^20 */
     int32_t passes_in_flight; /* passes queued on the GPU; 0 = 2; at most 64 */
+    int32_t schedule;         /* how a pass is filled from the admitted requests:
+                                 CRT_SCHED_SHORTEST_FIRST (0, default) or CRT_SCHED_ADMISSION_ORDER */
 } crt_server_config;
+
+/* Pass filling. Shortest first: the oldest admitted request takes up to half
+ * of each pass (so no request starves), the rest of the pass goes to the
+ * requests with the fewest paths left, which keeps small requests' latency
+ * low behind large ones. Admission order: requests in the order they were
+ * admitted (first come, first served). */
+#define CRT_SCHED_SHORTEST_FIRST 0
+#define CRT_SCHED_ADMISSION_ORDER 1
 
 typedef struct crt_request {
     int32_t scene;            /* id from crt_server_add_scene */

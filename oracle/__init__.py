@@ -314,7 +314,7 @@ def ref_render_lib() -> C.CDLL:
         L.refr_info.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float), _VP]
         L.refr_render.argtypes = [_VP, C.c_int, C.c_int, _VP, _VP, _VP, C.POINTER(C.c_float)]
         L.refr_svgf.argtypes = [C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP, _VP, C.c_int, C.c_float,
-                                C.c_float, C.c_float, C.c_float, C.c_int, _VP, _VP]
+                                C.c_float, C.c_float, C.c_float, C.c_int, _VP, _VP, _VP]
         _refrender = L
     return _refrender
 
@@ -353,10 +353,11 @@ class RefRenderer:
 
 
 def ref_svgf(noisy_d, noisy_i, pos_tri, normal_mat, bary_mesh, motion_depth, max_history=24, sigma_light=8.0,
-             sigma_normal=256.0, sigma_depth=1.0, reproj=0.1, atrous=5):
+             sigma_normal=256.0, sigma_depth=1.0, reproj=0.1, atrous=5, timing=False):
     """The reference's SVGF kernels (headless CUDA build) over a frame
     sequence: arrays of shape (F, H, W, 4) (normal_mat / bary_mesh uint16).
-    Returns (out_direct, out_indirect), float32 (F, H, W, 4)."""
+    Returns (out_direct, out_indirect), float32 (F, H, W, 4), and with
+    timing=True also the GPU ms of each frame's denoise block."""
     nd = np.ascontiguousarray(noisy_d, np.float32)
     ni = np.ascontiguousarray(noisy_i, np.float32)
     gp = np.ascontiguousarray(pos_tri, np.float32)
@@ -366,9 +367,10 @@ def ref_svgf(noisy_d, noisy_i, pos_tri, normal_mat, bary_mesh, motion_depth, max
     f, h, w, _ = nd.shape
     od = np.zeros_like(nd)
     oi = np.zeros_like(ni)
+    ms = np.zeros(f, np.float32)
     rc = ref_render_lib().refr_svgf(w, h, f, nd.ctypes.data, ni.ctypes.data, gp.ctypes.data, gn.ctypes.data,
                                     gb.ctypes.data, gm.ctypes.data, max_history, sigma_light, sigma_normal,
-                                    sigma_depth, reproj, atrous, od.ctypes.data, oi.ctypes.data)
+                                    sigma_depth, reproj, atrous, od.ctypes.data, oi.ctypes.data, ms.ctypes.data)
     if rc:
         raise RuntimeError(f"reference SVGF failed: cudaError {rc}")
-    return od, oi
+    return (od, oi, ms) if timing else (od, oi)

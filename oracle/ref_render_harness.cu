@@ -165,8 +165,14 @@ cudaArray_t make_array(cudaChannelFormatDesc d, int w, int h) {
 extern "C" int refr_svgf(int w, int h, int frames, const float *noisy_d, const float *noisy_i, const float *gb_pos,
                          const unsigned short *gb_nm, const unsigned short *gb_bm, const float *gb_md,
                          int max_history, float sigma_light, float sigma_normal, float sigma_depth, float reproj,
-                         int atrous, float *out_d, float *out_i) {
+                         int atrous, float *out_d, float *out_i, float *ms_frames) {
+    // ms_frames (optional, `frames` floats): GPU time of each frame's
+    // denoise block, temporal kernel through the last a-trous pass (CUDA
+    // events; the harness's host uploads and downloads excluded)
     const int n = w * h;
+    cudaEvent_t ev0, ev1;
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
     renderParam.width = w;
     renderParam.height = h;
     DenoiseParam dp;
@@ -228,6 +234,7 @@ extern "C" int refr_svgf(int w, int h, int frames, const float *noisy_d, const f
         int t = dp.currentTemporalBufferIndex;
         RenderBuffer histCur = hist[t], histLast = hist[1 - t];
         GBuffer gBuffer = gbs[gi], lastGBuffer = gbs[1 - gi];
+        cudaEventRecord(ev0);
         TemporalDenoiseKernel<<<grid, denoiseBlockSize>>>(dp, cameraParam, renderParam, renderBuffer, histLast, gBuffer,
                                                           lastGBuffer, firstFrame);
         cudaDeviceSynchronize();
@@ -247,6 +254,9 @@ extern "C" int refr_svgf(int w, int h, int frames, const float *noisy_d, const f
                 cur = 1 - cur;
             }
         }
+        cudaEventRecord(ev1);
+        cudaEventSynchronize(ev1);
+        if (ms_frames) cudaEventElapsedTime(&ms_frames[f], ev0, ev1);
         cudaMemcpy(out_d + off, rbs[cur].directLightingBuffer, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost);
         cudaMemcpy(out_i + off, rbs[cur].indirectLightingBuffer, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost);
         // end of frame (renderer.cuh:1299-1304)
@@ -256,6 +266,8 @@ extern "C" int refr_svgf(int w, int h, int frames, const float *noisy_d, const f
         firstFrame = false;
     }
     int err = (int)cudaGetLastError();
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
     for (int i = 0; i < 2; i++) {
         cudaFree(dp.directMoments[i]);
         cudaFree(dp.indirectMoments[i]);

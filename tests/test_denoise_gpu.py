@@ -23,3 +23,28 @@ def test_trained_kpcn_beats_raw_and_svgf_on_unseen_scenes(crt_ctx):
     assert tab["kpcn_4"] < 0.25 * tab["raw_4"]
     # ... and does better than SVGF on the same 4-spp image
     assert tab["kpcn_4"] < tab["svgf_4"]
+
+
+def test_sequence_evaluation_and_online_pipelines(crt_ctx):
+    """SVGF run temporally over an orbit sequence improves on the raw frames
+    as its history grows; the plain one-at-a-time SVGF loop and the
+    learned pipeline through the server each finish every request once and
+    report latency percentiles."""
+    from cudaraytracer_b200 import denoise as D
+    from cudaraytracer_b200.kpcn import Kpcn
+
+    net = Kpcn(crt_ctx, seed=0)  # untrained: the pipeline mechanics are under test here
+    tab = D.evaluate_sequences(crt_ctx, net, [200], 64, 64, 6, [2], svgf_spp_list=(1, 8), ref_spp=256)
+    for k in ("raw_2", "kpcn_2", "svgf_1", "svgf_8", "raw_1", "raw_8"):
+        assert k in tab and tab[k] > 0.0
+    assert tab["steady"]["svgf_1"] < tab["steady"]["raw_1"]
+    assert tab["steady"]["svgf_8"] < tab["steady"]["raw_8"]
+    scs, reqs = D.sequence_requests(crt_ctx, [200, 201], 64, 64, 4, 0.0)
+    assert [r["frame"] for r in reqs] == [0, 0, 1, 1, 2, 2, 3, 3]
+    plain = D.run_plain_svgf_loop(crt_ctx, scs, reqs, 64, 64, spp=8)
+    learned = D.run_learned_served(crt_ctx, net, scs, reqs, 64, 64, 2)
+    for r in (plain, learned):
+        assert r["requests"] == 8 and r["req_per_s"] > 0 and 0 < r["p50_ms"] <= r["p99_ms"]
+    for sc in scs:
+        sc.close()
+    net.close()

@@ -57,10 +57,11 @@ def render_alone(sc, r):
     return d.cpu().numpy(), i.cpu().numpy()
 
 
-def test_each_request_same_alone_and_in_the_mix(crt_ctx, resident):
+@pytest.mark.parametrize("schedule", [Server.SHORTEST_FIRST, Server.ADMISSION_ORDER])
+def test_each_request_same_alone_and_in_the_mix(crt_ctx, resident, schedule):
     reqs = mix(resident)
     # small wavefronts so requests straddle passes and passes mix requests
-    srv = Server(crt_ctx, paths_per_pass=3000, passes_in_flight=3)
+    srv = Server(crt_ctx, paths_per_pass=3000, passes_in_flight=3, schedule=schedule)
     for sc in resident:
         srv.add_scene(sc)
     ids = [srv.submit(r) for r in reqs]
@@ -146,3 +147,30 @@ def test_open_loop_driver_reports_latency(crt_ctx, resident):
     pd, pi = render_alone(resident[reqs[j].scene], reqs[j])
     np.testing.assert_allclose(res[j][0], pd, rtol=2e-5, atol=2e-6)
     np.testing.assert_allclose(res[j][1], pi, rtol=2e-5, atol=2e-6)
+
+
+@pytest.mark.parametrize("schedule", [Server.SHORTEST_FIRST, Server.ADMISSION_ORDER])
+def test_shortest_first_finishes_a_small_request_behind_a_large_one(crt_ctx, resident, schedule):
+    """A large request (1M paths) admitted first and a small one (2K paths)
+    right behind it: filling passes shortest-first finishes the small one
+    in the first pass while the large one still runs; in admission order
+    the small one waits for the large one's last pass."""
+    cb = resident[0]
+    srv = Server(crt_ctx, paths_per_pass=1 << 15, passes_in_flight=1, schedule=schedule)
+    srv.add_scene(cb)
+    big = srv.submit(RenderRequest(0, 128, 128, 64, orbit(cb, 90, 0), seed=21))
+    small = srv.submit(RenderRequest(0, 32, 32, 2, orbit(cb, 90, 10), seed=22))
+    order = []
+    while len(order) < 2:
+        srv.step(wait=True)
+        for rid in (big, small):
+            if rid not in order and srv.poll(rid) == DONE:
+                order.append(rid)
+    if schedule == Server.SHORTEST_FIRST:
+        assert order == [small, big]
+        assert srv.stats()["passes"] >= 32  # 1M paths of the large request in passes of 32K
+    else:
+        assert order == [big, small]
+    for rid in (big, small):
+        srv.release(rid)
+    srv.close()
