@@ -79,6 +79,21 @@ __device__ __forceinline__ unsigned visit8(const float4 *nodes, int node, V3 o, 
     return mask;
 }
 
+// The eight child links of wide node `node` (one 32 B read-only load).
+__device__ __forceinline__ void load_links8(const int *links, int node, int (&lk)[8]) {
+    asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=r"(lk[0]), "=r"(lk[1]), "=r"(lk[2]), "=r"(lk[3]), "=r"(lk[4]), "=r"(lk[5]), "=r"(lk[6]), "=r"(lk[7])
+        : "l"(links + 8 * (size_t)node));
+}
+
+// lk[s] for a run-time slot s without indexing registers dynamically.
+__device__ __forceinline__ int select_link(const int (&lk)[8], unsigned s) {
+    const int a = (s & 1) ? lk[1] : lk[0], b = (s & 1) ? lk[3] : lk[2];
+    const int c = (s & 1) ? lk[5] : lk[4], d = (s & 1) ? lk[7] : lk[6];
+    const int e = (s & 2) ? b : a, f = (s & 2) ? d : c;
+    return (s & 4) ? f : e;
+}
+
 __device__ __forceinline__ unsigned ray_octant(V3 d) {
     return (d.x < 0.f ? 4u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 1u : 0u);
 }
@@ -113,22 +128,31 @@ struct ShortStack {
 
 // Finds the next leaf of an ordered traversal. `cur` holds the current
 // wide node and its children still to visit; returns a leaf link (< 0), or
-// 0 when the stack is exhausted.
-template <int kShort>
+// 0 when the stack is exhausted. With kRegLinks the links of the node last
+// visited are fetched with its boxes and kept in registers (lk, valid while
+// `fresh`), so descending into its children needs no further load; links of
+// nodes popped from the stack are read from memory.
+template <int kShort, bool kRegLinks = false>
 __device__ __forceinline__ int next_leaf8(const BvhView &bvh, unsigned &cur, ShortStack<kShort> &st, V3 o, V3 inv,
-                                          float tmin, float tmax, unsigned oct) {
+                                          float tmin, float tmax, unsigned oct, int (&lk)[8], bool &fresh) {
     while (true) {
         unsigned m = cur & 0xffu;
         if (m == 0) {
             if (st.empty()) return 0;
             cur = st.pop();
             m = cur & 0xffu;
+            fresh = false;
         }
         const unsigned k = __ffs(m) - 1;
         cur &= ~(1u << k);
-        const int link = __ldg(bvh.wlinks + 8 * (size_t)(cur >> 8) + (k ^ oct));
+        const int link = (kRegLinks && fresh) ? select_link(lk, k ^ oct)
+                                              : __ldg(bvh.wlinks + 8 * (size_t)(cur >> 8) + (k ^ oct));
         if (link < 0) return link;
         if (cur & 0xffu) st.push(cur);
+        if (kRegLinks) {
+            load_links8(bvh.wlinks, link, lk);
+            fresh = true;
+        }
         cur = ((unsigned)link << 8) | visit8(bvh.wnodes, link, o, inv, tmin, tmax, oct);
     }
 }
@@ -147,8 +171,10 @@ __device__ __forceinline__ Hit closest_hit8(const BvhView &bvh, ShortStack<kShor
     const unsigned oct = ray_octant(d);
     st.reset();
     unsigned cur = visit8(bvh.wnodes, 0, o, inv, tmin, hit.t, oct);
+    int lk[8];
+    bool fresh = false;
     while (true) {
-        const int leaf = next_leaf8(bvh, cur, st, o, inv, tmin, hit.t, oct);
+        const int leaf = next_leaf8<kShort>(bvh, cur, st, o, inv, tmin, hit.t, oct, lk, fresh);
         if (leaf == 0) break;
         const int code = ~leaf;
         const int first = code >> 4, count = code & 15;

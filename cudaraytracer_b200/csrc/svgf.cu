@@ -16,12 +16,17 @@
 // SVGF: TemporalDenoising (renderer.cuh:524-677), ComputeVarianceKernel
 // (:689-805) and AtrousKernel (:807-954) restated pixel for pixel, driven in
 // the order of RenderLoop's denoise block (:1208-1258): temporal reprojection
-// into the current buffers, history copy, 7x7 variance estimate, then
-// atrous_iterations a-trous passes at steps 1, 2, 4, ... (skipped on the
-// first frame).
+// (which also writes the history the reference copies afterwards), 7x7
+// variance estimate, then atrous_iterations a-trous passes at steps 1, 2,
+// 4, ... (skipped on the first frame), the last of them writing the
+// caller's output. The temporal pass also stores, per pixel, the decoded
+// normal, depth, material/mesh ids and history length that every later tap
+// compares against (one 16 B and one 8 B load per tap instead of four
+// G-buffer loads and a normal decode).
 #include "svgf.h"
 #include "shade.cuh"
 #include <cstring>
+#include <cstdlib>
 
 namespace crt {
 
@@ -218,10 +223,22 @@ __device__ __forceinline__ bool valid_tap(int tx, int ty, int W, int H, int mesh
     return mesh == (int)lb.w && mat == (int)ln.w && tri == (int)lp.w && dotn >= 0.9f && dd <= thr;
 }
 
+// Per-pixel edge-stopping record written by the temporal pass and read by
+// the variance and a-trous taps: the decoded G-buffer normal and linear
+// depth (edge), and the material | mesh << 16 id with the history length
+// (tag). decode_normal runs once per pixel instead of once per tap; the
+// values are the same.
+struct EdgeOut {
+    float4 *edge;
+    int2 *tag;
+};
+
 struct TemporalArgs {
     int W, H, max_hist;
     float reproj;
-    float4 *cur_d, *cur_i;                // current noisy -> blended (in place)
+    const float4 *noisy_d, *noisy_i;      // current noisy frame
+    float4 *cur_d, *cur_i;                // blended result
+    float4 *hist_out_d, *hist_out_i;      // the same, kept as next frame's history
     const float4 *hist_d, *hist_i;        // last frame's temporal history
     float2 *mom_d, *mom_i;                // moments written this frame
     const float2 *lmom_d, *lmom_i;        // last frame's moments
@@ -230,27 +247,35 @@ struct TemporalArgs {
     bool first;
 };
 
-// TemporalDenoising (renderer.cuh:524-677).
-__global__ void k_svgf_temporal(TemporalArgs a, GB cur, GB last) {
+// TemporalDenoising (renderer.cuh:524-677). Reads the noisy frame, writes
+// the blended result both as the frame's working buffer and as the next
+// frame's history, and the pixel's edge-stopping record.
+__global__ void k_svgf_temporal(TemporalArgs a, GB cur, GB last, EdgeOut eo) {
     int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.W || y >= a.H) return;
     int idx = y * a.W + x;
-    V3 cd = rgb(a.cur_d, idx), ci = rgb(a.cur_i, idx);
-    if (a.first) {
-        float dl = luminance(cd), il = luminance(ci);
-        a.mom_d[idx] = make_float2(dl, dl * dl);
-        a.mom_i[idx] = make_float2(il, il * il);
-        a.cur_d[idx].w = 1.f;
-        a.cur_i[idx].w = 1.f;
-        a.hlen[idx] = 1;
-        return;
-    }
+    const float4 nd4 = a.noisy_d[idx], ni4 = a.noisy_i[idx];
+    V3 cd{nd4.x, nd4.y, nd4.z}, ci{ni4.x, ni4.y, ni4.z};
     float4 pt = cur.pos_tri[idx];
     ushort4 bm = cur.bary_mesh[idx], nm = cur.normal_mat[idx];
     float4 md = cur.motion_depth[idx];
     int mat = nm.w, mesh = bm.w, tri = (int)pt.w;
     V3 n = decode_normal(nm);
     float depth = md.z, dz = md.w;
+    eo.edge[idx] = make_float4(n.x, n.y, n.z, depth);
+    if (a.first) {
+        float dl = luminance(cd), il = luminance(ci);
+        a.mom_d[idx] = make_float2(dl, dl * dl);
+        a.mom_i[idx] = make_float2(il, il * il);
+        const float4 od = make_float4(nd4.x, nd4.y, nd4.z, 1.f), oi = make_float4(ni4.x, ni4.y, ni4.z, 1.f);
+        a.cur_d[idx] = od;
+        a.cur_i[idx] = oi;
+        a.hist_out_d[idx] = od;
+        a.hist_out_i[idx] = oi;
+        a.hlen[idx] = 1;
+        eo.tag[idx] = make_int2(mat | (mesh << 16), 1);
+        return;
+    }
     float mvx = md.x * a.W * 0.5f, mvy = md.y * a.H * 0.5f;
     float pixdist = sqrtf(mvx * mvx + mvy * mvy);
     // GetLastFramePos (renderer.cuh:446-455)
@@ -342,14 +367,17 @@ __global__ void k_svgf_temporal(TemporalArgs a, GB cur, GB last) {
     if (valid) {
         od.w = mdd.y - mdd.x * mdd.x;
         oi.w = mii.y - mii.x * mii.x;
-        a.hlen[idx] = hl;
     } else {
         od.w = 1.f;
         oi.w = 1.f;
-        a.hlen[idx] = 1;
+        hl = 1;
     }
+    a.hlen[idx] = hl;
+    eo.tag[idx] = make_int2(mat | (mesh << 16), hl);
     a.cur_d[idx] = od;
     a.cur_i[idx] = oi;
+    a.hist_out_d[idx] = od;
+    a.hist_out_i[idx] = oi;
 }
 
 struct VarianceArgs {
@@ -358,27 +386,48 @@ struct VarianceArgs {
     const float4 *in_d, *in_i;
     float4 *out_d, *out_i;
     const float2 *mom_d, *mom_i;
-    const int *hlen;
+    const float4 *edge;
+    const int2 *tag;
 };
 
-// ComputeVarianceKernel (renderer.cuh:689-805).
-__global__ void k_svgf_variance(VarianceArgs a, GB g) {
-    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= a.W || y >= a.H) return;
-    int idx = y * a.W + x;
-    int h = a.hlen[idx];
-    if (h >= 4) {
-        a.out_d[idx] = a.in_d[idx];
-        a.out_i[idx] = a.in_i[idx];
-        return;
+// Tap sources for the variance body (global memory or a shared tile).
+struct VarGlobalTaps {
+    const VarianceArgs &a;
+    __device__ __forceinline__ float4 d(int x, int y) const { return a.in_d[y * a.W + x]; }
+    __device__ __forceinline__ float4 i(int x, int y) const { return a.in_i[y * a.W + x]; }
+    __device__ __forceinline__ float4 e(int x, int y) const { return a.edge[y * a.W + x]; }
+    __device__ __forceinline__ int t(int x, int y) const { return a.tag[y * a.W + x].x; }
+    __device__ __forceinline__ float4 m(int x, int y) const {
+        const float2 md = a.mom_d[y * a.W + x], mi = a.mom_i[y * a.W + x];
+        return make_float4(md.x, md.y, mi.x, mi.y);
     }
-    V3 cd = rgb(a.in_d, idx), ci = rgb(a.in_i, idx);
+};
+
+struct VarTileTaps {
+    const float4 *sd, *si, *se, *sm;
+    const int *st;
+    int x0, y0, rw;
+    __device__ __forceinline__ int at(int x, int y) const { return (y - y0) * rw + (x - x0); }
+    __device__ __forceinline__ float4 d(int x, int y) const { return sd[at(x, y)]; }
+    __device__ __forceinline__ float4 i(int x, int y) const { return si[at(x, y)]; }
+    __device__ __forceinline__ float4 e(int x, int y) const { return se[at(x, y)]; }
+    __device__ __forceinline__ int t(int x, int y) const { return st[at(x, y)]; }
+    __device__ __forceinline__ float4 m(int x, int y) const { return sm[at(x, y)]; }
+};
+
+// ComputeVarianceKernel (renderer.cuh:689-805) for pixel (x, y) with a
+// history shorter than 4 frames: 7x7 edge-stopped filter of colour and
+// moments, variance from the filtered moments.
+template <class Taps>
+__device__ __forceinline__ void variance_pixel(const VarianceArgs &a, const GB &g, const Taps &src, int x, int y, int h,
+                                               int ctag) {
+    int idx = y * a.W + x;
+    const float4 cd4 = src.d(x, y), ci4 = src.i(x, y);
+    V3 cd{cd4.x, cd4.y, cd4.z}, ci{ci4.x, ci4.y, ci4.z};
     float cdl = luminance(cd), cil = luminance(ci);
-    float4 md = g.motion_depth[idx];
-    float cdepth = md.z, dz = fmaxf(md.w, 1e-4f);
-    ushort4 nm = g.normal_mat[idx], bm = g.bary_mesh[idx];
-    int cmat = nm.w, cmesh = bm.w;
-    V3 cn = decode_normal(nm);
+    const float4 ce = src.e(x, y);
+    float cdepth = ce.w, dz = fmaxf(g.motion_depth[idx].w, 1e-4f);
+    V3 cn{ce.x, ce.y, ce.z};
     V3 fd{0.f, 0.f, 0.f}, fi{0.f, 0.f, 0.f};
     float fmd0 = 0.f, fmd1 = 0.f, fmi0 = 0.f, fmi1 = 0.f, twd = 0.f, twi = 0.f;
     float sd = a.sigma_depth * fmaxf(dz, 1e-4f);
@@ -386,14 +435,14 @@ __global__ void k_svgf_variance(VarianceArgs a, GB g) {
         for (int ki = -a.half; ki <= a.half; ki++) {
             int ni = x + ki, nj = y + kj;
             if (!(ni >= 0 && ni < a.W && nj >= 0 && nj < a.H)) continue;
-            int nidx = nj * a.W + ni;
-            V3 nd = rgb(a.in_d, nidx), nid = rgb(a.in_i, nidx);
-            float nz = g.motion_depth[nidx].z;
-            ushort4 nnm = g.normal_mat[nidx], nbm = g.bary_mesh[nidx];
-            if (cmat != (int)nnm.w || cmesh != (int)nbm.w) continue;
-            V3 nn = decode_normal(nnm);
+            if (src.t(ni, nj) != ctag) continue;
+            const float4 nd4 = src.d(ni, nj), ni4 = src.i(ni, nj);
+            V3 nd{nd4.x, nd4.y, nd4.z}, nid{ni4.x, ni4.y, ni4.z};
+            const float4 ne = src.e(ni, nj);
+            float nz = ne.w;
+            V3 nn{ne.x, ne.y, ne.z};
             float ndl = luminance(nd), nil = luminance(nid);
-            float2 mdn = a.mom_d[nidx], min_ = a.mom_i[nidx];
+            const float4 mm = src.m(ni, nj);
             float dist = sqrtf(float(ki * ki + kj * kj));
             float wz = -fabsf(cdepth - nz) / (sd * dist + 1e-4f);
             float wn = powf(fmaxf(0.f, dot(cn, nn)), a.sigma_normal);
@@ -403,10 +452,10 @@ __global__ void k_svgf_variance(VarianceArgs a, GB g) {
             float dw = expf(wz + wdl) * wn, iw = expf(wz + wil) * wn;
             fd = fd + nd * dw;
             fi = fi + nid * iw;
-            fmd0 += mdn.x * dw;
-            fmd1 += mdn.y * dw;
-            fmi0 += min_.x * iw;
-            fmi1 += min_.y * iw;
+            fmd0 += mm.x * dw;
+            fmd1 += mm.y * dw;
+            fmi0 += mm.z * iw;
+            fmi1 += mm.w * iw;
             twd += dw;
             twi += iw;
         }
@@ -423,37 +472,118 @@ __global__ void k_svgf_variance(VarianceArgs a, GB g) {
     a.out_i[idx] = make_float4(fi.x, fi.y, fi.z, vi);
 }
 
+// One thread per pixel, taps from global memory.
+__global__ void k_svgf_variance(VarianceArgs a, GB g) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.W || y >= a.H) return;
+    int idx = y * a.W + x;
+    const int2 ctag = a.tag[idx];
+    if (ctag.y >= 4) {
+        a.out_d[idx] = a.in_d[idx];
+        a.out_i[idx] = a.in_i[idx];
+        return;
+    }
+    variance_pixel(a, g, VarGlobalTaps{a}, x, y, ctag.y, ctag.x);
+}
+
+// Tiled: a block whose pixels all have 4 frames of history only copies
+// (the steady state); otherwise its 32 x 8 pixels and a 3-pixel halo
+// (colour, edge record, tag, moments: 68 B per pixel) are staged in shared
+// memory for the 7x7 taps.
+constexpr int kVarTileX = 32, kVarTileY = 8, kVarHalf = 3;
+
+__global__ void __launch_bounds__(kVarTileX * kVarTileY) k_svgf_variance_tiled(VarianceArgs a, GB g) {
+    constexpr int R = kVarHalf, RW = kVarTileX + 2 * R, RH = kVarTileY + 2 * R, N = RW * RH;
+    __shared__ float4 sd[N], si[N], se[N], sm[N];
+    __shared__ int stg[N];
+    const int bx = blockIdx.x * kVarTileX, by = blockIdx.y * kVarTileY;
+    const int x = bx + threadIdx.x, y = by + threadIdx.y;
+    const bool inside = x < a.W && y < a.H;
+    int2 ctag = make_int2(0, 4);
+    if (inside) ctag = a.tag[y * a.W + x];
+    const bool filter = inside && ctag.y < 4;
+    if (!__syncthreads_or(filter)) {
+        if (inside) {
+            a.out_d[y * a.W + x] = a.in_d[y * a.W + x];
+            a.out_i[y * a.W + x] = a.in_i[y * a.W + x];
+        }
+        return;
+    }
+    const int tid = threadIdx.y * kVarTileX + threadIdx.x;
+    for (int k = tid; k < N; k += kVarTileX * kVarTileY) {
+        const int gx = bx - R + k % RW, gy = by - R + k / RW;
+        if (gx < 0 || gx >= a.W || gy < 0 || gy >= a.H) continue;  // never read: taps check the image bounds
+        const int gi = gy * a.W + gx;
+        sd[k] = a.in_d[gi];
+        si[k] = a.in_i[gi];
+        se[k] = a.edge[gi];
+        stg[k] = a.tag[gi].x;
+        const float2 md = a.mom_d[gi], mi = a.mom_i[gi];
+        sm[k] = make_float4(md.x, md.y, mi.x, mi.y);
+    }
+    __syncthreads();
+    if (!inside) return;
+    if (!filter) {
+        const VarTileTaps t{sd, si, se, sm, stg, bx - R, by - R, RW};
+        a.out_d[y * a.W + x] = t.d(x, y);
+        a.out_i[y * a.W + x] = t.i(x, y);
+        return;
+    }
+    variance_pixel(a, g, VarTileTaps{sd, si, se, sm, stg, bx - R, by - R, RW}, x, y, ctag.y, ctag.x);
+}
+
 struct AtrousArgs {
     int W, H, step;
     float sigma_depth, sigma_normal, sigma_light;
     const float4 *in_d, *in_i;
     float4 *out_d, *out_i;
-    const int *hlen;
+    const float4 *edge;
+    const int2 *tag;
 };
 
-// AtrousKernel (renderer.cuh:807-954).
-__global__ void k_svgf_atrous(AtrousArgs a, GB g) {
-    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= a.W || y >= a.H) return;
+// Tap sources for the a-trous body: straight from global memory, or from a
+// shared-memory tile that covers the block and its halo.
+struct GlobalTaps {
+    const AtrousArgs &a;
+    __device__ __forceinline__ float4 d(int x, int y) const { return a.in_d[y * a.W + x]; }
+    __device__ __forceinline__ float4 i(int x, int y) const { return a.in_i[y * a.W + x]; }
+    __device__ __forceinline__ float4 e(int x, int y) const { return a.edge[y * a.W + x]; }
+    __device__ __forceinline__ int2 t(int x, int y) const { return a.tag[y * a.W + x]; }
+};
+
+struct TileTaps {
+    const float4 *sd, *si, *se;
+    const int2 *st;
+    int x0, y0, rw;  // tile origin (image coordinates of its first element) and row width
+    __device__ __forceinline__ int at(int x, int y) const { return (y - y0) * rw + (x - x0); }
+    __device__ __forceinline__ float4 d(int x, int y) const { return sd[at(x, y)]; }
+    __device__ __forceinline__ float4 i(int x, int y) const { return si[at(x, y)]; }
+    __device__ __forceinline__ float4 e(int x, int y) const { return se[at(x, y)]; }
+    __device__ __forceinline__ int2 t(int x, int y) const { return st[at(x, y)]; }
+};
+
+// AtrousKernel (renderer.cuh:807-954) for pixel (x, y): 3x3 pre-blur of
+// the variance, then the 5x5 edge-stopped filter at a.step.
+template <class Taps>
+__device__ __forceinline__ void atrous_pixel(const AtrousArgs &a, const GB &g, const Taps &src, int x, int y) {
     int idx = y * a.W + x;
-    int ch = max(a.hlen[idx], 1);
-    V3 cd = rgb(a.in_d, idx), ci = rgb(a.in_i, idx);
+    const int2 ctag = src.t(x, y);
+    int ch = max(ctag.y, 1);
+    const float4 cd4 = src.d(x, y), ci4 = src.i(x, y);
+    V3 cd{cd4.x, cd4.y, cd4.z}, ci{ci4.x, ci4.y, ci4.z};
     float cdl = luminance(cd), cil = luminance(ci);
-    float4 md = g.motion_depth[idx];
-    float cdepth = md.z, dz = fmaxf(md.w, 1e-4f);
-    ushort4 nm = g.normal_mat[idx], bm = g.bary_mesh[idx];
-    int cmat = nm.w, cmesh = bm.w;
-    V3 cn = decode_normal(nm);
+    const float4 ce = src.e(x, y);
+    float cdepth = ce.w, dz = fmaxf(g.motion_depth[idx].w, 1e-4f);
+    V3 cn{ce.x, ce.y, ce.z};
     const float vk[2] = {0.5f, 0.25f};
     float fvd = 0.f, fvi = 0.f, fvw = 0.f;
     for (int vj = -1; vj <= 1; vj++)
         for (int vi = -1; vi <= 1; vi++) {
             int sx = x + vi, sy = y + vj;
             if (sx < 0 || sx >= a.W || sy < 0 || sy >= a.H) continue;
-            int k = sy * a.W + sx;
             float w = vk[abs(vi)] * vk[abs(vj)];
-            fvd += w * fmaxf(0.0f, a.in_d[k].w);
-            fvi += w * fmaxf(0.0f, a.in_i[k].w);
+            fvd += w * fmaxf(0.0f, src.d(sx, sy).w);
+            fvi += w * fmaxf(0.0f, src.i(sx, sy).w);
             fvw += w;
         }
     fvw = fmaxf(fvw, 1e-6f);
@@ -472,13 +602,13 @@ __global__ void k_svgf_atrous(AtrousArgs a, GB g) {
         for (int ki = -2; ki <= 2; ki++) {
             int ni = x + ki * a.step, nj = y + kj * a.step;
             if (!(ni >= 0 && ni < a.W && nj >= 0 && nj < a.H)) continue;
-            int nidx = nj * a.W + ni;
-            int nh = max(a.hlen[nidx], 1);
-            float nz = g.motion_depth[nidx].z;
-            ushort4 nnm = g.normal_mat[nidx], nbm = g.bary_mesh[nidx];
-            if (cmat != (int)nnm.w || cmesh != (int)nbm.w) continue;
-            V3 nn = decode_normal(nnm);
-            float4 nd4 = a.in_d[nidx], ni4 = a.in_i[nidx];
+            const int2 ntag = src.t(ni, nj);
+            if (ntag.x != ctag.x) continue;
+            int nh = max(ntag.y, 1);
+            const float4 ne = src.e(ni, nj);
+            float nz = ne.w;
+            V3 nn{ne.x, ne.y, ne.z};
+            float4 nd4 = src.d(ni, nj), ni4 = src.i(ni, nj);
             V3 nd{nd4.x, nd4.y, nd4.z}, nic{ni4.x, ni4.y, ni4.z};
             float nvd = fmaxf(0.0f, nd4.w), nvi = fmaxf(0.0f, ni4.w);
             float dist = sqrtf(float(ki * ki + kj * kj)) * a.step;
@@ -508,6 +638,42 @@ __global__ void k_svgf_atrous(AtrousArgs a, GB g) {
         a.out_i[idx] = make_float4(ci.x, ci.y, ci.z, 1.f);
 }
 
+// One thread per pixel, taps from global memory (large steps).
+__global__ void k_svgf_atrous(AtrousArgs a, GB g) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.W || y >= a.H) return;
+    atrous_pixel(a, g, GlobalTaps{a}, x, y);
+}
+
+// Small steps (1 and 2): the block's kTileX x kTileY pixels and their halo
+// of 2 * kStep (the 5x5 taps; it also covers the 3x3 pre-blur) are staged
+// once in shared memory (colour, variance, edge record and tag: 56 B per
+// pixel), so each loaded pixel serves up to 25 taps of the block instead
+// of being fetched per tap.
+constexpr int kTileX = 32, kTileY = 8;
+
+template <int kStep>
+__global__ void __launch_bounds__(kTileX * kTileY) k_svgf_atrous_tiled(AtrousArgs a, GB g) {
+    constexpr int R = 2 * kStep, RW = kTileX + 2 * R, RH = kTileY + 2 * R, N = RW * RH;
+    __shared__ float4 sd[N], si[N], se[N];
+    __shared__ int2 stg[N];
+    const int bx = blockIdx.x * kTileX, by = blockIdx.y * kTileY;
+    const int tid = threadIdx.y * kTileX + threadIdx.x;
+    for (int k = tid; k < N; k += kTileX * kTileY) {
+        const int gx = bx - R + k % RW, gy = by - R + k / RW;
+        if (gx < 0 || gx >= a.W || gy < 0 || gy >= a.H) continue;  // never read: taps check the image bounds
+        const int gi = gy * a.W + gx;
+        sd[k] = a.in_d[gi];
+        si[k] = a.in_i[gi];
+        se[k] = a.edge[gi];
+        stg[k] = a.tag[gi];
+    }
+    __syncthreads();
+    const int x = bx + threadIdx.x, y = by + threadIdx.y;
+    if (x >= a.W || y >= a.H) return;
+    atrous_pixel(a, g, TileTaps{sd, si, se, stg, bx - R, by - R, RW}, x, y);
+}
+
 // ---------------------------------------------------------------------------
 // host: state and frame
 // ---------------------------------------------------------------------------
@@ -525,6 +691,8 @@ void SvgfState::allocate(int w, int h) {
         CRT_CUDA(cudaMalloc(&mom_i[k], n * sizeof(float2)));
         CRT_CUDA(cudaMalloc(&hlen[k], n * sizeof(int)));
     }
+    CRT_CUDA(cudaMalloc(&edge, n * sizeof(float4)));
+    CRT_CUDA(cudaMalloc(&tag, n * sizeof(int2)));
     reset_sync();
 }
 
@@ -542,6 +710,8 @@ void SvgfState::reset_sync() {
 }
 
 void SvgfState::release() {
+    if (edge) cudaFree(edge), edge = nullptr;
+    if (tag) cudaFree(tag), tag = nullptr;
     for (int k = 0; k < 2; ++k) {
         for (void **p : {(void **)&buf_d[k], (void **)&buf_i[k], (void **)&hist_d[k], (void **)&hist_i[k],
                          (void **)&mom_d[k], (void **)&mom_i[k], (void **)&hlen[k]})
@@ -555,21 +725,29 @@ void SvgfState::release() {
 int svgf_frame(SvgfState &st, const DenoiseParams &p, const GBufferPlanes &cur, const GBufferPlanes &last,
                const float4 *noisy_d, const float4 *noisy_i, float4 *out_d, float4 *out_i, cudaStream_t s) {
     const int W = st.W, H = st.H;
-    const size_t bytes = (size_t)W * H * sizeof(float4);
     dim3 b(16, 16), g((W + 15) / 16, (H + 15) / 16);
+    dim3 bt(kTileX, kTileY), gt((W + kTileX - 1) / kTileX, (H + kTileY - 1) / kTileY);
+    // CRT_SVGF_TILED=0 runs every a-trous pass from global memory
+    const char *tv = getenv("CRT_SVGF_TILED");
+    const bool tiled = !(tv && tv[0] == '0');
     GB gc{cur.pos_tri, cur.normal_mat, cur.bary_mesh, cur.motion_depth};
     GB gl{last.pos_tri, last.normal_mat, last.bary_mesh, last.motion_depth};
-    int c = 0;  // index of the buffer holding the current result
-    CRT_CUDA(cudaMemcpyAsync(st.buf_d[c], noisy_d, bytes, cudaMemcpyDeviceToDevice, s));
-    CRT_CUDA(cudaMemcpyAsync(st.buf_i[c], noisy_i, bytes, cudaMemcpyDeviceToDevice, s));
     const int t = st.t;
+    const int passes = st.first ? 0 : (p.atrous_iterations < 1 ? 1 : (p.atrous_iterations > 8 ? 8 : p.atrous_iterations));
+    // The passes ping-pong between buf[0] and buf[1]; the last one writes
+    // the caller's output directly.
+    int c = 0;  // buffer holding the current result
     TemporalArgs ta;
     ta.W = W;
     ta.H = H;
     ta.max_hist = p.max_history_length;
     ta.reproj = p.reprojection_depth_factor;
+    ta.noisy_d = noisy_d;
+    ta.noisy_i = noisy_i;
     ta.cur_d = st.buf_d[c];
     ta.cur_i = st.buf_i[c];
+    ta.hist_out_d = st.hist_d[t];
+    ta.hist_out_i = st.hist_i[t];
     ta.hist_d = st.hist_d[1 - t];
     ta.hist_i = st.hist_i[1 - t];
     ta.mom_d = st.mom_d[t];
@@ -579,10 +757,8 @@ int svgf_frame(SvgfState &st, const DenoiseParams &p, const GBufferPlanes &cur, 
     ta.hlen = st.hlen[t];
     ta.lhlen = st.hlen[1 - t];
     ta.first = st.first;
-    k_svgf_temporal<<<g, b, 0, s>>>(ta, gc, gl);
+    k_svgf_temporal<<<g, b, 0, s>>>(ta, gc, gl, EdgeOut{st.edge, st.tag});
     int launches = 1;
-    CRT_CUDA(cudaMemcpyAsync(st.hist_d[t], st.buf_d[c], bytes, cudaMemcpyDeviceToDevice, s));
-    CRT_CUDA(cudaMemcpyAsync(st.hist_i[t], st.buf_i[c], bytes, cudaMemcpyDeviceToDevice, s));
     VarianceArgs va;
     va.W = W;
     va.H = H;
@@ -592,37 +768,44 @@ int svgf_frame(SvgfState &st, const DenoiseParams &p, const GBufferPlanes &cur, 
     va.sigma_light = p.sigma_light;
     va.in_d = st.buf_d[c];
     va.in_i = st.buf_i[c];
-    va.out_d = st.buf_d[1 - c];
-    va.out_i = st.buf_i[1 - c];
+    va.out_d = passes ? st.buf_d[1 - c] : out_d;
+    va.out_i = passes ? st.buf_i[1 - c] : out_i;
     va.mom_d = st.mom_d[t];
     va.mom_i = st.mom_i[t];
-    va.hlen = st.hlen[t];
-    k_svgf_variance<<<g, b, 0, s>>>(va, gc);
+    va.edge = st.edge;
+    va.tag = st.tag;
+    if (tiled && va.half == kVarHalf)
+        k_svgf_variance_tiled<<<dim3((W + kVarTileX - 1) / kVarTileX, (H + kVarTileY - 1) / kVarTileY),
+                                dim3(kVarTileX, kVarTileY), 0, s>>>(va, gc);
+    else
+        k_svgf_variance<<<g, b, 0, s>>>(va, gc);
     ++launches;
     c = 1 - c;
-    if (!st.first) {
-        int passes = p.atrous_iterations < 1 ? 1 : (p.atrous_iterations > 8 ? 8 : p.atrous_iterations);
-        for (int i = 0; i < passes; ++i) {
-            AtrousArgs aa;
-            aa.W = W;
-            aa.H = H;
-            aa.step = 1 << i;
-            aa.sigma_depth = p.sigma_depth;
-            aa.sigma_normal = p.sigma_normal;
-            aa.sigma_light = p.sigma_light;
-            aa.in_d = st.buf_d[c];
-            aa.in_i = st.buf_i[c];
-            aa.out_d = st.buf_d[1 - c];
-            aa.out_i = st.buf_i[1 - c];
-            aa.hlen = st.hlen[t];
+    for (int i = 0; i < passes; ++i) {
+        AtrousArgs aa;
+        aa.W = W;
+        aa.H = H;
+        aa.step = 1 << i;
+        aa.sigma_depth = p.sigma_depth;
+        aa.sigma_normal = p.sigma_normal;
+        aa.sigma_light = p.sigma_light;
+        aa.in_d = st.buf_d[c];
+        aa.in_i = st.buf_i[c];
+        const bool last_pass = i == passes - 1;
+        aa.out_d = last_pass ? out_d : st.buf_d[1 - c];
+        aa.out_i = last_pass ? out_i : st.buf_i[1 - c];
+        aa.edge = st.edge;
+        aa.tag = st.tag;
+        if (aa.step == 1 && tiled)
+            k_svgf_atrous_tiled<1><<<gt, bt, 0, s>>>(aa, gc);
+        else if (aa.step == 2 && tiled)
+            k_svgf_atrous_tiled<2><<<gt, bt, 0, s>>>(aa, gc);
+        else
             k_svgf_atrous<<<g, b, 0, s>>>(aa, gc);
-            ++launches;
-            c = 1 - c;
-        }
+        ++launches;
+        c = 1 - c;
     }
     CRT_CUDA(cudaGetLastError());
-    CRT_CUDA(cudaMemcpyAsync(out_d, st.buf_d[c], bytes, cudaMemcpyDeviceToDevice, s));
-    CRT_CUDA(cudaMemcpyAsync(out_i, st.buf_i[c], bytes, cudaMemcpyDeviceToDevice, s));
     st.t = 1 - t;
     st.first = false;
     return launches;

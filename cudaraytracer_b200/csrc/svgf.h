@@ -30,6 +30,8 @@ struct SvgfState {
     float4 *hist_d[2] = {}, *hist_i[2] = {};
     float2 *mom_d[2] = {}, *mom_i[2] = {};
     int *hlen[2] = {};
+    float4 *edge = nullptr;  // per-pixel decoded normal + depth of the current frame
+    int2 *tag = nullptr;     // per-pixel material | mesh << 16, history length
     int t = 0;
     bool first = true;
     void allocate(int w, int h);

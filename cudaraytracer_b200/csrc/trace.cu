@@ -87,9 +87,26 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8(BvhView bvh, cons
     trace_dynamic8<true, kShort>(job, n, s_stack);
 }
 
+template <int kShort>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_closest8r(BvhView bvh, const float4 *__restrict__ rays, int n,
+                                                                 float4 *__restrict__ hits) {
+    __shared__ unsigned s_stack[kShort * kTraceBlock];
+    ClosestJob job{bvh, rays, hits};
+    trace_dynamic8<true, kShort, ClosestJob, true>(job, n, s_stack);
+}
+
+template <int kShort>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8r(BvhView bvh, const float4 *__restrict__ q, int n,
+                                                                uint8_t *__restrict__ occ) {
+    __shared__ unsigned s_stack[kShort * kTraceBlock];
+    ShadowJob job{bvh, q, occ, {}};
+    trace_dynamic8<true, kShort, ShadowJob, true>(job, n, s_stack);
+}
+
 // Traversal variant: 8 = the 8-wide tree with a 16-entry shared-memory
-// stack (default), 82 = the same with 8 entries, 2 = the binary tree with
-// a local-memory stack. CRT_TRAVERSAL overrides the default.
+// stack (default), 82 = the same with 8 entries, 83 = 16 entries with the
+// visited node's links kept in registers, 2 = the binary tree with a
+// local-memory stack. CRT_TRAVERSAL overrides the default.
 static int traversal_variant() {
     const char *e = getenv("CRT_TRAVERSAL");
     return e ? atoi(e) : 8;
@@ -113,6 +130,9 @@ void launch_trace_closest(const BvhView &bvh, const float4 *d_rays, int64_t n, f
     else if (v == 82)
         k_trace_closest8<8><<<trace_grid((const void *)k_trace_closest8<8>, n), kTraceBlock, 0, s>>>(
             bvh, d_rays, (int)n, d_hits);
+    else if (v == 83)
+        k_trace_closest8r<16><<<trace_grid((const void *)k_trace_closest8r<16>, n), kTraceBlock, 0, s>>>(
+            bvh, d_rays, (int)n, d_hits);
     else
         k_trace_closest<<<trace_grid((const void *)k_trace_closest, n), kTraceBlock, 0, s>>>(bvh, d_rays, (int)n,
                                                                                             d_hits);
@@ -130,6 +150,9 @@ void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_
     else if (v == 82)
         k_trace_shadow8<8><<<trace_grid((const void *)k_trace_shadow8<8>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
                                                                                                   d_occ);
+    else if (v == 83)
+        k_trace_shadow8r<16><<<trace_grid((const void *)k_trace_shadow8r<16>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
+                                                                                                      d_occ);
     else
         k_trace_shadow<<<trace_grid((const void *)k_trace_shadow, n), kTraceBlock, 0, s>>>(bvh, q, (int)n, d_occ);
     CRT_CUDA(cudaGetLastError());

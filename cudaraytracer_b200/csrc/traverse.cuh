@@ -132,7 +132,7 @@ __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
 // finished take new rays as above. Hit records equal closest_hit's (same
 // triangle test, conservative boxes); only the order in which equal-t
 // triangles are met may differ.
-template <bool kCull, int kShort, class Job>
+template <bool kCull, int kShort, class Job, bool kRegLinks = false>
 __device__ __forceinline__ void trace_dynamic8(Job &job, int n, unsigned *s_stack) {
     const unsigned lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -153,6 +153,8 @@ __device__ __forceinline__ void trace_dynamic8(Job &job, int n, unsigned *s_stac
     st.col = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     st.sp = 0;
+    int lk[8];
+    bool fresh = false;
 
     while (true) {
         const unsigned idle = __ballot_sync(0xffffffffu, idx < 0);
@@ -169,6 +171,8 @@ __device__ __forceinline__ void trace_dynamic8(Job &job, int n, unsigned *s_stac
                 hit.slot = -1;
                 hit.b1 = hit.b2 = 0.f;
                 st.reset();
+                if (kRegLinks) load_links8(bvh.wlinks, 0, lk);
+                fresh = kRegLinks;
                 cur = visit8(bvh.wnodes, 0, o, inv, tmin, hit.t, oct);
             }
             cbase += take;
@@ -176,7 +180,7 @@ __device__ __forceinline__ void trace_dynamic8(Job &job, int n, unsigned *s_stac
         }
         if (__ballot_sync(0xffffffffu, idx >= 0) == 0) break;
         if (idx < 0) continue;
-        const int leaf = next_leaf8(bvh, cur, st, o, inv, tmin, hit.t, oct);
+        const int leaf = next_leaf8<kShort, kRegLinks>(bvh, cur, st, o, inv, tmin, hit.t, oct, lk, fresh);
         bool finished = leaf == 0;
         if (!finished) {
             const int code = ~leaf;
