@@ -98,6 +98,7 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
         for (int k = 0; k < 5; ++k) q[j].p[k] = sc.wf.q[j][k];
     ShadowView sh{{sc.wf.shadow[0], sc.wf.shadow[1], sc.wf.shadow[2], sc.wf.shadow[3]}};
     const int blk = sc.rp.block();
+    const bool smem = stage_smem_stack();
     const int g_ext = persistent_grid((const void *)k_extend, blk);
     const int g_sh = persistent_grid((const void *)k_shade, blk);
     const int g_sd = persistent_grid((const void *)k_shadow, blk);
@@ -115,12 +116,12 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
             const int in = b & 1, out = 1 - in;
             StepParams bp = sp;
             bp.bounce = b;
-            k_extend<<<g_ext, blk, 0, s>>>(stage_bvh(view.bvh), q[in], sc.wf.counters + in, sc.wf.hits, sc.wf.counters,
-                                           out);
+            k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], sc.wf.counters + in, sc.wf.hits, sc.wf.counters, out,
+                                           smem);
             k_shade<<<g_sh, blk, 0, s>>>(view, bp, q[in], sc.wf.hits, sc.wf.counters + in, q[out], sc.wf.counters,
                                          out, sh, sc.wf.term[0], sc.wf.term[1], av);
-            k_shadow<<<g_sd, blk, 0, s>>>(stage_bvh(view.bvh), sh, sc.wf.counters, q[out], sc.wf.term[0], sc.wf.term[1],
-                                          av);
+            k_shadow<<<g_sd, blk, 0, s>>>(view.bvh, sh, sc.wf.counters, q[out], sc.wf.term[0], sc.wf.term[1], av,
+                                          smem);
         }
         k_advance_pass<<<1, 1, 0, s>>>(d_pass, chunk);
     };

@@ -33,7 +33,17 @@ struct BvhView {
     int num_tris;
     const float4 *wnodes;  // 8-wide quantised nodes, 4 float4 each (bvh8.cuh)
     const int *wlinks;     // 8 child links per wide node
+    int num_nodes;         // binary nodes (bound of interior links)
+    int *err;              // device error word (kErrTraversalBounds), or null
 };
+
+#ifdef __CUDACC__
+// Records a traversal that met an index outside the tree (the traversal
+// then stops instead of reading out of bounds).
+__device__ __forceinline__ void report_traversal_bounds(const BvhView &bvh) {
+    if (bvh.err) atomicOr(bvh.err, kErrTraversalBounds);
+}
+#endif
 
 __host__ __device__ __forceinline__ int leaf_link(int first, int count) { return ~((first << 4) | count); }
 
@@ -114,21 +124,79 @@ __device__ __forceinline__ void load_node(const float4 *nd, float4 &n0, float4 &
         : "l"(nd + 2));
 }
 
+// Traversal stacks with one interface (reset / empty / push / pop of 32-bit
+// entries; at most kStackSize entries, which the builder's depth bound
+// guarantees).
+//
+// LocalStack: the whole stack in the thread's local memory (L1-cached,
+// spilled to L2 under pressure).
+struct LocalStack {
+    unsigned s[kStackSize];
+    int sp;
+    __device__ __forceinline__ void reset() { sp = 0; }
+    __device__ __forceinline__ bool empty() const { return sp == 0; }
+    __device__ __forceinline__ void push(unsigned v) { s[sp++] = v; }
+    __device__ __forceinline__ unsigned pop() { return s[--sp]; }
+};
+
+// ShortStack: the top kShort entries (a power of two) in shared memory, one
+// column per thread (`col` = &smem[threadIdx.x], `stride` = words per
+// level = threads per block), so the 32 lanes of a warp touch 32 different
+// banks at every level; deeper entries spill to local memory, oldest first.
+template <int kShort>
+struct ShortStack {
+    unsigned *col;
+    int stride;
+    int sp;
+    unsigned spill[kStackSize - kShort];
+    __device__ __forceinline__ void reset() { sp = 0; }
+    __device__ __forceinline__ bool empty() const { return sp == 0; }
+    __device__ __forceinline__ void push(unsigned v) {
+        unsigned *slot = col + (sp & (kShort - 1)) * stride;
+        if (sp >= kShort) spill[sp - kShort] = *slot;
+        *slot = v;
+        ++sp;
+    }
+    __device__ __forceinline__ unsigned pop() {
+        --sp;
+        unsigned *slot = col + (sp & (kShort - 1)) * stride;
+        const unsigned v = *slot;
+        if (sp >= kShort) *slot = spill[sp - kShort];
+        return v;
+    }
+};
+
+template <bool kEarlyExit, bool kCull = true, class Stack>
+__device__ __forceinline__ Hit closest_hit_st(const BvhView &bvh, Stack &st, V3 o, V3 d, float tmin, float tmax,
+                                              float t_exit = 0.f);
+
+// closest_hit with the whole stack in local memory.
 template <bool kEarlyExit, bool kCull = true>
 __device__ __forceinline__ Hit closest_hit(const BvhView &bvh, V3 o, V3 d, float tmin, float tmax,
                                            float t_exit = 0.f) {
+    LocalStack st;
+    return closest_hit_st<kEarlyExit, kCull>(bvh, st, o, d, tmin, tmax, t_exit);
+}
+
+// The ordered traversal over a given stack (far child pushed, near child
+// descended first; the empty stack ends it).
+template <bool kEarlyExit, bool kCull, class Stack>
+__device__ __forceinline__ Hit closest_hit_st(const BvhView &bvh, Stack &st, V3 o, V3 d, float tmin, float tmax,
+                                              float t_exit) {
     Hit hit;
     hit.t = tmax;
     hit.slot = -1;
     hit.b1 = hit.b2 = 0.f;
     V3 inv = v3(rrcp(d.x), rrcp(d.y), rrcp(d.z));
-    int stack[kStackSize];
-    int sp = 0;
-    stack[sp++] = kSentinel;
+    st.reset();
     int link = 0;  // root interior node
     while (link != kSentinel) {
         // Descend interior nodes until a leaf link or an empty stack.
         while (link >= 0) {
+            if (link >= bvh.num_nodes) {
+                report_traversal_bounds(bvh);
+                return hit;
+            }
             const float4 *n = bvh.nodes + 4 * (size_t)link;
             float4 n0 = __ldg(n + 0), n1 = __ldg(n + 1), n2 = __ldg(n + 2);
             int4 n3 = __ldg(reinterpret_cast<const int4 *>(n + 3));
@@ -138,20 +206,28 @@ __device__ __forceinline__ Hit closest_hit(const BvhView &bvh, V3 o, V3 d, float
             if (h0 && h1) {
                 int near = n3.x, far = n3.y;
                 if (t1 < t0) { near = n3.y; far = n3.x; }
-                stack[sp++] = far;
+                if (st.sp >= kStackSize) {
+                    report_traversal_bounds(bvh);
+                    return hit;
+                }
+                st.push((unsigned)far);
                 link = near;
             } else if (h0) {
                 link = n3.x;
             } else if (h1) {
                 link = n3.y;
             } else {
-                link = stack[--sp];
+                link = st.empty() ? kSentinel : (int)st.pop();
             }
         }
         if (link == kSentinel) break;
         // Leaf.
         int code = ~link;
         int first = code >> 4, count = code & 15;
+        if (first + count > bvh.num_tris) {
+            report_traversal_bounds(bvh);
+            return hit;
+        }
         for (int k = 0; k < count; ++k) {
             int slot = first + k;
             const float4 *tp = bvh.tris + 3 * (size_t)slot;
@@ -159,7 +235,7 @@ __device__ __forceinline__ Hit closest_hit(const BvhView &bvh, V3 o, V3 d, float
             bool acc = intersect_triangle<kCull>(o, d, a, b, c, slot, hit);
             if (kEarlyExit && acc && hit.t < t_exit) return hit;
         }
-        link = stack[--sp];
+        link = st.empty() ? kSentinel : (int)st.pop();
     }
     return hit;
 }

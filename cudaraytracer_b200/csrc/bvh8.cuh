@@ -98,34 +98,6 @@ __device__ __forceinline__ unsigned ray_octant(V3 d) {
     return (d.x < 0.f ? 4u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 1u : 0u);
 }
 
-// Per-lane traversal stack: the top kShort entries in shared memory (one
-// column per thread, so the 32 lanes of a warp touch 32 banks), deeper
-// entries spilled to local memory. Entries are (wide node << 8 | mask of
-// children still to visit). The stack holds at most one entry per tree
-// level, and the builder keeps the depth below kBvh8MaxDepth.
-template <int kShort>
-struct ShortStack {
-    unsigned *col;  // &smem[threadIdx.x], stride `stride` words per level
-    int stride;
-    int sp;
-    unsigned spill[kBvh8MaxDepth - kShort];
-    __device__ __forceinline__ void reset() { sp = 0; }
-    __device__ __forceinline__ bool empty() const { return sp == 0; }
-    __device__ __forceinline__ void push(unsigned v) {
-        unsigned *slot = col + (sp & (kShort - 1)) * stride;
-        if (sp >= kShort) spill[sp - kShort] = *slot;
-        *slot = v;
-        ++sp;
-    }
-    __device__ __forceinline__ unsigned pop() {
-        --sp;
-        unsigned *slot = col + (sp & (kShort - 1)) * stride;
-        const unsigned v = *slot;
-        if (sp >= kShort) *slot = spill[sp - kShort];
-        return v;
-    }
-};
-
 // Finds the next leaf of an ordered traversal. `cur` holds the current
 // wide node and its children still to visit; returns a leaf link (< 0), or
 // 0 when the stack is exhausted. With kRegLinks the links of the node last

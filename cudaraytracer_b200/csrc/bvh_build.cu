@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cstring>
 #include <chrono>
+#include <cstdlib>
 
 namespace crt {
 namespace {
@@ -787,9 +788,14 @@ void build_bvh(const float *d_verts, int n, cudaStream_t stream, BvhBuffers &out
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     out.num_tris = n;
-    const auto w0 = std::chrono::steady_clock::now();
-    build_bvh8(out, stream);
-    out.wide_build_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - w0).count();
+    // The 8-wide quantised tree is built only on request (CRT_BVH8=1): its
+    // traversal measured slower than the binary one on the icosphere field.
+    const char *w8 = getenv("CRT_BVH8");
+    if (w8 && w8[0] == '1') {
+        const auto w0 = std::chrono::steady_clock::now();
+        build_bvh8(out, stream);
+        out.wide_build_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - w0).count();
+    }
 }
 
 void free_bvh(BvhBuffers &b) {

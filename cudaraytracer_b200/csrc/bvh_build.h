@@ -21,7 +21,8 @@ struct BvhBuffers {
     int64_t num_wide_nodes = 0;
     int wide_depth = 0;
     float wide_build_ms = 0.f;
-    BvhView view() const { return BvhView{nodes, tris, num_tris, wnodes, wlinks}; }
+    int *err = nullptr;  // the owning context's device error word
+    BvhView view() const { return BvhView{nodes, tris, num_tris, wnodes, wlinks, (int)num_nodes, err}; }
 };
 
 // Builds the BVH of n triangles given as n x 9 floats (v0, v1, v2) on the

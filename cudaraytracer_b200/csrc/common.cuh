@@ -17,6 +17,10 @@ struct Error : std::runtime_error {
 
 void set_last_error(const std::string &msg);
 
+// Bits of a context's device error word (crt_check_device_errors).
+constexpr int kErrWaitGaveUp = 1;       // a tensor-core kernel gave up a bounded mbarrier wait
+constexpr int kErrTraversalBounds = 2;  // a BVH traversal met an out-of-range node, leaf or stack depth
+
 #define CRT_CUDA(call)                                                          \
     do {                                                                        \
         cudaError_t e_ = (call);                                                \

@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (tid == 0 && abort_flag) atomicExch(a.err, 1);
+    if (tid == 0 && abort_flag) atomicOr(a.err, kErrWaitGaveUp);
     if (warp == 1) tc::tmem_dealloc(tmem, ncols);
 }
 
@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (tid == 0 && abort_flag) atomicExch(a.err, 1);
+    if (tid == 0 && abort_flag) atomicOr(a.err, kErrWaitGaveUp);
     if (warp == 1) tc::tmem_dealloc(tmem, ncols);
 }
 
@@ -716,7 +716,7 @@ __global__ void __launch_bounds__(kThreads) k_conv3x3_wgrad(WgradArgs a) {
             }
         }
     }
-    if (failed && tid == 0) atomicExch(a.err, 1);
+    if (failed && tid == 0) atomicOr(a.err, kErrWaitGaveUp);
     tc::cp_async_wait_all();
     tc::fence_before_sync();
     __syncthreads();
@@ -1001,6 +1001,8 @@ extern "C" crt_status crt_check_device_errors(crt_ctx *ctx) {
         CRT_CUDA(cudaMemcpy(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
         if (e) {
             CRT_CUDA(cudaMemset(ctx->d_err, 0, sizeof(int)));
+            if (e & kErrTraversalBounds)
+                throw Error(CRT_ERR_CUDA, "a BVH traversal met an out-of-range node, leaf or stack depth and stopped");
             throw Error(CRT_ERR_TIMEOUT, "a tensor-core kernel gave up waiting on an mbarrier");
         }
     });

@@ -41,25 +41,27 @@ struct ShadowView {
 };
 
 __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *counters);
-__global__ void k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters, int out_idx);
+__global__ void k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters, int out_idx,
+                         bool smem_stack);
 __global__ void k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits, const int *n_in, QueueView qout,
                         int *counters, int out_idx, ShadowView sh, float4 *term0, float4 *term1, AccumView acc);
 __global__ void k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueView qout, float4 *term0,
-                         float4 *term1, AccumView acc);
+                         float4 *term1, AccumView acc, bool smem_stack);
 
 // Blocks per grid for a persistent launch of `kernel` (all SMs at full
 // occupancy).
 int persistent_grid(const void *kernel, int block);
 
 // Traversal stack entries per thread kept in shared memory by the extend
-// and shadow stages (8-wide tree; deeper entries spill to local memory),
-// and the largest block those stages are launched with.
+// and shadow stages (deeper entries spill to local memory), and the
+// largest block those stages are launched with.
 constexpr int kStageShort = 8;
 constexpr int kStageMaxBlock = 256;
+constexpr bool kStageSmemStackDefault = true;
 
-// The BVH view the stage kernels get: the 8-wide tree when the scene has
-// one (always, after build_bvh), unless CRT_TRAVERSAL=2 selects the binary
-// tree with its local-memory stack.
-BvhView stage_bvh(BvhView v);
+// Whether the extend and shadow stages keep the top of each lane's
+// traversal stack in shared memory (ShortStack) or the whole stack in
+// local memory (LocalStack); CRT_STAGE_STACK=local selects the latter.
+bool stage_smem_stack();
 
 }  // namespace crt

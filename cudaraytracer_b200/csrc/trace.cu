@@ -69,6 +69,30 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow(BvhView bvh, const
     trace_dynamic<true>(job, n);
 }
 
+// The binary traversal with the per-lane short stack in shared memory
+// (kShort entries per lane, kShort x 128 words per block).
+template <int kShort>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_closest_s(BvhView bvh, const float4 *__restrict__ rays, int n,
+                                                                 float4 *__restrict__ hits) {
+    __shared__ unsigned s_stack[kShort * kTraceBlock];
+    ShortStack<kShort> st;
+    st.col = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
+    ClosestJob job{bvh, rays, hits};
+    trace_dynamic_st<true>(job, n, st);
+}
+
+template <int kShort>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_shadow_s(BvhView bvh, const float4 *__restrict__ q, int n,
+                                                                uint8_t *__restrict__ occ) {
+    __shared__ unsigned s_stack[kShort * kTraceBlock];
+    ShortStack<kShort> st;
+    st.col = s_stack + threadIdx.x;
+    st.stride = blockDim.x;
+    ShadowJob job{bvh, q, occ, {}};
+    trace_dynamic_st<true>(job, n, st);
+}
+
 // The same over the 8-wide quantised tree with the shared-memory short
 // stack (kShort entries per lane, kShort x 128 words per block).
 template <int kShort>
@@ -103,13 +127,17 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8r(BvhView bvh, con
     trace_dynamic8<true, kShort, ShadowJob, true>(job, n, s_stack);
 }
 
-// Traversal variant: 8 = the 8-wide tree with a 16-entry shared-memory
-// stack (default), 82 = the same with 8 entries, 83 = 16 entries with the
-// visited node's links kept in registers, 2 = the binary tree with a
-// local-memory stack. CRT_TRAVERSAL overrides the default.
+// Traversal variant of the trace kernels (CRT_TRAVERSAL overrides the
+// default kTraceVariant): 2 = binary tree, stack in local memory;
+// 28 / 216 = binary tree, top 8 / 16 stack entries per lane in shared
+// memory; 8 / 82 = 8-wide quantised tree (built only with CRT_BVH8=1),
+// 16 / 8 shared-memory entries; 83 = the same as 8 with the visited node's
+// links kept in registers.
+constexpr int kTraceVariant = 2;
+
 static int traversal_variant() {
     const char *e = getenv("CRT_TRAVERSAL");
-    return e ? atoi(e) : 8;
+    return e ? atoi(e) : kTraceVariant;
 }
 
 // Persistent grid (all SMs at full occupancy), fewer blocks for small
@@ -123,8 +151,15 @@ static int trace_grid(const void *kernel, int64_t n) {
 void launch_trace_closest(const BvhView &bvh, const float4 *d_rays, int64_t n, float4 *d_hits, cudaStream_t s) {
     if (n <= 0) return;
     CRT_CHECK(n < (int64_t)1 << 31, CRT_ERR_CAPACITY, "trace batch larger than 2^31 rays");
-    const int v = bvh.wnodes ? traversal_variant() : 2;
-    if (v == 8)
+    int v = traversal_variant();
+    if ((v == 8 || v == 82 || v == 83) && !bvh.wnodes) v = 2;
+    if (v == 28)
+        k_trace_closest_s<8><<<trace_grid((const void *)k_trace_closest_s<8>, n), kTraceBlock, 0, s>>>(
+            bvh, d_rays, (int)n, d_hits);
+    else if (v == 216)
+        k_trace_closest_s<16><<<trace_grid((const void *)k_trace_closest_s<16>, n), kTraceBlock, 0, s>>>(
+            bvh, d_rays, (int)n, d_hits);
+    else if (v == 8)
         k_trace_closest8<16><<<trace_grid((const void *)k_trace_closest8<16>, n), kTraceBlock, 0, s>>>(
             bvh, d_rays, (int)n, d_hits);
     else if (v == 82)
@@ -143,8 +178,15 @@ void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_
     if (n <= 0) return;
     CRT_CHECK(n < (int64_t)1 << 31, CRT_ERR_CAPACITY, "trace batch larger than 2^31 queries");
     const float4 *q = reinterpret_cast<const float4 *>(d_q);
-    const int v = bvh.wnodes ? traversal_variant() : 2;
-    if (v == 8)
+    int v = traversal_variant();
+    if ((v == 8 || v == 82 || v == 83) && !bvh.wnodes) v = 2;
+    if (v == 28)
+        k_trace_shadow_s<8><<<trace_grid((const void *)k_trace_shadow_s<8>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
+                                                                                                  d_occ);
+    else if (v == 216)
+        k_trace_shadow_s<16><<<trace_grid((const void *)k_trace_shadow_s<16>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
+                                                                                                    d_occ);
+    else if (v == 8)
         k_trace_shadow8<16><<<trace_grid((const void *)k_trace_shadow8<16>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
                                                                                                     d_occ);
     else if (v == 82)

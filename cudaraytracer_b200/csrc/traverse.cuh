@@ -30,8 +30,19 @@ namespace crt {
 
 #ifdef __CUDACC__
 
+template <bool kCull, class Job, class Stack>
+__device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st);
+
+// The stack in local memory.
 template <bool kCull, class Job>
 __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
+    LocalStack st;
+    trace_dynamic_st<kCull>(job, n, st);
+}
+
+// Over a given per-lane stack (LocalStack or ShortStack, bvh.cuh).
+template <bool kCull, class Job, class Stack>
+__device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
     const unsigned lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     // warp-uniform: the rays [cbase, cbase + cleft) of this warp not yet started
@@ -41,15 +52,15 @@ __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
     int cleft = (int)((w + 1) * n / warps) - cbase;
     // per-lane ray state
     int idx = -1;
-    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr};
+    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr, 0, nullptr};
     V3 o{0.f, 0.f, 0.f}, d{0.f, 0.f, 0.f}, inv{0.f, 0.f, 0.f};
     float tmin = 0.f, t_exit = 0.f;
     Hit hit;
     hit.t = 0.f;
     hit.slot = -1;
     hit.b1 = hit.b2 = 0.f;
-    int stack[kStackSize];
-    int sp = 0, link = kSentinel;
+    int link = kSentinel;
+    st.reset();
 
     auto start = [&](int k) {
         idx = k;
@@ -59,8 +70,7 @@ __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
         hit.t = tmax;
         hit.slot = -1;
         hit.b1 = hit.b2 = 0.f;
-        sp = 0;
-        stack[sp++] = kSentinel;
+        st.reset();
         link = 0;
     };
 
@@ -76,7 +86,12 @@ __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
         if (__ballot_sync(0xffffffffu, idx >= 0) == 0) break;  // nothing in flight and nothing left
         if (idx < 0) continue;
         // one while-while iteration of closest_hit
+        bool bad = false;
         while (link >= 0) {
+            if (link >= bvh.num_nodes) {
+                bad = true;
+                break;
+            }
             float4 n0, n1, n2;
             int4 n3;
             load_node(bvh.nodes + 4 * (size_t)link, n0, n1, n2, n3);
@@ -89,17 +104,31 @@ __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
                     near = n3.y;
                     far = n3.x;
                 }
-                stack[sp++] = far;
+                if (st.sp >= kStackSize) {
+                    bad = true;
+                    break;
+                }
+                st.push((unsigned)far);
                 link = near;
             } else if (h0) {
                 link = n3.x;
             } else if (h1) {
                 link = n3.y;
             } else {
-                link = stack[--sp];
+                link = st.empty() ? kSentinel : (int)st.pop();
             }
         }
         bool finished = link == kSentinel;
+        if (!finished && !bad) {
+            const int code = ~link;
+            const int first = code >> 4, count = code & 15;
+            bad = first + count > bvh.num_tris;
+        }
+        if (bad) {
+            // an index outside the tree: record it and end this ray
+            report_traversal_bounds(bvh);
+            finished = true;
+        }
         if (!finished) {
             const int code = ~link;
             const int first = code >> 4, count = code & 15;
@@ -114,7 +143,7 @@ __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
                 }
             }
             if (!finished) {
-                link = stack[--sp];
+                link = st.empty() ? kSentinel : (int)st.pop();
                 finished = link == kSentinel;
             }
         }
@@ -141,7 +170,7 @@ __device__ __forceinline__ void trace_dynamic8(Job &job, int n, unsigned *s_stac
     int cbase = (int)(w * n / warps);
     int cleft = (int)((w + 1) * n / warps) - cbase;
     int idx = -1;
-    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr};
+    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr, 0, nullptr};
     V3 o{0.f, 0.f, 0.f}, d{0.f, 0.f, 0.f}, inv{0.f, 0.f, 0.f};
     float tmin = 0.f, t_exit = 0.f;
     unsigned oct = 0, cur = 0;

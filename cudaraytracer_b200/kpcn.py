@@ -71,8 +71,9 @@ def conv3x3_backward_weights(ctx, x, g, dw=None, stream=None):
 
 
 def check_device_errors(ctx) -> None:
-    """Raises CrtError (CRT_ERR_TIMEOUT) if a tensor-core kernel gave up a
-    bounded wait since the last check."""
+    """Raises CrtError if a kernel of ctx recorded a device-side error since
+    the last check (CRT_ERR_TIMEOUT: a tensor-core kernel gave up a bounded
+    wait)."""
     _lib.call("crt_check_device_errors", ctx.handle)
 
 

@@ -60,6 +60,13 @@ class Context:
             raise RuntimeError("context is closed")
         self._children.add(obj)
 
+    def check_device_errors(self) -> None:
+        """Synchronises and raises CrtError if a kernel of this context
+        recorded a device-side error since the last check (a BVH traversal
+        that met an index outside its tree, or a tensor-core kernel that gave
+        up a bounded wait)."""
+        _lib.call("crt_check_device_errors", self._h)
+
     def close(self):
         if self._h:
             # servers first: they reference scenes

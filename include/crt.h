@@ -511,8 +511,11 @@ crt_status crt_kpcn_train_step(crt_kpcn *k, int32_t n, int32_t h, int32_t w, con
  * 14 cat0; `bytes` must equal the tensor's size. */
 crt_status crt_kpcn_debug_tensor(crt_kpcn *k, int32_t which, void *host, int64_t bytes);
 
-/* Synchronises the device and returns CRT_ERR_TIMEOUT (clearing the flag)
- * when a tensor-core kernel of this context gave up a bounded wait. */
+/* Synchronises the device and reports (clearing the flag) a device-side
+ * error recorded by this context's kernels: CRT_ERR_TIMEOUT when a
+ * tensor-core kernel gave up a bounded wait, CRT_ERR_CUDA when a BVH
+ * traversal met a node, leaf or stack depth outside the tree and stopped
+ * that ray instead of reading out of bounds. */
 crt_status crt_check_device_errors(crt_ctx *ctx);
 
 #ifdef __cplusplus

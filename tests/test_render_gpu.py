@@ -160,3 +160,21 @@ def test_textured_two_light_render_matches_oracle(crt_ctx, textured_json):
     # the textures show: the back wall is not uniform
     back = (d + i)[..., :3][24:40, 16:32].reshape(-1, 3)
     assert back.std(0).max() > 0.02
+
+
+def test_stage_stack_in_shared_or_local_memory_agree(crt_ctx, ico_json, monkeypatch):
+    """The extend and shadow stages give the same frame whether the top of
+    each lane's traversal stack lives in shared memory (default) or the
+    whole stack in local memory (CRT_STAGE_STACK=local), up to the order of
+    the float atomics that add paths into pixels, and no traversal records
+    an out-of-range index."""
+    sc = Scene.load(crt_ctx, ico_json)
+    sc.set_render_params(seed=4)
+    monkeypatch.setenv("CRT_STAGE_STACK", "local")
+    d0, i0 = sc.render(4)
+    crt_ctx.check_device_errors()
+    monkeypatch.setenv("CRT_STAGE_STACK", "shared")
+    d1, i1 = sc.render(4)
+    crt_ctx.check_device_errors()
+    np.testing.assert_allclose(d1, d0, rtol=1e-5, atol=1e-5)
+    np.testing.assert_allclose(i1, i0, rtol=1e-5, atol=1e-5)

@@ -147,3 +147,27 @@ def test_empty_batches_and_errors(crt_ctx, cornell_tris):
     assert sc.trace_shadow(np.zeros((0, 12), np.float32)).shape == (0,)
     with pytest.raises(CrtError):
         Scene.from_triangles(crt_ctx, np.zeros((0, 9), np.float32))
+
+
+@pytest.mark.parametrize("variant", ["28", "216", "8", "82", "83"])
+def test_traversal_variants_agree(crt_ctx, ico_tris, variant, monkeypatch):
+    """Every traversal variant of the trace kernels (binary tree with the
+    top of each lane's stack in shared memory, 8 or 16 entries; the 8-wide
+    quantised tree, built on request) returns the hit records and shadow
+    answers of the binary traversal with its stack in local memory, ties
+    aside, and records no out-of-range index."""
+    import os
+
+    rays = scenes.random_rays(ico_tris, 1 << 18, seed=9)
+    q = scenes.random_shadow_queries(ico_tris, 1 << 18, seed=10)
+    monkeypatch.setenv("CRT_BVH8", "1")
+    sc = Scene.from_triangles(crt_ctx, ico_tris)
+    assert sc.info()["num_wide_nodes"] > 0
+    monkeypatch.setenv("CRT_TRAVERSAL", "2")
+    base_h, base_o = sc.trace_closest(rays), sc.trace_shadow(q)
+    monkeypatch.setenv("CRT_TRAVERSAL", variant)
+    h, o = sc.trace_closest(rays), sc.trace_shadow(q)
+    crt_ctx.check_device_errors()
+    assert_hits_match(h, base_h, ico_tris, rays)
+    assert (o != base_o).sum() <= 2
+    sc.close()
