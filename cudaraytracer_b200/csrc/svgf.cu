@@ -431,6 +431,9 @@ __device__ __forceinline__ void variance_pixel(const VarianceArgs &a, const GB &
     V3 fd{0.f, 0.f, 0.f}, fi{0.f, 0.f, 0.f};
     float fmd0 = 0.f, fmd1 = 0.f, fmi0 = 0.f, fmi1 = 0.f, twd = 0.f, twi = 0.f;
     float sd = a.sigma_depth * fmaxf(dz, 1e-4f);
+    // quotients as products with per-pixel reciprocals (see atrous_pixel)
+    const float inv_sl = 1.f / a.sigma_light;
+    const float il_scale = sqrtf(cil) * inv_sl;
     for (int kj = -a.half; kj <= a.half; kj++)
         for (int ki = -a.half; ki <= a.half; ki++) {
             int ni = x + ki, nj = y + kj;
@@ -447,8 +450,8 @@ __device__ __forceinline__ void variance_pixel(const VarianceArgs &a, const GB &
             float wz = -fabsf(cdepth - nz) / (sd * dist + 1e-4f);
             float wn = powf(fmaxf(0.f, dot(cn, nn)), a.sigma_normal);
             float dref = fmaxf(fmaxf(cdl, ndl), 1e-4f);
-            float wdl = -fabsf(cdl - ndl) / (a.sigma_light / sqrtf(dref));
-            float wil = -fabsf(cil - nil) / (a.sigma_light / sqrtf(cil));
+            float wdl = -fabsf(cdl - ndl) * sqrtf(dref) * inv_sl;
+            float wil = -fabsf(cil - nil) * il_scale;
             float dw = expf(wz + wdl) * wn, iw = expf(wz + wil) * wn;
             fd = fd + nd * dw;
             fi = fi + nid * iw;
@@ -598,6 +601,19 @@ __device__ __forceinline__ void atrous_pixel(const AtrousArgs &a, const GB &g, c
     float sli = a.sigma_light * (1.f + 1.5f * boot);
     float sn = fmaxf(8.f, a.sigma_normal * (1.f - 0.85f * boot));
     const float kw[3] = {3.f / 8.f, 1.f / 4.f, 1.f / 16.f};
+    // The per-tap quotients of the reference's weights become products with
+    // per-pixel reciprocals (same formula; the roundings differ by an ulp):
+    // wz = -|dz| / (sdep * dist + 1e-6) over the six tap distances of the
+    // 5x5 stencil, wdl = -|dl| * sqrt(dref) / (sld * sdd), and the indirect
+    // term's sqrt(iref) / (sli * sdi), constant over the taps.
+    const float inv_ld = 1.f / (sld * sdd);
+    const float il_scale = sqrtf(fmaxf(cil, 1e-4f)) / (sli * sdi);
+    float inv_z[6];
+    {
+        const int d2[6] = {0, 1, 2, 4, 5, 8};  // ki^2 + kj^2 of the stencil
+#pragma unroll
+        for (int k = 0; k < 6; ++k) inv_z[k] = 1.f / (sdep * (sqrtf(float(d2[k])) * a.step) + 1e-6f);
+    }
     for (int kj = -2; kj <= 2; kj++)
         for (int ki = -2; ki <= 2; ki++) {
             int ni = x + ki * a.step, nj = y + kj * a.step;
@@ -611,13 +627,14 @@ __device__ __forceinline__ void atrous_pixel(const AtrousArgs &a, const GB &g, c
             float4 nd4 = src.d(ni, nj), ni4 = src.i(ni, nj);
             V3 nd{nd4.x, nd4.y, nd4.z}, nic{ni4.x, ni4.y, ni4.z};
             float nvd = fmaxf(0.0f, nd4.w), nvi = fmaxf(0.0f, ni4.w);
-            float dist = sqrtf(float(ki * ki + kj * kj)) * a.step;
-            float wz = -fabsf(cdepth - nz) / (sdep * dist + 1e-6f);
+            const int r2 = ki * ki + kj * kj;
+            const int zi = r2 == 0 ? 0 : (r2 == 1 ? 1 : (r2 == 2 ? 2 : (r2 == 4 ? 3 : (r2 == 5 ? 4 : 5))));
+            float wz = -fabsf(cdepth - nz) * inv_z[zi];
             float wn = powf(fmaxf(0.f, dot(cn, nn)), sn);
             float ndl = luminance(nd), nil = luminance(nic);
-            float dref = fmaxf(fmaxf(cdl, ndl), 1e-4f), iref = fmaxf(cil, 1e-4f);
-            float wdl = -fabsf(cdl - ndl) / (sld * sdd / sqrtf(dref));
-            float wil = -fabsf(cil - nil) / (sli * sdi / sqrtf(iref));
+            float dref = fmaxf(fmaxf(cdl, ndl), 1e-4f);
+            float wdl = -fabsf(cdl - ndl) * sqrtf(dref) * inv_ld;
+            float wil = -fabsf(cil - nil) * il_scale;
             float hc = boot > 0.f ? (0.5f + 0.5f * fminf((float)nh / 4.f, 1.f)) : 1.f;
             float kwt = kw[abs(ki)] * kw[abs(kj)];
             float dw = expf(wz + wdl) * wn * kwt * hc, iw = expf(wz + wil) * wn * kwt * hc;

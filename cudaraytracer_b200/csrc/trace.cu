@@ -69,6 +69,38 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow(BvhView bvh, const
     trace_dynamic<true>(job, n);
 }
 
+// The binary traversal with its local stack, compiled for kMinBlocks
+// resident 128-thread blocks per SM (a register cap of 65536 / (128 x
+// kMinBlocks) per thread: more warps to hide load latency, against spills).
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTraceBlock, kMinBlocks) k_trace_closest_o(BvhView bvh, const float4 *__restrict__ rays,
+                                                                            int n, float4 *__restrict__ hits) {
+    ClosestJob job{bvh, rays, hits};
+    trace_dynamic<true>(job, n);
+}
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTraceBlock, kMinBlocks) k_trace_shadow_o(BvhView bvh, const float4 *__restrict__ q,
+                                                                           int n, uint8_t *__restrict__ occ) {
+    ShadowJob job{bvh, q, occ, {}};
+    trace_dynamic<true>(job, n);
+}
+
+// The binary traversal with postponed leaves (traverse.cuh), local stack.
+__global__ void __launch_bounds__(kTraceBlock) k_trace_closest_p(BvhView bvh, const float4 *__restrict__ rays, int n,
+                                                                 float4 *__restrict__ hits) {
+    ClosestJob job{bvh, rays, hits};
+    LocalStack st;
+    trace_dynamic_spec<true>(job, n, st);
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_trace_shadow_p(BvhView bvh, const float4 *__restrict__ q, int n,
+                                                                uint8_t *__restrict__ occ) {
+    ShadowJob job{bvh, q, occ, {}};
+    LocalStack st;
+    trace_dynamic_spec<true>(job, n, st);
+}
+
 // The binary traversal with the per-lane short stack in shared memory
 // (kShort entries per lane, kShort x 128 words per block).
 template <int kShort>
@@ -128,7 +160,9 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8r(BvhView bvh, con
 }
 
 // Traversal variant of the trace kernels (CRT_TRAVERSAL overrides the
-// default kTraceVariant): 2 = binary tree, stack in local memory;
+// default kTraceVariant): 2 = binary tree, stack in local memory
+// (210 / 212: the same capped at 51 / 42 registers for 10 / 12 blocks per SM;
+// 3: with postponed leaves);
 // 28 / 216 = binary tree, top 8 / 16 stack entries per lane in shared
 // memory; 8 / 82 = 8-wide quantised tree (built only with CRT_BVH8=1),
 // 16 / 8 shared-memory entries; 83 = the same as 8 with the visited node's
@@ -153,7 +187,16 @@ void launch_trace_closest(const BvhView &bvh, const float4 *d_rays, int64_t n, f
     CRT_CHECK(n < (int64_t)1 << 31, CRT_ERR_CAPACITY, "trace batch larger than 2^31 rays");
     int v = traversal_variant();
     if ((v == 8 || v == 82 || v == 83) && !bvh.wnodes) v = 2;
-    if (v == 28)
+    if (v == 3)
+        k_trace_closest_p<<<trace_grid((const void *)k_trace_closest_p, n), kTraceBlock, 0, s>>>(bvh, d_rays, (int)n,
+                                                                                                d_hits);
+    else if (v == 210)
+        k_trace_closest_o<10><<<trace_grid((const void *)k_trace_closest_o<10>, n), kTraceBlock, 0, s>>>(
+            bvh, d_rays, (int)n, d_hits);
+    else if (v == 212)
+        k_trace_closest_o<12><<<trace_grid((const void *)k_trace_closest_o<12>, n), kTraceBlock, 0, s>>>(
+            bvh, d_rays, (int)n, d_hits);
+    else if (v == 28)
         k_trace_closest_s<8><<<trace_grid((const void *)k_trace_closest_s<8>, n), kTraceBlock, 0, s>>>(
             bvh, d_rays, (int)n, d_hits);
     else if (v == 216)
@@ -180,7 +223,15 @@ void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_
     const float4 *q = reinterpret_cast<const float4 *>(d_q);
     int v = traversal_variant();
     if ((v == 8 || v == 82 || v == 83) && !bvh.wnodes) v = 2;
-    if (v == 28)
+    if (v == 3)
+        k_trace_shadow_p<<<trace_grid((const void *)k_trace_shadow_p, n), kTraceBlock, 0, s>>>(bvh, q, (int)n, d_occ);
+    else if (v == 210)
+        k_trace_shadow_o<10><<<trace_grid((const void *)k_trace_shadow_o<10>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
+                                                                                                    d_occ);
+    else if (v == 212)
+        k_trace_shadow_o<12><<<trace_grid((const void *)k_trace_shadow_o<12>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
+                                                                                                    d_occ);
+    else if (v == 28)
         k_trace_shadow_s<8><<<trace_grid((const void *)k_trace_shadow_s<8>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
                                                                                                   d_occ);
     else if (v == 216)

@@ -154,6 +154,131 @@ __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
     }
 }
 
+// trace_dynamic with postponed leaves (the speculative while-while loop of
+// Aila and Laine, "Understanding the Efficiency of Ray Traversal on GPUs",
+// HPG 2009): a lane that reaches a leaf keeps it pending and goes on
+// descending while other lanes of the warp are still looking for their
+// first leaf, so the node loop runs with more lanes busy; a lane that
+// meets a second leaf stops there and keeps it for the next turn. Leaves
+// are tested in the order they are found; the extra node visits use the
+// closest hit of the leaves tested so far, so results equal closest_hit's
+// up to the order in which equal-t triangles are met.
+template <bool kCull, class Job, class Stack>
+__device__ __forceinline__ void trace_dynamic_spec(Job &job, int n, Stack &st) {
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int cbase = (int)(w * n / warps);
+    int cleft = (int)((w + 1) * n / warps) - cbase;
+    int idx = -1;
+    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr, 0, nullptr};
+    V3 o{0.f, 0.f, 0.f}, d{0.f, 0.f, 0.f}, inv{0.f, 0.f, 0.f};
+    float tmin = 0.f, t_exit = 0.f;
+    Hit hit;
+    hit.t = 0.f;
+    hit.slot = -1;
+    hit.b1 = hit.b2 = 0.f;
+    int link = kSentinel;
+    st.reset();
+
+    while (true) {
+        const unsigned idle = __ballot_sync(0xffffffffu, idx < 0);
+        if (idle && cleft > 0) {
+            const int take = min(__popc(idle), cleft);
+            const int rank = __popc(idle & lt);
+            if (idx < 0 && rank < take) {
+                idx = cbase + rank;
+                float tmax;
+                job.setup(idx, bvh, o, d, tmin, tmax, t_exit);
+                inv = v3(rrcp(d.x), rrcp(d.y), rrcp(d.z));
+                hit.t = tmax;
+                hit.slot = -1;
+                hit.b1 = hit.b2 = 0.f;
+                st.reset();
+                link = 0;
+            }
+            cbase += take;
+            cleft -= take;
+        }
+        if (__ballot_sync(0xffffffffu, idx >= 0) == 0) break;
+        if (idx < 0) continue;
+        int pending = 0;  // postponed leaf link (< 0), 0 = none
+        bool bad = false;
+        while (true) {
+            if (link >= 0) {
+                if (link >= bvh.num_nodes) {
+                    bad = true;
+                    break;
+                }
+                float4 n0, n1, n2;
+                int4 n3;
+                load_node(bvh.nodes + 4 * (size_t)link, n0, n1, n2, n3);
+                float t0, t1;
+                bool h0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, tmin, hit.t, t0);
+                bool h1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, tmin, hit.t, t1);
+                if (h0 && h1) {
+                    int near = n3.x, far = n3.y;
+                    if (t1 < t0) {
+                        near = n3.y;
+                        far = n3.x;
+                    }
+                    if (st.sp >= kStackSize) {
+                        bad = true;
+                        break;
+                    }
+                    st.push((unsigned)far);
+                    link = near;
+                } else if (h0) {
+                    link = n3.x;
+                } else if (h1) {
+                    link = n3.y;
+                } else {
+                    link = st.empty() ? kSentinel : (int)st.pop();
+                }
+            }
+            if (link < 0 && link != kSentinel && pending == 0) {
+                pending = link;
+                link = st.empty() ? kSentinel : (int)st.pop();
+            }
+            // go on while some lane of the warp still has no leaf to test
+            // (lanes holding a second leaf in `link`, or done, idle meanwhile)
+            const bool searching = pending == 0 && link != kSentinel;
+            if (!__any_sync(__activemask(), searching)) break;
+        }
+        bool finished = false;
+        if (!bad && pending != 0) {
+            const int code = ~pending;
+            const int first = code >> 4, count = code & 15;
+            if (first + count > bvh.num_tris) {
+                bad = true;
+            } else {
+                for (int k = 0; k < count; ++k) {
+                    const int slot = first + k;
+                    const float4 *tp = bvh.tris + 3 * (size_t)slot;
+                    float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                    const bool acc = intersect_triangle<kCull>(o, d, a, b, c, slot, hit);
+                    if (acc && hit.t < t_exit) {
+                        finished = true;
+                        break;
+                    }
+                }
+            }
+        }
+        if (bad) {
+            report_traversal_bounds(bvh);
+            finished = true;
+        }
+        // nothing left: no leaf in hand and the stack exhausted (no push
+        // follows a pop of the empty stack)
+        if (!finished && link == kSentinel) finished = true;
+        if (finished) {
+            job.finish(idx, bvh, hit);
+            idx = -1;
+        }
+    }
+}
+
 // trace_dynamic over the 8-wide quantised tree (bvh8.cuh) with the
 // per-lane short stack in shared memory: `s_stack` is the block's
 // kShort x blockDim.x word array. One loop turn finds the next leaf
