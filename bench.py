@@ -358,9 +358,9 @@ def svgf_leg(ctx, stream, frames=4, with_reference=True):
             rd, ri, rms = oracle.ref_svgf(nd, ni, g["pos_tri"], g["normal_mat"].view(np.uint16),
                                           g["bary_mesh"].view(np.uint16), g["motion_depth"], timing=True)
             ref_ms = float(np.median(rms[1:]))
-            mine = np.stack([np.stack([host(od), host(oi)]) for od, oi in outs])[..., :3].astype(np.float64)
+            crt_out = np.stack([np.stack([host(od), host(oi)]) for od, oi in outs])[..., :3].astype(np.float64)
             ref = np.stack([np.stack([rd[f], ri[f]]) for f in range(frames)])[..., :3].astype(np.float64)
-            dif = np.abs(mine - ref)
+            dif = np.abs(crt_out - ref)
             out["reference_cuda"] = {"ms_per_frame": round(ref_ms, 4), "ms_frames": [round(float(x), 4) for x in rms],
                                      "build": "reference renderer.cuh SVGF kernels, nvcc -O3 -rdc sm_100a, headless",
                                      "outputs_vs_crt": {

@@ -124,44 +124,47 @@ __device__ __forceinline__ void load_node(const float4 *nd, float4 &n0, float4 &
         : "l"(nd + 2));
 }
 
-// Traversal stacks with one interface (reset / empty / push / pop of 32-bit
-// entries; at most kStackSize entries, which the builder's depth bound
-// guarantees).
+// Traversal stacks with one interface: reset / empty / push / pop of 32-bit
+// entries, at most kStackSize of them (the builder's depth bound). The
+// stack object holds only scalars, so it lives in registers; the entries
+// that live in local memory are in a separate array of kLocal words that
+// the traversal declares and passes to push / pop.
 //
-// LocalStack: the whole stack in the thread's local memory (L1-cached,
-// spilled to L2 under pressure).
+// LocalStack: every entry in that local array (L1-cached; local stores
+// are written through to L2).
 struct LocalStack {
-    unsigned s[kStackSize];
+    static constexpr int kLocal = kStackSize;
     int sp;
     __device__ __forceinline__ void reset() { sp = 0; }
     __device__ __forceinline__ bool empty() const { return sp == 0; }
-    __device__ __forceinline__ void push(unsigned v) { s[sp++] = v; }
-    __device__ __forceinline__ unsigned pop() { return s[--sp]; }
+    __device__ __forceinline__ void push(unsigned v, unsigned *lm) { lm[sp++] = v; }
+    __device__ __forceinline__ unsigned pop(unsigned *lm) { return lm[--sp]; }
 };
 
 // ShortStack: the top kShort entries (a power of two) in shared memory, one
 // column per thread (`col` = &smem[threadIdx.x], `stride` = words per
 // level = threads per block), so the 32 lanes of a warp touch 32 different
-// banks at every level; deeper entries spill to local memory, oldest first.
+// banks at every level; deeper entries spill to the local array, oldest
+// first.
 template <int kShort>
 struct ShortStack {
+    static constexpr int kLocal = kStackSize - kShort;
     unsigned *col;
     int stride;
     int sp;
-    unsigned spill[kStackSize - kShort];
     __device__ __forceinline__ void reset() { sp = 0; }
     __device__ __forceinline__ bool empty() const { return sp == 0; }
-    __device__ __forceinline__ void push(unsigned v) {
+    __device__ __forceinline__ void push(unsigned v, unsigned *lm) {
         unsigned *slot = col + (sp & (kShort - 1)) * stride;
-        if (sp >= kShort) spill[sp - kShort] = *slot;
+        if (sp >= kShort) lm[sp - kShort] = *slot;
         *slot = v;
         ++sp;
     }
-    __device__ __forceinline__ unsigned pop() {
+    __device__ __forceinline__ unsigned pop(unsigned *lm) {
         --sp;
         unsigned *slot = col + (sp & (kShort - 1)) * stride;
         const unsigned v = *slot;
-        if (sp >= kShort) *slot = spill[sp - kShort];
+        if (sp >= kShort) *slot = lm[sp - kShort];
         return v;
     }
 };
@@ -188,6 +191,7 @@ __device__ __forceinline__ Hit closest_hit_st(const BvhView &bvh, Stack &st, V3 
     hit.slot = -1;
     hit.b1 = hit.b2 = 0.f;
     V3 inv = v3(rrcp(d.x), rrcp(d.y), rrcp(d.z));
+    unsigned lm[Stack::kLocal];
     st.reset();
     int link = 0;  // root interior node
     while (link != kSentinel) {
@@ -210,14 +214,14 @@ __device__ __forceinline__ Hit closest_hit_st(const BvhView &bvh, Stack &st, V3 
                     report_traversal_bounds(bvh);
                     return hit;
                 }
-                st.push((unsigned)far);
+                st.push((unsigned)far, lm);
                 link = near;
             } else if (h0) {
                 link = n3.x;
             } else if (h1) {
                 link = n3.y;
             } else {
-                link = st.empty() ? kSentinel : (int)st.pop();
+                link = st.empty() ? kSentinel : (int)st.pop(lm);
             }
         }
         if (link == kSentinel) break;
@@ -235,7 +239,7 @@ __device__ __forceinline__ Hit closest_hit_st(const BvhView &bvh, Stack &st, V3 
             bool acc = intersect_triangle<kCull>(o, d, a, b, c, slot, hit);
             if (kEarlyExit && acc && hit.t < t_exit) return hit;
         }
-        link = st.empty() ? kSentinel : (int)st.pop();
+        link = st.empty() ? kSentinel : (int)st.pop(lm);
     }
     return hit;
 }

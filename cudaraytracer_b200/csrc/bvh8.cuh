@@ -105,13 +105,13 @@ __device__ __forceinline__ unsigned ray_octant(V3 d) {
 // `fresh`), so descending into its children needs no further load; links of
 // nodes popped from the stack are read from memory.
 template <int kShort, bool kRegLinks = false>
-__device__ __forceinline__ int next_leaf8(const BvhView &bvh, unsigned &cur, ShortStack<kShort> &st, V3 o, V3 inv,
-                                          float tmin, float tmax, unsigned oct, int (&lk)[8], bool &fresh) {
+__device__ __forceinline__ int next_leaf8(const BvhView &bvh, unsigned &cur, ShortStack<kShort> &st, unsigned *lm, V3 o,
+                                          V3 inv, float tmin, float tmax, unsigned oct, int (&lk)[8], bool &fresh) {
     while (true) {
         unsigned m = cur & 0xffu;
         if (m == 0) {
             if (st.empty()) return 0;
-            cur = st.pop();
+            cur = st.pop(lm);
             m = cur & 0xffu;
             fresh = false;
         }
@@ -120,7 +120,7 @@ __device__ __forceinline__ int next_leaf8(const BvhView &bvh, unsigned &cur, Sho
         const int link = (kRegLinks && fresh) ? select_link(lk, k ^ oct)
                                               : __ldg(bvh.wlinks + 8 * (size_t)(cur >> 8) + (k ^ oct));
         if (link < 0) return link;
-        if (cur & 0xffu) st.push(cur);
+        if (cur & 0xffu) st.push(cur, lm);
         if (kRegLinks) {
             load_links8(bvh.wlinks, link, lk);
             fresh = true;
@@ -142,11 +142,12 @@ __device__ __forceinline__ Hit closest_hit8(const BvhView &bvh, ShortStack<kShor
     const V3 inv = v3(rrcp(d.x), rrcp(d.y), rrcp(d.z));
     const unsigned oct = ray_octant(d);
     st.reset();
+    unsigned lm[ShortStack<kShort>::kLocal];
     unsigned cur = visit8(bvh.wnodes, 0, o, inv, tmin, hit.t, oct);
     int lk[8];
     bool fresh = false;
     while (true) {
-        const int leaf = next_leaf8<kShort>(bvh, cur, st, o, inv, tmin, hit.t, oct, lk, fresh);
+        const int leaf = next_leaf8<kShort>(bvh, cur, st, lm, o, inv, tmin, hit.t, oct, lk, fresh);
         if (leaf == 0) break;
         const int code = ~leaf;
         const int first = code >> 4, count = code & 15;

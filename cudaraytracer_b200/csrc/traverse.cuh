@@ -60,6 +60,7 @@ __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
     hit.slot = -1;
     hit.b1 = hit.b2 = 0.f;
     int link = kSentinel;
+    unsigned lm[Stack::kLocal];
     st.reset();
 
     auto start = [&](int k) {
@@ -108,14 +109,14 @@ __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
                     bad = true;
                     break;
                 }
-                st.push((unsigned)far);
+                st.push((unsigned)far, lm);
                 link = near;
             } else if (h0) {
                 link = n3.x;
             } else if (h1) {
                 link = n3.y;
             } else {
-                link = st.empty() ? kSentinel : (int)st.pop();
+                link = st.empty() ? kSentinel : (int)st.pop(lm);
             }
         }
         bool finished = link == kSentinel;
@@ -143,7 +144,7 @@ __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
                 }
             }
             if (!finished) {
-                link = st.empty() ? kSentinel : (int)st.pop();
+                link = st.empty() ? kSentinel : (int)st.pop(lm);
                 finished = link == kSentinel;
             }
         }
@@ -180,6 +181,7 @@ __device__ __forceinline__ void trace_dynamic_spec(Job &job, int n, Stack &st) {
     hit.slot = -1;
     hit.b1 = hit.b2 = 0.f;
     int link = kSentinel;
+    unsigned lm[Stack::kLocal];
     st.reset();
 
     while (true) {
@@ -227,19 +229,19 @@ __device__ __forceinline__ void trace_dynamic_spec(Job &job, int n, Stack &st) {
                         bad = true;
                         break;
                     }
-                    st.push((unsigned)far);
+                    st.push((unsigned)far, lm);
                     link = near;
                 } else if (h0) {
                     link = n3.x;
                 } else if (h1) {
                     link = n3.y;
                 } else {
-                    link = st.empty() ? kSentinel : (int)st.pop();
+                    link = st.empty() ? kSentinel : (int)st.pop(lm);
                 }
             }
             if (link < 0 && link != kSentinel && pending == 0) {
                 pending = link;
-                link = st.empty() ? kSentinel : (int)st.pop();
+                link = st.empty() ? kSentinel : (int)st.pop(lm);
             }
             // go on while some lane of the warp still has no leaf to test
             // (lanes holding a second leaf in `link`, or done, idle meanwhile)
@@ -309,6 +311,7 @@ __device__ __forceinline__ void trace_dynamic8(Job &job, int n, unsigned *s_stac
     st.sp = 0;
     int lk[8];
     bool fresh = false;
+    unsigned lm[ShortStack<kShort>::kLocal];
 
     while (true) {
         const unsigned idle = __ballot_sync(0xffffffffu, idx < 0);
@@ -334,7 +337,7 @@ __device__ __forceinline__ void trace_dynamic8(Job &job, int n, unsigned *s_stac
         }
         if (__ballot_sync(0xffffffffu, idx >= 0) == 0) break;
         if (idx < 0) continue;
-        const int leaf = next_leaf8<kShort, kRegLinks>(bvh, cur, st, o, inv, tmin, hit.t, oct, lk, fresh);
+        const int leaf = next_leaf8<kShort, kRegLinks>(bvh, cur, st, lm, o, inv, tmin, hit.t, oct, lk, fresh);
         bool finished = leaf == 0;
         if (!finished) {
             const int code = ~leaf;
