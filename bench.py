@@ -592,8 +592,8 @@ def denoise_leg(ctx, train_steps=1500):
     """Learned denoiser against SVGF (the learned-denoiser workload, at
     256x256 instead of 1920x1080 and 16-frame instead of 60-frame
     sequences so the 4096-spp references fit the bench): the KPCN is
-    trained on the GPU on 128 views of seeded Cornell variants (scene seeds
-    100-163, two views each, 1-16 spp inputs, 4096-spp references) for
+    trained on the GPU on 64 views of seeded Cornell variants (scene seeds
+    100-163, one view each, 1-16 spp inputs, 4096-spp references) for
     1500 Adam steps of 8 random 128x128 crops. Test: one 16-frame orbit
     sequence (1.5 deg per frame) per unseen scene (seeds 200-207), relMSE
     of every frame against its 4096-spp reference for raw and KPCN at 1-32
@@ -613,7 +613,7 @@ def denoise_leg(ctx, train_steps=1500):
 
     res = 256
     t0 = time.perf_counter()
-    data = D.build_dataset(ctx, range(100, 164), 2, res, res, [1, 2, 4, 8, 16], 4096, seed=0)
+    data = D.build_dataset(ctx, range(100, 164), 1, res, res, [1, 2, 4, 8, 16], 4096, seed=0)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     net = Kpcn(ctx, seed=0)
@@ -644,7 +644,7 @@ def denoise_leg(ctx, train_steps=1500):
         sc.close()
     px = train_steps * 8 * 128 * 128
     net.close()
-    return {"workload": f"Cornell variants at {res}x{res}: train seeds 100-163 (2 views each, 1-16 spp, 4096-spp refs); "
+    return {"workload": f"Cornell variants at {res}x{res}: train seeds 100-163 (1 view each, 1-16 spp, 4096-spp refs); "
                         f"test: {frames}-frame orbit sequences of seeds 200-207, 4096-spp refs per frame",
             "dataset_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2), "eval_s": round(t3 - t2, 2),
             "train_steps": train_steps,
