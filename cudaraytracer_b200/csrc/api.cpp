@@ -107,8 +107,8 @@ crt_status crt_scene_from_triangles(crt_ctx *ctx, const float *tri_verts, int64_
             size_t bytes = (size_t)n_tris * 9 * sizeof(float);
             CRT_CUDA(cudaMalloc(&s->d_verts, bytes));
             CRT_CUDA(cudaMemcpyAsync(s->d_verts, tri_verts, bytes, cudaMemcpyHostToDevice, ctx->stream));
-            build_bvh(s->d_verts, (int)n_tris, ctx->stream, s->bvh);
             s->bvh.err = ctx->d_err;
+            build_bvh(s->d_verts, (int)n_tris, ctx->stream, s->bvh);
         } catch (...) {
             delete s;
             throw;
@@ -264,8 +264,8 @@ void finish_scene(crt_scene *s) {
     CRT_CHECK(n < (size_t)(1 << 27) - 1, CRT_ERR_CAPACITY, "too many triangles");
     CRT_CUDA(cudaMalloc(&s->d_verts, h.verts.size() * sizeof(float)));
     CRT_CUDA(cudaMemcpy(s->d_verts, h.verts.data(), h.verts.size() * sizeof(float), cudaMemcpyHostToDevice));
-    build_bvh(s->d_verts, (int)n, s->ctx->stream, s->bvh);
     s->bvh.err = s->ctx->d_err;
+    build_bvh(s->d_verts, (int)n, s->ctx->stream, s->bvh);
     upload_render_data(h, s->rd);
     s->rp.width = h.width;
     s->rp.height = h.height;

@@ -27,6 +27,12 @@ constexpr int kStackSize = 64;
 constexpr int kSentinel = INT_MIN;  // never a valid link: first < 2^27 - 1
 constexpr float kTriTMax = 1e8f;    // Triangle::IsIntersect default tMax
 
+// Grid of the 16-bit quantised nodes of one scene (bvh16.cuh): per axis
+// the scale s = 2^e and the biased origin p'.
+struct QuantGrid {
+    float s[3], p[3];
+};
+
 struct BvhView {
     const float4 *nodes;   // 4 float4 per node
     const float4 *tris;    // 3 float4 per triangle
@@ -35,6 +41,8 @@ struct BvhView {
     const int *wlinks;     // 8 child links per wide node
     int num_nodes;         // binary nodes (bound of interior links)
     int *err;              // device error word (kErrTraversalBounds), or null
+    const float4 *cnodes;  // the binary nodes with 16-bit quantised boxes, 2 float4 each (bvh16.cuh)
+    QuantGrid grid;
 };
 
 #ifdef __CUDACC__
@@ -169,7 +177,37 @@ struct ShortStack {
     }
 };
 
-template <bool kEarlyExit, bool kCull = true, class Stack>
+// --- 16-bit quantised nodes (layout and grid: bvh16.cuh) ---
+
+// 2^23 + the low (kHi = 0) or high (kHi = 1) 16 bits of w, as a float.
+template <int kHi>
+__device__ __forceinline__ float q16_biased(unsigned w) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, kHi ? 0x7432u : 0x7410u));
+}
+
+// One 32 B quantised node: the two child boxes decoded to floats and the
+// links, in the float node's register layout (n0, n1: x/y bounds of child
+// 0 and 1; n2: z bounds of both; n3: links).
+__device__ __forceinline__ void load_node16(const float4 *cn, int node, const QuantGrid &g, float4 &n0, float4 &n1,
+                                            float4 &n2, int4 &n3) {
+    unsigned w[8];
+    asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+        : "l"(cn + 2 * (size_t)node));
+    // child c, component j (0-5: lo x y z, hi x y z) is index 6c + j
+#define CRT_Q16(I) q16_biased<(I)&1>(w[(I) >> 1])
+    n0 = make_float4(fmaf(CRT_Q16(0), g.s[0], g.p[0]), fmaf(CRT_Q16(3), g.s[0], g.p[0]),
+                     fmaf(CRT_Q16(1), g.s[1], g.p[1]), fmaf(CRT_Q16(4), g.s[1], g.p[1]));
+    n1 = make_float4(fmaf(CRT_Q16(6), g.s[0], g.p[0]), fmaf(CRT_Q16(9), g.s[0], g.p[0]),
+                     fmaf(CRT_Q16(7), g.s[1], g.p[1]), fmaf(CRT_Q16(10), g.s[1], g.p[1]));
+    n2 = make_float4(fmaf(CRT_Q16(2), g.s[2], g.p[2]), fmaf(CRT_Q16(5), g.s[2], g.p[2]),
+                     fmaf(CRT_Q16(8), g.s[2], g.p[2]), fmaf(CRT_Q16(11), g.s[2], g.p[2]));
+#undef CRT_Q16
+    n3 = make_int4((int)w[6], (int)w[7], 0, 0);
+}
+
+
+template <bool kEarlyExit, bool kCull = true, bool kQuant = false, class Stack>
 __device__ __forceinline__ Hit closest_hit_st(const BvhView &bvh, Stack &st, V3 o, V3 d, float tmin, float tmax,
                                               float t_exit = 0.f);
 
@@ -182,8 +220,9 @@ __device__ __forceinline__ Hit closest_hit(const BvhView &bvh, V3 o, V3 d, float
 }
 
 // The ordered traversal over a given stack (far child pushed, near child
-// descended first; the empty stack ends it).
-template <bool kEarlyExit, bool kCull, class Stack>
+// descended first; the empty stack ends it), over the float nodes or, with
+// kQuant, their 16-bit quantised copy.
+template <bool kEarlyExit, bool kCull, bool kQuant, class Stack>
 __device__ __forceinline__ Hit closest_hit_st(const BvhView &bvh, Stack &st, V3 o, V3 d, float tmin, float tmax,
                                               float t_exit) {
     Hit hit;
@@ -201,9 +240,17 @@ __device__ __forceinline__ Hit closest_hit_st(const BvhView &bvh, Stack &st, V3 
                 report_traversal_bounds(bvh);
                 return hit;
             }
-            const float4 *n = bvh.nodes + 4 * (size_t)link;
-            float4 n0 = __ldg(n + 0), n1 = __ldg(n + 1), n2 = __ldg(n + 2);
-            int4 n3 = __ldg(reinterpret_cast<const int4 *>(n + 3));
+            float4 n0, n1, n2;
+            int4 n3;
+            if (kQuant) {
+                load_node16(bvh.cnodes, link, bvh.grid, n0, n1, n2, n3);
+            } else {
+                const float4 *n = bvh.nodes + 4 * (size_t)link;
+                n0 = __ldg(n + 0);
+                n1 = __ldg(n + 1);
+                n2 = __ldg(n + 2);
+                n3 = __ldg(reinterpret_cast<const int4 *>(n + 3));
+            }
             float t0, t1;
             bool h0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, tmin, hit.t, t0);
             bool h1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, tmin, hit.t, t1);

@@ -788,6 +788,9 @@ void build_bvh(const float *d_verts, int n, cudaStream_t stream, BvhBuffers &out
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     out.num_tris = n;
+    // the 16-bit quantised copy of the nodes (bvh16.cuh), one kernel
+    build_bvh16(out, out.err, stream);
+    CRT_CUDA(cudaStreamSynchronize(stream));
     // The 8-wide quantised tree is built only on request (CRT_BVH8=1): its
     // traversal measured slower than the binary one on the icosphere field.
     const char *w8 = getenv("CRT_BVH8");
@@ -804,6 +807,7 @@ void free_bvh(BvhBuffers &b) {
     if (b.slot_of_prim) cudaFree(b.slot_of_prim);
     if (b.wnodes) cudaFree(b.wnodes);
     if (b.wlinks) cudaFree(b.wlinks);
+    if (b.cnodes) cudaFree(b.cnodes);
     b = BvhBuffers();
 }
 

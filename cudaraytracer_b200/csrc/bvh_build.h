@@ -2,6 +2,7 @@
 #pragma once
 #include "bvh.cuh"
 #include "bvh8.cuh"
+#include "bvh16.cuh"
 
 namespace crt {
 
@@ -22,7 +23,11 @@ struct BvhBuffers {
     int wide_depth = 0;
     float wide_build_ms = 0.f;
     int *err = nullptr;  // the owning context's device error word
-    BvhView view() const { return BvhView{nodes, tris, num_tris, wnodes, wlinks, (int)num_nodes, err}; }
+    float4 *cnodes = nullptr;  // 16-bit quantised copy of `nodes` (bvh16.cuh)
+    QuantGrid grid{};
+    BvhView view() const {
+        return BvhView{nodes, tris, num_tris, wnodes, wlinks, (int)num_nodes, err, cnodes, grid};
+    }
 };
 
 // Builds the BVH of n triangles given as n x 9 floats (v0, v1, v2) on the

@@ -86,6 +86,22 @@ __global__ void __launch_bounds__(kTraceBlock, kMinBlocks) k_trace_shadow_o(BvhV
     trace_dynamic<true>(job, n);
 }
 
+// The binary traversal over the 16-bit quantised nodes (bvh16.cuh), local
+// stack.
+__global__ void __launch_bounds__(kTraceBlock, 8) k_trace_closest_q(BvhView bvh, const float4 *__restrict__ rays, int n,
+                                                                 float4 *__restrict__ hits) {
+    ClosestJob job{bvh, rays, hits};
+    LocalStack st;
+    trace_dynamic_st<true, true>(job, n, st);
+}
+
+__global__ void __launch_bounds__(kTraceBlock, 8) k_trace_shadow_q(BvhView bvh, const float4 *__restrict__ q, int n,
+                                                                uint8_t *__restrict__ occ) {
+    ShadowJob job{bvh, q, occ, {}};
+    LocalStack st;
+    trace_dynamic_st<true, true>(job, n, st);
+}
+
 // The binary traversal with postponed leaves (traverse.cuh), local stack.
 __global__ void __launch_bounds__(kTraceBlock) k_trace_closest_p(BvhView bvh, const float4 *__restrict__ rays, int n,
                                                                  float4 *__restrict__ hits) {
@@ -103,7 +119,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow_p(BvhView bvh, con
 
 // The binary traversal with the per-lane short stack in shared memory
 // (kShort entries per lane, kShort x 128 words per block).
-template <int kShort>
+template <int kShort, bool kQuant>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_closest_s(BvhView bvh, const float4 *__restrict__ rays, int n,
                                                                  float4 *__restrict__ hits) {
     __shared__ unsigned s_stack[kShort * kTraceBlock];
@@ -111,10 +127,10 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_closest_s(BvhView bvh, co
     st.col = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     ClosestJob job{bvh, rays, hits};
-    trace_dynamic_st<true>(job, n, st);
+    trace_dynamic_st<true, kQuant>(job, n, st);
 }
 
-template <int kShort>
+template <int kShort, bool kQuant>
 __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow_s(BvhView bvh, const float4 *__restrict__ q, int n,
                                                                 uint8_t *__restrict__ occ) {
     __shared__ unsigned s_stack[kShort * kTraceBlock];
@@ -122,7 +138,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow_s(BvhView bvh, con
     st.col = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     ShadowJob job{bvh, q, occ, {}};
-    trace_dynamic_st<true>(job, n, st);
+    trace_dynamic_st<true, kQuant>(job, n, st);
 }
 
 // The same over the 8-wide quantised tree with the shared-memory short
@@ -162,7 +178,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8r(BvhView bvh, con
 // Traversal variant of the trace kernels (CRT_TRAVERSAL overrides the
 // default kTraceVariant): 2 = binary tree, stack in local memory
 // (210 / 212: the same capped at 51 / 42 registers for 10 / 12 blocks per SM;
-// 3: with postponed leaves);
+// 3: with postponed leaves; 4 / 416: over the 16-bit quantised nodes with
+// the stack in local / shared memory);
 // 28 / 216 = binary tree, top 8 / 16 stack entries per lane in shared
 // memory; 8 / 82 = 8-wide quantised tree (built only with CRT_BVH8=1),
 // 16 / 8 shared-memory entries; 83 = the same as 8 with the visited node's
@@ -187,7 +204,14 @@ void launch_trace_closest(const BvhView &bvh, const float4 *d_rays, int64_t n, f
     CRT_CHECK(n < (int64_t)1 << 31, CRT_ERR_CAPACITY, "trace batch larger than 2^31 rays");
     int v = traversal_variant();
     if ((v == 8 || v == 82 || v == 83) && !bvh.wnodes) v = 2;
-    if (v == 3)
+    if ((v == 4 || v == 416) && !bvh.cnodes) v = 2;
+    if (v == 4)
+        k_trace_closest_q<<<trace_grid((const void *)k_trace_closest_q, n), kTraceBlock, 0, s>>>(bvh, d_rays, (int)n,
+                                                                                                d_hits);
+    else if (v == 416)
+        k_trace_closest_s<16, true><<<trace_grid((const void *)k_trace_closest_s<16, true>, n), kTraceBlock, 0, s>>>(
+            bvh, d_rays, (int)n, d_hits);
+    else if (v == 3)
         k_trace_closest_p<<<trace_grid((const void *)k_trace_closest_p, n), kTraceBlock, 0, s>>>(bvh, d_rays, (int)n,
                                                                                                 d_hits);
     else if (v == 210)
@@ -197,10 +221,10 @@ void launch_trace_closest(const BvhView &bvh, const float4 *d_rays, int64_t n, f
         k_trace_closest_o<12><<<trace_grid((const void *)k_trace_closest_o<12>, n), kTraceBlock, 0, s>>>(
             bvh, d_rays, (int)n, d_hits);
     else if (v == 28)
-        k_trace_closest_s<8><<<trace_grid((const void *)k_trace_closest_s<8>, n), kTraceBlock, 0, s>>>(
+        k_trace_closest_s<8, false><<<trace_grid((const void *)k_trace_closest_s<8, false>, n), kTraceBlock, 0, s>>>(
             bvh, d_rays, (int)n, d_hits);
     else if (v == 216)
-        k_trace_closest_s<16><<<trace_grid((const void *)k_trace_closest_s<16>, n), kTraceBlock, 0, s>>>(
+        k_trace_closest_s<16, false><<<trace_grid((const void *)k_trace_closest_s<16, false>, n), kTraceBlock, 0, s>>>(
             bvh, d_rays, (int)n, d_hits);
     else if (v == 8)
         k_trace_closest8<16><<<trace_grid((const void *)k_trace_closest8<16>, n), kTraceBlock, 0, s>>>(
@@ -223,7 +247,13 @@ void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_
     const float4 *q = reinterpret_cast<const float4 *>(d_q);
     int v = traversal_variant();
     if ((v == 8 || v == 82 || v == 83) && !bvh.wnodes) v = 2;
-    if (v == 3)
+    if ((v == 4 || v == 416) && !bvh.cnodes) v = 2;
+    if (v == 4)
+        k_trace_shadow_q<<<trace_grid((const void *)k_trace_shadow_q, n), kTraceBlock, 0, s>>>(bvh, q, (int)n, d_occ);
+    else if (v == 416)
+        k_trace_shadow_s<16, true><<<trace_grid((const void *)k_trace_shadow_s<16, true>, n), kTraceBlock, 0, s>>>(
+            bvh, q, (int)n, d_occ);
+    else if (v == 3)
         k_trace_shadow_p<<<trace_grid((const void *)k_trace_shadow_p, n), kTraceBlock, 0, s>>>(bvh, q, (int)n, d_occ);
     else if (v == 210)
         k_trace_shadow_o<10><<<trace_grid((const void *)k_trace_shadow_o<10>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
@@ -232,10 +262,10 @@ void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_
         k_trace_shadow_o<12><<<trace_grid((const void *)k_trace_shadow_o<12>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
                                                                                                     d_occ);
     else if (v == 28)
-        k_trace_shadow_s<8><<<trace_grid((const void *)k_trace_shadow_s<8>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
+        k_trace_shadow_s<8, false><<<trace_grid((const void *)k_trace_shadow_s<8, false>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
                                                                                                   d_occ);
     else if (v == 216)
-        k_trace_shadow_s<16><<<trace_grid((const void *)k_trace_shadow_s<16>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
+        k_trace_shadow_s<16, false><<<trace_grid((const void *)k_trace_shadow_s<16, false>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
                                                                                                     d_occ);
     else if (v == 8)
         k_trace_shadow8<16><<<trace_grid((const void *)k_trace_shadow8<16>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,

@@ -30,18 +30,19 @@ namespace crt {
 
 #ifdef __CUDACC__
 
-template <bool kCull, class Job, class Stack>
+template <bool kCull, bool kQuant, class Job, class Stack>
 __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st);
 
-// The stack in local memory.
+// The stack in local memory, float nodes.
 template <bool kCull, class Job>
 __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
     LocalStack st;
-    trace_dynamic_st<kCull>(job, n, st);
+    trace_dynamic_st<kCull, false>(job, n, st);
 }
 
-// Over a given per-lane stack (LocalStack or ShortStack, bvh.cuh).
-template <bool kCull, class Job, class Stack>
+// Over a given per-lane stack (LocalStack or ShortStack, bvh.cuh), and over
+// the float nodes or (kQuant) their 16-bit quantised copy (bvh16.cuh).
+template <bool kCull, bool kQuant, class Job, class Stack>
 __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
     const unsigned lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -52,7 +53,7 @@ __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
     int cleft = (int)((w + 1) * n / warps) - cbase;
     // per-lane ray state
     int idx = -1;
-    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr, 0, nullptr};
+    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr, 0, nullptr, nullptr, {}};
     V3 o{0.f, 0.f, 0.f}, d{0.f, 0.f, 0.f}, inv{0.f, 0.f, 0.f};
     float tmin = 0.f, t_exit = 0.f;
     Hit hit;
@@ -95,7 +96,10 @@ __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
             }
             float4 n0, n1, n2;
             int4 n3;
-            load_node(bvh.nodes + 4 * (size_t)link, n0, n1, n2, n3);
+            if (kQuant)
+                load_node16(bvh.cnodes, link, bvh.grid, n0, n1, n2, n3);
+            else
+                load_node(bvh.nodes + 4 * (size_t)link, n0, n1, n2, n3);
             float t0, t1;
             bool h0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, tmin, hit.t, t0);
             bool h1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, tmin, hit.t, t1);
@@ -173,7 +177,7 @@ __device__ __forceinline__ void trace_dynamic_spec(Job &job, int n, Stack &st) {
     int cbase = (int)(w * n / warps);
     int cleft = (int)((w + 1) * n / warps) - cbase;
     int idx = -1;
-    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr, 0, nullptr};
+    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr, 0, nullptr, nullptr, {}};
     V3 o{0.f, 0.f, 0.f}, d{0.f, 0.f, 0.f}, inv{0.f, 0.f, 0.f};
     float tmin = 0.f, t_exit = 0.f;
     Hit hit;
@@ -297,7 +301,7 @@ __device__ __forceinline__ void trace_dynamic8(Job &job, int n, unsigned *s_stac
     int cbase = (int)(w * n / warps);
     int cleft = (int)((w + 1) * n / warps) - cbase;
     int idx = -1;
-    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr, 0, nullptr};
+    BvhView bvh{nullptr, nullptr, 0, nullptr, nullptr, 0, nullptr, nullptr, {}};
     V3 o{0.f, 0.f, 0.f}, d{0.f, 0.f, 0.f}, inv{0.f, 0.f, 0.f};
     float tmin = 0.f, t_exit = 0.f;
     unsigned oct = 0, cur = 0;

@@ -149,19 +149,22 @@ def test_empty_batches_and_errors(crt_ctx, cornell_tris):
         Scene.from_triangles(crt_ctx, np.zeros((0, 9), np.float32))
 
 
-@pytest.mark.parametrize("variant", ["28", "216", "210", "212", "3", "8", "82", "83"])
+@pytest.mark.parametrize("variant", ["28", "216", "210", "212", "3", "4", "416", "8", "82", "83"])
 def test_traversal_variants_agree(crt_ctx, ico_tris, variant, monkeypatch):
     """Every traversal variant of the trace kernels (binary tree with the
-    top of each lane's stack in shared memory, 8 or 16 entries; the 8-wide
-    quantised tree, built on request) returns the hit records and shadow
-    answers of the binary traversal with its stack in local memory, ties
-    aside, and records no out-of-range index."""
+    top of each lane's stack in shared memory, 8 or 16 entries; capped
+    registers; postponed leaves; the nodes with 16-bit quantised boxes; the
+    8-wide quantised tree, built on request) returns the hit records and
+    shadow answers of the binary traversal with its stack in local memory,
+    ties aside; no quantised box fails to contain its child and no traversal
+    records an out-of-range index."""
     import os
 
     rays = scenes.random_rays(ico_tris, 1 << 18, seed=9)
     q = scenes.random_shadow_queries(ico_tris, 1 << 18, seed=10)
     monkeypatch.setenv("CRT_BVH8", "1")
     sc = Scene.from_triangles(crt_ctx, ico_tris)
+    crt_ctx.check_device_errors()  # the quantised copy of the nodes contains every child box
     assert sc.info()["num_wide_nodes"] > 0
     monkeypatch.setenv("CRT_TRAVERSAL", "2")
     base_h, base_o = sc.trace_closest(rays), sc.trace_shadow(q)
