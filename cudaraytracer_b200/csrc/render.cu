@@ -370,7 +370,7 @@ __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *co
 // Extend: closest hit of every live path (TraceRay, renderer.cuh:124-130:
 // tMin 0, closest starts at 1e8). Also clears the next bounce's counters.
 __global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters,
-                                                int out_idx, bool smem_stack) {
+                                                int out_idx, int mode) {
     __shared__ unsigned s_stack[kStageShort * kStageMaxBlock];
     ShortStack<kStageShort> st;
     st.col = s_stack + threadIdx.x;
@@ -385,8 +385,7 @@ __global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const 
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = q.p[0][i], b = q.p[1][i];
         const V3 o{a.x, a.y, a.z}, d{b.x, b.y, b.z};
-        Hit h = smem_stack ? closest_hit_st<false, true>(bvh, st, o, d, 0.f, kTriTMax)
-                           : closest_hit<false>(bvh, o, d, 0.f, kTriTMax);
+        Hit h = stage_closest<false>(bvh, st, mode, o, d, 0.f, kTriTMax);
         hits[i] = make_float4(h.t, __int_as_float(h.slot), h.b1, h.b2);
     }
 }
@@ -447,7 +446,7 @@ __global__ void __launch_bounds__(256) k_shade(SceneView s, StepParams sp, Queue
 // contribution joins its path's direct or indirect radiance; a path that
 // already terminated is then added to its pixel.
 __global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueView qout,
-                                                float4 *term0, float4 *term1, AccumView acc, bool smem_stack) {
+                                                float4 *term0, float4 *term1, AccumView acc, int mode) {
     __shared__ unsigned s_stack[kStageShort * kStageMaxBlock];
     ShortStack<kStageShort> st;
     st.col = s_stack + threadIdx.x;
@@ -459,7 +458,7 @@ __global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, cons
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = sh.r[0][i], b = sh.r[1][i], c = sh.r[2][i], d = sh.r[3][i];
         const V3 hp{a.x, a.y, a.z}, hn{a.w, b.x, b.y}, lp{b.z, b.w, c.x}, ln{c.y, c.z, c.w};
-        const bool vis = smem_stack ? visible_st(bvh, st, hp, hn, lp, ln) : visible(bvh, hp, hn, lp, ln);
+        const bool vis = stage_visible(bvh, st, mode, hp, hn, lp, ln);
         uint32_t target = __float_as_uint(d.w);
         uint32_t idx = target & kIndexMask;
         bool direct = (target & kDirectBit) != 0;
@@ -494,9 +493,15 @@ __global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, cons
     }
 }
 
-bool stage_smem_stack() {
-    const char *e = getenv("CRT_STAGE_STACK");
-    return e ? e[0] != 'l' : kStageSmemStackDefault;
+int stage_traversal() {
+    const char *e = getenv("CRT_STAGE_TRAVERSAL");
+    if (!e) return kStageTraversalDefault;
+    const std::string v(e);
+    if (v == "local") return kStageLocal;
+    if (v == "shared") return kStageShared;
+    if (v == "local-quant") return kStageLocalQuant;
+    if (v == "shared-quant") return kStageSharedQuant;
+    return kStageTraversalDefault;
 }
 
 int persistent_grid(const void *kernel, int block) {
@@ -535,7 +540,7 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
         for (int k = 0; k < 5; ++k) q[j].p[k] = wf.q[j][k];
     ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
     const int blk = rp.block();
-    const bool smem = stage_smem_stack();
+    const int smem = stage_traversal();
     const int g_ext = persistent_grid((const void *)k_extend, blk);
     const int g_sh = persistent_grid((const void *)k_shade, blk);
     const int g_sd = persistent_grid((const void *)k_shadow, blk);

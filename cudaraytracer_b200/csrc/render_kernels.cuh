@@ -2,6 +2,7 @@
 // kernel parameter blocks and the stage kernels (defined in render.cu).
 #pragma once
 #include "render.h"
+#include "trace.cuh"
 
 namespace crt {
 
@@ -42,11 +43,11 @@ struct ShadowView {
 
 __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *counters);
 __global__ void k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters, int out_idx,
-                         bool smem_stack);
+                         int mode);
 __global__ void k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits, const int *n_in, QueueView qout,
                         int *counters, int out_idx, ShadowView sh, float4 *term0, float4 *term1, AccumView acc);
 __global__ void k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueView qout, float4 *term0,
-                         float4 *term1, AccumView acc, bool smem_stack);
+                         float4 *term1, AccumView acc, int mode);
 
 // Blocks per grid for a persistent launch of `kernel` (all SMs at full
 // occupancy).
@@ -57,11 +58,41 @@ int persistent_grid(const void *kernel, int block);
 // largest block those stages are launched with.
 constexpr int kStageShort = 8;
 constexpr int kStageMaxBlock = 256;
-constexpr bool kStageSmemStackDefault = true;
+// How the extend and shadow stages traverse: the top of each lane's stack
+// in shared memory (ShortStack) or the whole stack in local memory
+// (LocalStack), over the float nodes or their 16-bit quantised copy.
+enum StageTraversal : int {
+    kStageLocal = 0,
+    kStageShared = 1,
+    kStageLocalQuant = 2,
+    kStageSharedQuant = 3,
+};
+constexpr int kStageTraversalDefault = kStageShared;
 
-// Whether the extend and shadow stages keep the top of each lane's
-// traversal stack in shared memory (ShortStack) or the whole stack in
-// local memory (LocalStack); CRT_STAGE_STACK=local selects the latter.
-bool stage_smem_stack();
+// The mode for the next launches: kStageTraversalDefault, or the one named
+// by CRT_STAGE_TRAVERSAL (local, shared, local-quant, shared-quant).
+int stage_traversal();
+
+#ifdef __CUDACC__
+// Closest hit and Light::Visible in the given mode (`sst` is the lane's
+// shared-memory stack column).
+template <bool kEarlyExit>
+__device__ __forceinline__ Hit stage_closest(const BvhView &bvh, ShortStack<kStageShort> &sst, int mode, V3 o, V3 d,
+                                             float tmin, float tmax, float t_exit = 0.f) {
+    if (mode == kStageShared) return closest_hit_st<kEarlyExit, true, false>(bvh, sst, o, d, tmin, tmax, t_exit);
+    if (mode == kStageSharedQuant) return closest_hit_st<kEarlyExit, true, true>(bvh, sst, o, d, tmin, tmax, t_exit);
+    LocalStack lst;
+    if (mode == kStageLocalQuant) return closest_hit_st<kEarlyExit, true, true>(bvh, lst, o, d, tmin, tmax, t_exit);
+    return closest_hit_st<kEarlyExit, true, false>(bvh, lst, o, d, tmin, tmax, t_exit);
+}
+
+__device__ __forceinline__ bool stage_visible(const BvhView &bvh, ShortStack<kStageShort> &sst, int mode, V3 hp, V3 hn,
+                                              V3 lp, V3 ln) {
+    ShadowRay r;
+    shadow_ray_init(r, hp, hn, lp, ln);
+    const Hit hit = stage_closest<true>(bvh, sst, mode, r.o, r.dir, 1e-6f, 1e8f, r.t_exit);
+    return shadow_ray_visible(r, bvh, hit);
+}
+#endif
 
 }  // namespace crt

@@ -87,7 +87,7 @@ __global__ void ks_raygen(const ReqDesc *reqs, const Segment *segs, int nseg, in
 }
 
 __global__ void __launch_bounds__(128) ks_extend(const SceneView *scenes, QueueView q, const int *n_in, float4 *hits,
-                                                 int *counters, int out_idx, bool smem_stack) {
+                                                 int *counters, int out_idx, int mode) {
     __shared__ unsigned s_stack[kStageShort * 128];
     ShortStack<kStageShort> st;
     st.col = s_stack + threadIdx.x;
@@ -102,8 +102,7 @@ __global__ void __launch_bounds__(128) ks_extend(const SceneView *scenes, QueueV
         float4 a = q.p[0][i], b = q.p[1][i];
         const BvhView bvh = scenes[path_tag(q, i) >> kSlotBits].bvh;
         const V3 o{a.x, a.y, a.z}, d{b.x, b.y, b.z};
-        Hit h = smem_stack ? closest_hit_st<false, true>(bvh, st, o, d, 0.f, kTriTMax)
-                           : closest_hit<false>(bvh, o, d, 0.f, kTriTMax);
+        Hit h = stage_closest<false>(bvh, st, mode, o, d, 0.f, kTriTMax);
         hits[i] = make_float4(h.t, __int_as_float(h.slot), h.b1, h.b2);
     }
 }
@@ -179,7 +178,7 @@ __global__ void __launch_bounds__(128) ks_shade(const SceneView *scenes, const R
 // it belongs to; then as k_shadow in render.cu.
 __global__ void __launch_bounds__(128) ks_shadow(const SceneView *scenes, const ReqDesc *reqs, ShadowView sh,
                                                  const int *counters, QueueView qout, float4 *term0, float4 *term1,
-                                                 bool smem_stack) {
+                                                 int mode) {
     __shared__ unsigned s_stack[kStageShort * 128];
     ShortStack<kStageShort> st;
     st.col = s_stack + threadIdx.x;
@@ -194,7 +193,7 @@ __global__ void __launch_bounds__(128) ks_shadow(const SceneView *scenes, const 
         float4 a = sh.r[0][i], b = sh.r[1][i], c = sh.r[2][i];
         const BvhView bvh = scenes[tag >> kSlotBits].bvh;
         const V3 hp{a.x, a.y, a.z}, hn{a.w, b.x, b.y}, lp{b.z, b.w, c.x}, ln{c.y, c.z, c.w};
-        const bool vis = smem_stack ? visible_st(bvh, st, hp, hn, lp, ln) : visible(bvh, hp, hn, lp, ln);
+        const bool vis = stage_visible(bvh, st, mode, hp, hn, lp, ln);
         bool direct = (target & kDirectBit) != 0;
         V3 C{d.x, d.y, d.z};
         if (term) {
@@ -421,7 +420,7 @@ struct crt_server {
             for (int c = 0; c < 5; ++c) q[j].p[c] = wf.q[j][c];
         ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
         ks_raygen<<<(n + 255) / 256, 256, 0, stream>>>(d_reqs, ds, nseg, n, q[0], wf.counters);
-        const bool smem = stage_smem_stack();
+        const int smem = stage_traversal();
         for (int b = 0; b < max_b; ++b) {
             const int in = b & 1, out = 1 - in;
             ks_extend<<<g_ext, 128, 0, stream>>>(d_scenes, q[in], wf.counters + in, wf.hits, wf.counters, out, smem);

@@ -62,15 +62,6 @@ __device__ __forceinline__ bool visible(const BvhView &bvh, V3 hp, V3 hn, V3 lp,
     return shadow_ray_visible(r, bvh, hit);
 }
 
-// visible() over a given per-lane stack (LocalStack or ShortStack).
-template <class Stack>
-__device__ __forceinline__ bool visible_st(const BvhView &bvh, Stack &st, V3 hp, V3 hn, V3 lp, V3 ln) {
-    ShadowRay r;
-    shadow_ray_init(r, hp, hn, lp, ln);
-    Hit hit = closest_hit_st<true, true>(bvh, st, r.o, r.dir, 1e-6f, 1e8f, r.t_exit);
-    return shadow_ray_visible(r, bvh, hit);
-}
-
 // visible() over the 8-wide tree with a short stack (bvh8.cuh).
 template <int kShort>
 __device__ __forceinline__ bool visible8(const BvhView &bvh, ShortStack<kShort> &st, V3 hp, V3 hn, V3 lp, V3 ln) {
