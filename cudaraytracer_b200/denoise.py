@@ -366,6 +366,18 @@ def run_plain_svgf_loop(ctx, scs, reqs, width: int, height: int, spp: int = 64):
 
     states = [Svgf(ctx, width, height) for _ in scs]
     last = [None] * len(scs)
+    dev = torch.device("cuda", ctx.device)
+
+    def gbuf():
+        return {"pos_tri": torch.empty((height, width, 4), dtype=torch.float32, device=dev),
+                "normal_mat": torch.empty((height, width, 4), dtype=torch.int16, device=dev),
+                "bary_mesh": torch.empty((height, width, 4), dtype=torch.int16, device=dev),
+                "motion_depth": torch.empty((height, width, 4), dtype=torch.float32, device=dev)}
+
+    gbs = [[gbuf(), gbuf()] for _ in scs]  # current / previous G-buffer per sequence
+    d = torch.empty((height, width, 4), device=dev)
+    i = torch.empty_like(d)
+    od, oi = torch.empty_like(d), torch.empty_like(d)
     lat = []
     t0 = time.perf_counter()
     for r in reqs:
@@ -374,15 +386,22 @@ def run_plain_svgf_loop(ctx, scs, reqs, width: int, height: int, spp: int = 64):
             time.sleep(r["arrival_s"] - now)
         si = r["scene"]
         sc = scs[si]
-        d, i = render_view(sc, r["camera"], width, height, spp, r["seed"])
-        prev_cam, prev_g = last[si] if last[si] is not None else (None, None)
-        g = sc.gbuffer(prev_camera=prev_cam)
-        nd, ni = (d / spp).contiguous(), (i / spp).contiguous()
-        od, oi = torch.empty_like(nd), torch.empty_like(ni)
-        states[si].frame(g, prev_g if prev_g is not None else g, nd, ni, od, oi)
+        sc.set_render_params(width=width, height=height, seed=r["seed"])
+        c = r["camera"]
+        sc.set_camera_orbit(c["target"], c["distance"], c["theta_deg"], c["phi_deg"], c["fovy_deg"])
+        d.zero_()
+        i.zero_()
+        sc.render_device(d, i, spp)
+        prev_cam = last[si]
+        g, pg = gbs[si]
+        sc.gbuffer(prev_camera=prev_cam, out=g)
+        d.mul_(1.0 / spp)
+        i.mul_(1.0 / spp)
+        states[si].frame(g, pg if prev_cam is not None else g, d, i, od, oi)
         torch.cuda.synchronize()
         lat.append(time.perf_counter() - t0 - r["arrival_s"])
-        last[si] = (sc.camera(), g)
+        last[si] = sc.camera()
+        gbs[si] = [pg, g]
     wall = time.perf_counter() - t0
     for st in states:
         st.close()
@@ -393,8 +412,9 @@ def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: 
     """The learned pipeline, open loop: each request is submitted to the
     multi-scene server (continuous batching) at spp when it arrives; the
     requests that finish rendering in a server step get their G-buffer and
-    features and go through one batched KPCN forward together; latency =
-    completion of that forward - arrival."""
+    features (built straight from the server's accumulators into one batch)
+    and go through one batched KPCN forward together; latency = completion
+    of that forward - arrival."""
     import torch
 
     from .serve import DONE, RenderRequest, Server
@@ -407,6 +427,14 @@ def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: 
     ids = {}
     done = 0
     k = 0
+    dev = torch.device("cuda", ctx.device)
+    g = {"pos_tri": torch.empty((height, width, 4), dtype=torch.float32, device=dev),
+         "normal_mat": torch.empty((height, width, 4), dtype=torch.int16, device=dev),
+         "bary_mesh": torch.empty((height, width, 4), dtype=torch.int16, device=dev),
+         "motion_depth": torch.empty((height, width, 4), dtype=torch.float32, device=dev)}
+    feats = torch.empty((n, height, width, 16), dtype=torch.bfloat16, device=dev)
+    noisy = torch.empty((n, height, width, 4), dtype=torch.float32, device=dev)
+    outb = torch.empty((n, height, width, 4), dtype=torch.float32, device=dev)
     t0 = time.perf_counter()
     while done < n:
         now = time.perf_counter() - t0
@@ -417,30 +445,26 @@ def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: 
         nd = srv.step(wait=k == n)
         if nd:
             fin = [(rid, j) for rid, j in ids.items() if srv.poll(rid) == DONE]
-            feats, noisy = [], []
-            for rid, j in fin:
+            for b, (rid, j) in enumerate(fin):
                 r = reqs[j]
                 dp, ip = srv.result_device(rid)
-                d = torch.empty((height, width, 4), device="cuda")
-                i = torch.empty_like(d)
-                d.view(-1).copy_(_wrap_device(dp, height * width * 4))
-                i.view(-1).copy_(_wrap_device(ip, height * width * 4))
                 sc = scs[r["scene"]]
                 sc.set_render_params(width=width, height=height)
                 c = r["camera"]
                 sc.set_camera_orbit(c["target"], c["distance"], c["theta_deg"], c["phi_deg"], c["fovy_deg"])
-                f, nz = make_features(sc, sc.gbuffer(), d, i, spp, DEPTH_SCALE)
-                feats.append(f)
-                noisy.append(nz)
-                srv.release(rid)
-                del ids[rid]
+                sc.gbuffer(out=g)
+                make_features(sc, g, dp, ip, spp, DEPTH_SCALE, out=(feats[b], noisy[b]))
             if fin:
-                net.forward(torch.stack(feats).contiguous(), torch.stack(noisy).contiguous())
+                m = len(fin)
+                net.forward(feats[:m], noisy[:m], out=outb[:m])
                 torch.cuda.synchronize()
+                for rid, _ in fin:
+                    srv.release(rid)
+                    del ids[rid]
                 now = time.perf_counter() - t0
                 for _, j in fin:
                     lat[j] = now - reqs[j]["arrival_s"]
-                done += len(fin)
+                done += m
         elif k < n and not ids:
             time.sleep(min(2e-4, max(0.0, reqs[k]["arrival_s"] - (time.perf_counter() - t0))))
     wall = time.perf_counter() - t0

@@ -159,18 +159,29 @@ class Kpcn:
         return a
 
 
-def make_features(scene, gbuffer: dict, direct, indirect, spp: int, depth_scale: float, stream=None):
+def make_features(scene, gbuffer: dict, direct, indirect, spp: int, depth_scale: float, stream=None, out=None):
     """Network input of one rendered view: (features (h, w, 16) bfloat16,
     noisy radiance (h, w, 4) float32 = (direct + indirect) / spp) from the
-    render accumulators and the view's G-buffer (Scene.gbuffer())."""
+    render accumulators and the view's G-buffer (Scene.gbuffer()). direct
+    and indirect are CUDA tensors (h, w, 4), or device addresses (ints) of
+    such float4 planes when `out` = (feat, noisy) gives the output tensors
+    to fill."""
     import torch
 
     from .tracer import _gbuffer_struct
 
-    h, w = direct.shape[0], direct.shape[1]
-    feat = torch.empty((h, w, 16), dtype=torch.bfloat16, device=direct.device)
-    noisy = torch.empty((h, w, 4), dtype=torch.float32, device=direct.device)
+    if out is not None:
+        feat, noisy = out
+        h, w = feat.shape[0], feat.shape[1]
+        dev = feat.device
+    else:
+        h, w = direct.shape[0], direct.shape[1]
+        dev = direct.device
+        feat = torch.empty((h, w, 16), dtype=torch.bfloat16, device=dev)
+        noisy = torch.empty((h, w, 4), dtype=torch.float32, device=dev)
+    dp = C.c_void_p(direct) if isinstance(direct, int) else _ptr(direct)
+    ip = C.c_void_p(indirect) if isinstance(indirect, int) else _ptr(indirect)
     gb = _gbuffer_struct(gbuffer)
-    _lib.call("crt_kpcn_features", scene.handle, C.byref(gb), _ptr(direct), _ptr(indirect), int(spp), h * w,
-              float(depth_scale), _ptr(feat), _ptr(noisy), C.c_void_p(_torch_stream(direct.device, stream)))
+    _lib.call("crt_kpcn_features", scene.handle, C.byref(gb), dp, ip, int(spp), h * w, float(depth_scale), _ptr(feat),
+              _ptr(noisy), C.c_void_p(_torch_stream(dev, stream)))
     return feat, noisy

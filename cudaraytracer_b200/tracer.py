@@ -288,20 +288,26 @@ class Scene:
         _lib.call("crt_render_device_noalloc", self._h, int(first_sample), int(spp), direct.data_ptr(),
                   indirect.data_ptr(), sumsq.data_ptr() if sumsq is not None else None, C.c_void_p(s))
 
-    def gbuffer(self, prev_camera: dict | None = None, stream=None):
+    def gbuffer(self, prev_camera: dict | None = None, stream=None, out: dict | None = None):
         """Primary-hit G-buffer of the current camera (motion against
         prev_camera, a dict as returned by camera()). Returns a dict of CUDA
         tensors: pos_tri (H,W,4) f32, normal_mat (H,W,4) i16 bits of uint16,
-        bary_mesh (H,W,4) same, motion_depth (H,W,4) f32."""
+        bary_mesh (H,W,4) same, motion_depth (H,W,4) f32. Every pixel is
+        written; `out` (a dict of that shape) is filled instead of new
+        tensors."""
         import torch
 
-        rp = self.render_params()
-        h, w = rp["height"], rp["width"]
-        dev = torch.device("cuda", self.ctx.device)
-        g = {"pos_tri": torch.zeros((h, w, 4), dtype=torch.float32, device=dev),
-             "normal_mat": torch.zeros((h, w, 4), dtype=torch.int16, device=dev),
-             "bary_mesh": torch.zeros((h, w, 4), dtype=torch.int16, device=dev),
-             "motion_depth": torch.zeros((h, w, 4), dtype=torch.float32, device=dev)}
+        if out is not None:
+            g = out
+        else:
+            rp = self.render_params()
+            h, w = rp["height"], rp["width"]
+            dev = torch.device("cuda", self.ctx.device)
+            g = {"pos_tri": torch.empty((h, w, 4), dtype=torch.float32, device=dev),
+                 "normal_mat": torch.empty((h, w, 4), dtype=torch.int16, device=dev),
+                 "bary_mesh": torch.empty((h, w, 4), dtype=torch.int16, device=dev),
+                 "motion_depth": torch.empty((h, w, 4), dtype=torch.float32, device=dev)}
+        dev = g["pos_tri"].device
         gb = _gbuffer_struct(g)
         cam = None
         if prev_camera is not None:
