@@ -98,7 +98,7 @@ __device__ __forceinline__ bool nee_sample(const SceneView &s, Pcg32 &rng, int &
 
 // ProbeOutgongingPoint (material.cu:405-441): two probe rays along -n and +n
 // through the displaced point, the nearer hit wins.
-__device__ __forceinline__ void sss_probe(const SceneView &s, V3 hitPoint, V3 normal, float distance, float angle,
+static __device__ __noinline__ void sss_probe(const SceneView &s, V3 hitPoint, V3 normal, float distance, float angle,
                                           V3 &outP, V3 &outN) {
     V3 pn = normalized(normal), t, b;
     create_onb(pn, t, b);
