@@ -67,7 +67,7 @@ enum StageTraversal : int {
     kStageLocalQuant = 2,
     kStageSharedQuant = 3,
 };
-constexpr int kStageTraversalDefault = kStageShared;
+constexpr int kStageTraversalDefault = kStageLocal;
 
 // The mode for the next launches: kStageTraversalDefault, or the one named
 // by CRT_STAGE_TRAVERSAL (local, shared, local-quant, shared-quant).

@@ -435,25 +435,36 @@ def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: 
     feats = torch.empty((n, height, width, 16), dtype=torch.bfloat16, device=dev)
     noisy = torch.empty((n, height, width, 4), dtype=torch.float32, device=dev)
     outb = torch.empty((n, height, width, 4), dtype=torch.float32, device=dev)
+    for sc in scs:
+        sc.set_render_params(width=width, height=height)
+    tm = {"submit_s": 0.0, "step_s": 0.0, "poll_s": 0.0, "features_s": 0.0, "forward_s": 0.0}
     t0 = time.perf_counter()
     while done < n:
-        now = time.perf_counter() - t0
+        ta = time.perf_counter()
+        now = ta - t0
         while k < n and reqs[k]["arrival_s"] <= now:
             r = reqs[k]
             ids[srv.submit(RenderRequest(r["scene"], width, height, spp, r["camera"], seed=r["seed"]))] = k
             k += 1
+        tb = time.perf_counter()
         nd = srv.step(wait=k == n)
+        tc = time.perf_counter()
+        tm["submit_s"] += tb - ta
+        tm["step_s"] += tc - tb
         if nd:
             fin = [(rid, j) for rid, j in ids.items() if srv.poll(rid) == DONE]
+            td = time.perf_counter()
             for b, (rid, j) in enumerate(fin):
                 r = reqs[j]
                 dp, ip = srv.result_device(rid)
                 sc = scs[r["scene"]]
-                sc.set_render_params(width=width, height=height)
                 c = r["camera"]
                 sc.set_camera_orbit(c["target"], c["distance"], c["theta_deg"], c["phi_deg"], c["fovy_deg"])
                 sc.gbuffer(out=g)
                 make_features(sc, g, dp, ip, spp, DEPTH_SCALE, out=(feats[b], noisy[b]))
+            te = time.perf_counter()
+            tm["poll_s"] += td - tc
+            tm["features_s"] += te - td
             if fin:
                 m = len(fin)
                 net.forward(feats[:m], noisy[:m], out=outb[:m])
@@ -462,6 +473,7 @@ def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: 
                     srv.release(rid)
                     del ids[rid]
                 now = time.perf_counter() - t0
+                tm["forward_s"] += now + t0 - te
                 for _, j in fin:
                     lat[j] = now - reqs[j]["arrival_s"]
                 done += m
@@ -469,7 +481,9 @@ def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: 
             time.sleep(min(2e-4, max(0.0, reqs[k]["arrival_s"] - (time.perf_counter() - t0))))
     wall = time.perf_counter() - t0
     srv.close()
-    return _lat_summary(lat, wall, n)
+    out = _lat_summary(lat, wall, n)
+    out["host_time_split_s"] = {k2: round(v, 4) for k2, v in tm.items()}
+    return out
 
 
 def _wrap_device(ptr: int, count: int):
