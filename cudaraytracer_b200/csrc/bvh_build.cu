@@ -36,6 +36,28 @@ constexpr int kMedianDepth = 36;   // below this depth, split by index median
 constexpr float kCostTrav = 1.0f;
 constexpr float kCostTri = 1.0f;
 
+// The SAH's leaf decision in the small phase: traversal cost relative to
+// one triangle test, and the largest leaf it may form (1..kMaxLeafSAH).
+// Defaults kCostTrav and kMaxLeafSAH; CRT_SAH_TRAV and CRT_SAH_MAX_LEAF
+// override them at build time (for measuring other tree shapes).
+struct SahParams {
+    float cost_trav;
+    int max_leaf;
+};
+
+SahParams sah_params() {
+    SahParams p{kCostTrav, kMaxLeafSAH};
+    if (const char *e = getenv("CRT_SAH_TRAV")) {
+        const float v = (float)atof(e);
+        if (v > 0.f && v < 100.f) p.cost_trav = v;
+    }
+    if (const char *e = getenv("CRT_SAH_MAX_LEAF")) {
+        const int v = atoi(e);
+        if (v >= 1 && v <= kMaxLeafSAH) p.max_leaf = v;
+    }
+    return p;
+}
+
 struct Task {
     int start, count, link_slot, depth;
     float blo[3], bhi[3];  // bounds of the primitives
@@ -456,7 +478,8 @@ struct SmallShared {
 };
 
 __global__ void __launch_bounds__(kBlock) k_small(const Task *tasks, int *idx, const float4 *plo, const float4 *phi,
-                                                  float4 *nodes, int *node_counter, int *max_depth, int *error_flag) {
+                                                  float4 *nodes, int *node_counter, int *max_depth, int *error_flag,
+                                                  SahParams sah) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SmallShared &S = *reinterpret_cast<SmallShared *>(smem_raw);
     const int tid = threadIdx.x;
@@ -504,9 +527,9 @@ __global__ void __launch_bounds__(kBlock) k_small(const Task *tasks, int *idx, c
             int mode;
             float area = half_area(t.blo[0], t.blo[1], t.blo[2], t.bhi[0], t.bhi[1], t.bhi[2]);
             float leaf_cost = kCostTri * t.count;
-            float split_cost = axis >= 0 ? kCostTrav + kCostTri * (area > 0.f ? best / area : (float)t.count)
+            float split_cost = axis >= 0 ? sah.cost_trav + kCostTri * (area > 0.f ? best / area : (float)t.count)
                                          : INFINITY;
-            if (t.count <= 1 || (t.count <= kMaxLeafSAH && leaf_cost <= split_cost))
+            if (t.count <= 1 || (t.count <= sah.max_leaf && leaf_cost <= split_cost))
                 mode = 0;
             else if (axis >= 0)
                 mode = 1;
@@ -767,7 +790,8 @@ void build_bvh(const float *d_verts, int n, cudaStream_t stream, BvhBuffers &out
             size_t smem = sizeof(SmallShared);
             CRT_CUDA(cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_small<<<(int)small.size(), kBlock, smem, stream>>>(d_small.p, idx.p, plo.p, phi.p, out.nodes,
-                                                                counters.p, counters.p + 1, counters.p + 2);
+                                                                counters.p, counters.p + 1, counters.p + 2,
+                                                                sah_params());
             CRT_CUDA(cudaGetLastError());
             CRT_CUDA(cudaStreamSynchronize(stream));
         }

@@ -351,8 +351,10 @@ struct crt_kpcn {
     float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
     __nv_bfloat16 *wbuf = nullptr;  // BF16 weights and transposes
     int64_t step = 0;
-    // activation / gradient buffers sized for (n, h, w)
+    // activation / gradient buffers: the current (n, h, w) and the pixel
+    // count the buffers hold (a smaller batch or image reuses them)
     int n = 0, h = 0, w = 0;
+    size_t cap_px = 0;
     std::vector<void *> bufs;
     __nv_bfloat16 *act[kLayers] = {};
     __nv_bfloat16 *pool0 = nullptr, *pool1 = nullptr, *cat1 = nullptr, *cat0 = nullptr;
@@ -371,6 +373,7 @@ struct crt_kpcn {
         for (void *p : bufs) cudaFree(p);
         bufs.clear();
         n = h = w = 0;
+        cap_px = 0;
     }
     template <class T>
     T *alloc(size_t count) {
@@ -382,10 +385,17 @@ struct crt_kpcn {
     void ensure(int n_, int h_, int w_) {
         CRT_CHECK(n_ > 0 && h_ > 0 && w_ > 0 && h_ % 4 == 0 && w_ % 4 == 0, CRT_ERR_INVALID,
                   "kpcn: image height and width must be multiples of 4");
-        if (n_ == n && h_ == h && w_ == w) return;
+        // every buffer is a per-pixel plane of the full, half or quarter
+        // resolution, so buffers for cap_px pixels hold any n * h * w <= cap_px
+        const size_t P0 = (size_t)n_ * h_ * w_, P1 = P0 / 4, P2 = P0 / 16;
+        if (P0 <= cap_px) {
+            n = n_;
+            h = h_;
+            w = w_;
+            return;
+        }
         CRT_CUDA(cudaDeviceSynchronize());
         free_buffers();
-        const size_t P0 = (size_t)n_ * h_ * w_, P1 = P0 / 4, P2 = P0 / 16;
         const size_t P[kLayers] = {P0, P0, P1, P1, P2, P2, P1, P1, P0, P0, P0};
         for (int i = 0; i < OUT; ++i) act[i] = alloc<__nv_bfloat16>(P[i] * L[i].cout);
         pool0 = alloc<__nv_bfloat16>(P1 * 32);
@@ -404,6 +414,7 @@ struct crt_kpcn {
         n = n_;
         h = h_;
         w = w_;
+        cap_px = P0;
     }
     void conv(int i, const __nv_bfloat16 *in, int ln, int lh, int lw, __nv_bfloat16 *out, float *out_f32,
               cudaStream_t s) {

@@ -390,9 +390,10 @@ __global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const 
     }
 }
 
-__global__ void __launch_bounds__(256) k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits,
-                                               const int *n_in, QueueView qout, int *counters, int out_idx,
-                                               ShadowView sh, float4 *term0, float4 *term1, AccumView acc) {
+__device__ __forceinline__ void shade_body(const SceneView &s, const StepParams &sp, const QueueView &qin,
+                                           const float4 *hits, const int *n_in, const QueueView &qout, int *counters,
+                                           int out_idx, const ShadowView &sh, float4 *term0, float4 *term1,
+                                           const AccumView &acc) {
     const int n = *n_in;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         PathState ps = load_path(qin, i);
@@ -440,6 +441,30 @@ __global__ void __launch_bounds__(256) k_shade(SceneView s, StepParams sp, Queue
             sh.r[3][sslot] = make_float4(nee.C.x, nee.C.y, nee.C.z, __uint_as_float(target));
         }
     }
+}
+
+__global__ void __launch_bounds__(256) k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits,
+                                               const int *n_in, QueueView qout, int *counters, int out_idx,
+                                               ShadowView sh, float4 *term0, float4 *term1, AccumView acc) {
+    shade_body(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc);
+}
+
+// The same with registers capped for kMinBlocks resident 128-thread blocks
+// per SM (more warps to cover the shade stage's instruction-fetch stalls,
+// against spills); selected by CRT_SHADE_MIN_BLOCKS = 6 or 8 for blocks of
+// at most 128 threads.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(128, kMinBlocks) k_shade_mb(SceneView s, StepParams sp, QueueView qin,
+                                                               const float4 *hits, const int *n_in, QueueView qout,
+                                                               int *counters, int out_idx, ShadowView sh,
+                                                               float4 *term0, float4 *term1, AccumView acc) {
+    shade_body(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc);
+}
+
+static int shade_min_blocks(int block) {
+    const char *e = getenv("CRT_SHADE_MIN_BLOCKS");
+    const int v = e ? atoi(e) : 0;
+    return (block <= 128 && (v == 6 || v == 8)) ? v : 0;
 }
 
 // Shadow: Light::Visible for each deferred NEE sample; a visible sample's
@@ -542,7 +567,10 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
     const int blk = rp.block();
     const int smem = stage_traversal();
     const int g_ext = persistent_grid((const void *)k_extend, blk);
-    const int g_sh = persistent_grid((const void *)k_shade, blk);
+    const int mb = shade_min_blocks(blk);
+    const void *shade_fn = mb == 6 ? (const void *)k_shade_mb<6> : mb == 8 ? (const void *)k_shade_mb<8>
+                                                                              : (const void *)k_shade;
+    const int g_sh = persistent_grid(shade_fn, blk);
     const int g_sd = persistent_grid((const void *)k_shadow, blk);
     int launches = 0;
     for (int done = 0; done < spp; done += per_pass) {
@@ -561,8 +589,15 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
             int in = b & 1, out = 1 - in;
             sp.bounce = b;
             k_extend<<<g_ext, blk, 0, stream>>>(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out, smem);
-            k_shade<<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out], wf.counters, out, sh,
-                                              wf.term[0], wf.term[1], av);
+            if (mb == 6)
+                k_shade_mb<6><<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out],
+                                                        wf.counters, out, sh, wf.term[0], wf.term[1], av);
+            else if (mb == 8)
+                k_shade_mb<8><<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out],
+                                                        wf.counters, out, sh, wf.term[0], wf.term[1], av);
+            else
+                k_shade<<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out], wf.counters,
+                                                  out, sh, wf.term[0], wf.term[1], av);
             k_shadow<<<g_sd, blk, 0, stream>>>(view.bvh, sh, wf.counters, q[out], wf.term[0], wf.term[1], av, smem);
             launches += 3;
         }

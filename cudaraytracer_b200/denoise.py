@@ -330,15 +330,18 @@ def evaluate_sequences(ctx, net: Kpcn, scene_seeds, width: int, height: int, fra
     return out
 
 
-def sequence_requests(ctx, scene_seeds, width: int, height: int, frames: int, rate_per_s: float, seed: int = 0):
+def sequence_requests(ctx, scene_seeds, width: int, height: int, frames: int, rate_per_s: float, seed: int = 0,
+                      scenes_in=None):
     """Requests for the frames of one orbit sequence per scene, interleaved
     by frame (frame f of every sequence before frame f + 1), arriving as a
     Poisson process at rate_per_s (all at t = 0 when rate_per_s is 0).
     Returns (scenes, requests) with requests as dicts (scene index,
-    sequence frame, camera, seed, arrival_s)."""
+    sequence frame, camera, seed, arrival_s). scenes_in: the scenes of an
+    earlier call with the same seeds, reused instead of built again."""
     from . import scenes
 
-    scs = [Scene.from_spec(ctx, scenes.cornell_box(width=width, height=height, seed=int(s))) for s in scene_seeds]
+    scs = scenes_in or [Scene.from_spec(ctx, scenes.cornell_box(width=width, height=height, seed=int(s)))
+                        for s in scene_seeds]
     seqs = [orbit_sequence(sc, frames, int(s) * 7 + 3) for sc, s in zip(scs, scene_seeds)]
     rng = np.random.default_rng(seed)
     t = 0.0
@@ -408,20 +411,32 @@ def run_plain_svgf_loop(ctx, scs, reqs, width: int, height: int, spp: int = 64):
     return _lat_summary(lat, wall, len(reqs))
 
 
-def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: int, paths_per_pass: int = 8 << 20):
+def learned_server(ctx, scs, paths_per_pass: int = 8 << 20):
+    """A multi-scene server holding scs (in order) for run_learned_served."""
+    from .serve import Server
+
+    srv = Server(ctx, paths_per_pass=paths_per_pass)
+    for sc in scs:
+        srv.add_scene(sc)
+    return srv
+
+
+def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: int, paths_per_pass: int = 8 << 20,
+                       server=None):
     """The learned pipeline, open loop: each request is submitted to the
     multi-scene server (continuous batching) at spp when it arrives; the
     requests that finish rendering in a server step get their G-buffer and
     features (built straight from the server's accumulators into one batch)
     and go through one batched KPCN forward together; latency = completion
-    of that forward - arrival."""
+    of that forward - arrival. server: a long-lived server from
+    learned_server(ctx, scs) (its wavefront and accumulator pool stay
+    allocated between runs, as in a serving process); without one a server
+    is created and closed inside the timed loop."""
     import torch
 
-    from .serve import DONE, RenderRequest, Server
+    from .serve import DONE, RenderRequest
 
-    srv = Server(ctx, paths_per_pass=paths_per_pass)
-    for sc in scs:
-        srv.add_scene(sc)
+    srv = server or learned_server(ctx, scs, paths_per_pass)
     n = len(reqs)
     lat = [0.0] * n
     ids = {}
@@ -437,6 +452,10 @@ def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: 
     outb = torch.empty((n, height, width, 4), dtype=torch.float32, device=dev)
     for sc in scs:
         sc.set_render_params(width=width, height=height)
+    # size the network's buffers for the largest batch (every request at
+    # once); smaller batches reuse them
+    net.forward(feats, noisy, out=outb)
+    torch.cuda.synchronize()
     tm = {"submit_s": 0.0, "step_s": 0.0, "poll_s": 0.0, "features_s": 0.0, "forward_s": 0.0}
     t0 = time.perf_counter()
     while done < n:
@@ -468,7 +487,8 @@ def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: 
             if fin:
                 m = len(fin)
                 net.forward(feats[:m], noisy[:m], out=outb[:m])
-                torch.cuda.synchronize()
+                # this batch's stream only: the server's next passes keep running
+                torch.cuda.current_stream().synchronize()
                 for rid, _ in fin:
                     srv.release(rid)
                     del ids[rid]
@@ -480,7 +500,8 @@ def run_learned_served(ctx, net: Kpcn, scs, reqs, width: int, height: int, spp: 
         elif k < n and not ids:
             time.sleep(min(2e-4, max(0.0, reqs[k]["arrival_s"] - (time.perf_counter() - t0))))
     wall = time.perf_counter() - t0
-    srv.close()
+    if server is None:
+        srv.close()
     out = _lat_summary(lat, wall, n)
     out["host_time_split_s"] = {k2: round(v, 4) for k2, v in tm.items()}
     return out

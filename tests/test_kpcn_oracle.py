@@ -13,7 +13,7 @@ def test_bf16_rounding_is_nearest_even():
     assert r[2] == np.float32(1.0 + 4 * 2 ** -8)
     assert r[3] == -2.5 and r[4] == 0.0
     b = K.bf16_bits(np.float32(1.0))
-    assert int(b) == 0x3F80
+    assert int(np.asarray(b).reshape(-1)[0]) == 0x3F80
     np.testing.assert_array_equal(K.from_bf16_bits(K.bf16_bits(r)), r)
 
 

@@ -178,3 +178,19 @@ def test_stage_traversal_modes_agree(crt_ctx, ico_json, monkeypatch, mode):
     crt_ctx.check_device_errors()
     compare(d1, d0, 1e-4, 0.002)
     compare(i1, i0, 1e-4, 0.002)
+
+
+@pytest.mark.parametrize("min_blocks", ["6", "8"])
+def test_shade_register_caps_agree(crt_ctx, ico_json, monkeypatch, min_blocks):
+    """The shade stage compiled for 6 or 8 resident blocks per SM (registers
+    capped, spilling to local memory) gives the frame of the default build,
+    up to the order of the float atomics that add paths into pixels."""
+    sc = Scene.load(crt_ctx, ico_json)
+    sc.set_render_params(seed=9)
+    monkeypatch.delenv("CRT_SHADE_MIN_BLOCKS", raising=False)
+    d0, i0 = sc.render(4)
+    monkeypatch.setenv("CRT_SHADE_MIN_BLOCKS", min_blocks)
+    d1, i1 = sc.render(4)
+    crt_ctx.check_device_errors()
+    compare(d1, d0, 1e-4, 0.002)
+    compare(i1, i0, 1e-4, 0.002)
