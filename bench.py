@@ -58,7 +58,7 @@ def measured_peaks():
 # the same kernel build on the same batch distribution, scaled x2 (ray bytes
 # scale exactly, node visits linearly for uniform random rays). The capture
 # and its command are summarised in profiles/ (traversal summary).
-TRAFFIC_PER_16M = {"extend": 1698088448, "shadow": 5904843776}
+TRAFFIC_PER_16M = {"extend": 2 * (564561664 + 132257024), "shadow": 2 * (1538991104 + 26396672)}
 
 
 def profiled_traffic(kernel: str):
@@ -588,13 +588,13 @@ def kpcn_layers_leg(ctx, reps=10):
             "peak_tflops": peak}
 
 
-def denoise_leg(ctx, train_steps=1500):
+def denoise_leg(ctx, train_steps=3000):
     """Learned denoiser against SVGF (the learned-denoiser workload, at
     256x256 instead of 1920x1080 and 16-frame instead of 60-frame
     sequences so the 4096-spp references fit the bench): the KPCN is
     trained on the GPU on 64 views of seeded Cornell variants (scene seeds
     100-163, one view each, 1-16 spp inputs, 4096-spp references) for
-    1500 Adam steps of 8 random 128x128 crops. Test: one 16-frame orbit
+    3000 Adam steps of 8 random 128x128 crops. Test: one 16-frame orbit
     sequence (1.5 deg per frame) per unseen scene (seeds 200-207), relMSE
     of every frame against its 4096-spp reference for raw and KPCN at 1-32
     spp and for SVGF run temporally over the sequence at 1 and 64 spp.

@@ -5,7 +5,9 @@
 // host-synchronised launch sequence per bounce (Src/Core/renderer.cuh:
 // 1144-1193: cudaDeviceSynchronize after every kernel, two blocking copies
 // in every StreamCompaction). Here the flattened index space
-// (sample, view, pixel) is cut into passes of `paths_per_pass` paths. One
+// (view, sample, pixel) is cut into passes of `paths_per_pass` paths (view
+// outermost, so a pass adds into the accumulators of a few views, which stay
+// in L2, rather than of every view). One
 // pass - view-aware raygen, max_bounces x (extend, shade, shadow), and a
 // one-thread kernel that advances the device-side pass base - is captured
 // once as a CUDA graph and replayed; queue lengths and the pass base live in
@@ -31,10 +33,10 @@ __global__ void k_raygen_views(const CamView *cams, int n_views, StepParams sp, 
     if (i == 0) counters[0] = n;
     if (i >= n) return;
     const int64_t g = base + i;
-    const int64_t per_sample = (int64_t)n_views * sp.pixels;
-    const uint32_t sample = (uint32_t)(sp.first_sample + g / per_sample);
-    const int64_t rest = g % per_sample;
-    const int view = (int)(rest / sp.pixels);
+    const int64_t per_view = total / n_views;  // spp * pixels
+    const int view = (int)(g / per_view);
+    const int64_t rest = g % per_view;
+    const uint32_t sample = (uint32_t)(sp.first_sample + rest / sp.pixels);
     const int pix = (int)(rest % sp.pixels);
     const CamView &cam = cams[view];
     const uint32_t pixel = (uint32_t)(view * sp.pixels + pix);  // accumulator index

@@ -33,7 +33,11 @@ constexpr int kChunk = 4096;       // primitives per block in the large phase
 constexpr int kBlock = 256;
 constexpr int kMaxLeafSAH = 8;     // largest leaf the SAH may choose
 constexpr int kMedianDepth = 36;   // below this depth, split by index median
-constexpr float kCostTrav = 1.0f;
+// Traversal step cost relative to one triangle test: 3 (leaves of 4.5
+// triangles on average on the icosphere field, 293k nodes for 1.31M
+// triangles) measured 6% faster shadow queries than 1 (1.7 per leaf, 764k
+// nodes), extend within 1.5%; higher costs were not faster.
+constexpr float kCostTrav = 3.0f;
 constexpr float kCostTri = 1.0f;
 
 // The SAH's leaf decision in the small phase: traversal cost relative to

@@ -443,16 +443,19 @@ __device__ __forceinline__ void shade_body(const SceneView &s, const StepParams 
     }
 }
 
-__global__ void __launch_bounds__(256) k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits,
-                                               const int *n_in, QueueView qout, int *counters, int out_idx,
-                                               ShadowView sh, float4 *term0, float4 *term1, AccumView acc) {
+// Registers capped at 64 (4 blocks of 256 or 8 of 128 threads per SM): the
+// shade body is bound by instruction fetch, and twice the resident warps of
+// its natural 112 registers cover more of it than the spills cost (measured
+// 5% faster per 1080p frame).
+__global__ void __launch_bounds__(256, 4) k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits,
+                                                  const int *n_in, QueueView qout, int *counters, int out_idx,
+                                                  ShadowView sh, float4 *term0, float4 *term1, AccumView acc) {
     shade_body(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc);
 }
 
-// The same with registers capped for kMinBlocks resident 128-thread blocks
-// per SM (more warps to cover the shade stage's instruction-fetch stalls,
-// against spills); selected by CRT_SHADE_MIN_BLOCKS = 6 or 8 for blocks of
-// at most 128 threads.
+// The same compiled for kMinBlocks resident 128-thread blocks per SM (4: no
+// cap, 112 registers; 6: 80; 10: 48), to measure the trade against the
+// default; selected by CRT_SHADE_MIN_BLOCKS for blocks of at most 128 threads.
 template <int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) k_shade_mb(SceneView s, StepParams sp, QueueView qin,
                                                                const float4 *hits, const int *n_in, QueueView qout,
@@ -464,7 +467,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_shade_mb(SceneView s, StepP
 static int shade_min_blocks(int block) {
     const char *e = getenv("CRT_SHADE_MIN_BLOCKS");
     const int v = e ? atoi(e) : 0;
-    return (block <= 128 && (v == 6 || v == 8)) ? v : 0;
+    return (block <= 128 && (v == 4 || v == 6 || v == 10)) ? v : 0;
 }
 
 // Shadow: Light::Visible for each deferred NEE sample; a visible sample's
@@ -568,8 +571,10 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
     const int smem = stage_traversal();
     const int g_ext = persistent_grid((const void *)k_extend, blk);
     const int mb = shade_min_blocks(blk);
-    const void *shade_fn = mb == 6 ? (const void *)k_shade_mb<6> : mb == 8 ? (const void *)k_shade_mb<8>
-                                                                              : (const void *)k_shade;
+    const void *shade_fn = mb == 4    ? (const void *)k_shade_mb<4>
+                           : mb == 6  ? (const void *)k_shade_mb<6>
+                           : mb == 10 ? (const void *)k_shade_mb<10>
+                                      : (const void *)k_shade;
     const int g_sh = persistent_grid(shade_fn, blk);
     const int g_sd = persistent_grid((const void *)k_shadow, blk);
     int launches = 0;
@@ -589,12 +594,15 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
             int in = b & 1, out = 1 - in;
             sp.bounce = b;
             k_extend<<<g_ext, blk, 0, stream>>>(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out, smem);
-            if (mb == 6)
+            if (mb == 4)
+                k_shade_mb<4><<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out],
+                                                        wf.counters, out, sh, wf.term[0], wf.term[1], av);
+            else if (mb == 6)
                 k_shade_mb<6><<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out],
                                                         wf.counters, out, sh, wf.term[0], wf.term[1], av);
-            else if (mb == 8)
-                k_shade_mb<8><<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out],
-                                                        wf.counters, out, sh, wf.term[0], wf.term[1], av);
+            else if (mb == 10)
+                k_shade_mb<10><<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out],
+                                                         wf.counters, out, sh, wf.term[0], wf.term[1], av);
             else
                 k_shade<<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out], wf.counters,
                                                   out, sh, wf.term[0], wf.term[1], av);

@@ -110,8 +110,9 @@ __global__ void __launch_bounds__(128) ks_extend(const SceneView *scenes, QueueV
 // The single-scene shade (k_shade in render.cu) with per-path scene and
 // request. A path still alive after its request's last bounce is dropped
 // with its pending NEE sample, as the reference drops survivors
-// (renderer.cuh:1166-1193).
-__global__ void __launch_bounds__(128) ks_shade(const SceneView *scenes, const ReqDesc *reqs, int bounce,
+// (renderer.cuh:1166-1193). Registers capped for 8 resident blocks per
+// SM, as k_shade.
+__global__ void __launch_bounds__(128, 8) ks_shade(const SceneView *scenes, const ReqDesc *reqs, int bounce,
                                                 QueueView qin, const float4 *hits, const int *n_in, QueueView qout,
                                                 int *counters, int out_idx, ShadowView sh, float4 *term0,
                                                 float4 *term1) {

@@ -415,6 +415,24 @@ struct VarTileTaps {
     __device__ __forceinline__ float4 m(int x, int y) const { return sm[at(x, y)]; }
 };
 
+// Edge-stopping weights in the log domain. The reference's tap weight
+// powf(c, s) * expf(w) (c the clamped normal dot, w the summed depth and
+// luminance terms) equals exp2(s * log2(c) + w * log2(e)); it is evaluated
+// with one lg2 and one ex2 of the special-function unit (relative error
+// about 1e-6, against the filters' 1e-3 parity bound) instead of powf, expf
+// and their range reductions. c = 0 gives log2 = -inf and a weight of 0, as
+// powf(0, s) does for s > 0.
+constexpr float kLog2e = 1.44269504088896341f;
+__device__ __forceinline__ float log_weight(float c, float s) { return s * __log2f(c); }
+__device__ __forceinline__ float sqrt_fast(float x) { return x * rsqrtf(x); }  // x > 0
+
+// sqrt(ki^2 + kj^2) for |ki|, |kj| <= 3, at [|kj| * 4 + |ki|] (correctly
+// rounded values; the tap loops index it with warp-uniform offsets).
+__constant__ float c_tap_dist[16] = {0.f,         1.f,         2.f,         3.f,
+                                     1.f,         1.41421356f, 2.23606798f, 3.16227766f,
+                                     2.f,         2.23606798f, 2.82842712f, 3.60555128f,
+                                     3.f,         3.16227766f, 3.60555128f, 4.24264069f};
+
 // ComputeVarianceKernel (renderer.cuh:689-805) for pixel (x, y) with a
 // history shorter than 4 frames: 7x7 edge-stopped filter of colour and
 // moments, variance from the filtered moments.
@@ -446,13 +464,13 @@ __device__ __forceinline__ void variance_pixel(const VarianceArgs &a, const GB &
             V3 nn{ne.x, ne.y, ne.z};
             float ndl = luminance(nd), nil = luminance(nid);
             const float4 mm = src.m(ni, nj);
-            float dist = sqrtf(float(ki * ki + kj * kj));
-            float wz = -fabsf(cdepth - nz) / (sd * dist + 1e-4f);
-            float wn = powf(fmaxf(0.f, dot(cn, nn)), a.sigma_normal);
+            const float dist = c_tap_dist[abs(kj) * 4 + abs(ki)];
+            float wz = -__fdividef(fabsf(cdepth - nz), sd * dist + 1e-4f);
+            const float ln = log_weight(fmaxf(0.f, dot(cn, nn)), a.sigma_normal);
             float dref = fmaxf(fmaxf(cdl, ndl), 1e-4f);
-            float wdl = -fabsf(cdl - ndl) * sqrtf(dref) * inv_sl;
+            float wdl = -fabsf(cdl - ndl) * sqrt_fast(dref) * inv_sl;
             float wil = -fabsf(cil - nil) * il_scale;
-            float dw = expf(wz + wdl) * wn, iw = expf(wz + wil) * wn;
+            float dw = exp2f(fmaf(wz + wdl, kLog2e, ln)), iw = exp2f(fmaf(wz + wil, kLog2e, ln));
             fd = fd + nd * dw;
             fi = fi + nid * iw;
             fmd0 += mm.x * dw;
@@ -630,14 +648,14 @@ __device__ __forceinline__ void atrous_pixel(const AtrousArgs &a, const GB &g, c
             const int r2 = ki * ki + kj * kj;
             const int zi = r2 == 0 ? 0 : (r2 == 1 ? 1 : (r2 == 2 ? 2 : (r2 == 4 ? 3 : (r2 == 5 ? 4 : 5))));
             float wz = -fabsf(cdepth - nz) * inv_z[zi];
-            float wn = powf(fmaxf(0.f, dot(cn, nn)), sn);
+            const float ln = log_weight(fmaxf(0.f, dot(cn, nn)), sn);
             float ndl = luminance(nd), nil = luminance(nic);
             float dref = fmaxf(fmaxf(cdl, ndl), 1e-4f);
-            float wdl = -fabsf(cdl - ndl) * sqrtf(dref) * inv_ld;
+            float wdl = -fabsf(cdl - ndl) * sqrt_fast(dref) * inv_ld;
             float wil = -fabsf(cil - nil) * il_scale;
             float hc = boot > 0.f ? (0.5f + 0.5f * fminf((float)nh / 4.f, 1.f)) : 1.f;
-            float kwt = kw[abs(ki)] * kw[abs(kj)];
-            float dw = expf(wz + wdl) * wn * kwt * hc, iw = expf(wz + wil) * wn * kwt * hc;
+            float kwt = kw[abs(ki)] * kw[abs(kj)] * hc;
+            float dw = exp2f(fmaf(wz + wdl, kLog2e, ln)) * kwt, iw = exp2f(fmaf(wz + wil, kLog2e, ln)) * kwt;
             fd = fd + dw * nd;
             fi = fi + iw * nic;
             twd += dw;

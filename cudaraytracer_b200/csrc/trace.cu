@@ -102,6 +102,25 @@ __global__ void __launch_bounds__(kTraceBlock, 8) k_trace_shadow_q(BvhView bvh, 
     trace_dynamic_st<true, true>(job, n, st);
 }
 
+// The binary traversal with the local stack and pipelined triangle loads,
+// for at least kMinBlocks resident blocks per SM (1: no register cap).
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTraceBlock, kMinBlocks) k_trace_closest_pf(BvhView bvh,
+                                                                             const float4 *__restrict__ rays, int n,
+                                                                             float4 *__restrict__ hits) {
+    ClosestJob job{bvh, rays, hits};
+    LocalStack st;
+    trace_dynamic_st<true, false, ClosestJob, LocalStack, true>(job, n, st);
+}
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTraceBlock, kMinBlocks) k_trace_shadow_pf(BvhView bvh, const float4 *__restrict__ q,
+                                                                            int n, uint8_t *__restrict__ occ) {
+    ShadowJob job{bvh, q, occ, {}};
+    LocalStack st;
+    trace_dynamic_st<true, false, ShadowJob, LocalStack, true>(job, n, st);
+}
+
 // The binary traversal with postponed leaves (traverse.cuh), local stack.
 __global__ void __launch_bounds__(kTraceBlock) k_trace_closest_p(BvhView bvh, const float4 *__restrict__ rays, int n,
                                                                  float4 *__restrict__ hits) {
@@ -178,7 +197,9 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8r(BvhView bvh, con
 // Traversal variant of the trace kernels (CRT_TRAVERSAL overrides the
 // default kTraceVariant): 2 = binary tree, stack in local memory
 // (210 / 212: the same capped at 51 / 42 registers for 10 / 12 blocks per SM;
-// 3: with postponed leaves; 4 / 416: over the 16-bit quantised nodes with
+// 3: with postponed leaves; 5 / 58: with pipelined triangle loads (no
+// register cap / 8 blocks per SM); 4 / 416: over
+// the 16-bit quantised nodes with
 // the stack in local / shared memory);
 // 28 / 216 = binary tree, top 8 / 16 stack entries per lane in shared
 // memory; 8 / 82 = 8-wide quantised tree (built only with CRT_BVH8=1),
@@ -214,6 +235,12 @@ void launch_trace_closest(const BvhView &bvh, const float4 *d_rays, int64_t n, f
     else if (v == 3)
         k_trace_closest_p<<<trace_grid((const void *)k_trace_closest_p, n), kTraceBlock, 0, s>>>(bvh, d_rays, (int)n,
                                                                                                 d_hits);
+    else if (v == 5)
+        k_trace_closest_pf<1><<<trace_grid((const void *)k_trace_closest_pf<1>, n), kTraceBlock, 0, s>>>(
+            bvh, d_rays, (int)n, d_hits);
+    else if (v == 58)
+        k_trace_closest_pf<8><<<trace_grid((const void *)k_trace_closest_pf<8>, n), kTraceBlock, 0, s>>>(
+            bvh, d_rays, (int)n, d_hits);
     else if (v == 210)
         k_trace_closest_o<10><<<trace_grid((const void *)k_trace_closest_o<10>, n), kTraceBlock, 0, s>>>(
             bvh, d_rays, (int)n, d_hits);
@@ -255,6 +282,12 @@ void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_
             bvh, q, (int)n, d_occ);
     else if (v == 3)
         k_trace_shadow_p<<<trace_grid((const void *)k_trace_shadow_p, n), kTraceBlock, 0, s>>>(bvh, q, (int)n, d_occ);
+    else if (v == 5)
+        k_trace_shadow_pf<1><<<trace_grid((const void *)k_trace_shadow_pf<1>, n), kTraceBlock, 0, s>>>(bvh, q,
+                                                                                                      (int)n, d_occ);
+    else if (v == 58)
+        k_trace_shadow_pf<8><<<trace_grid((const void *)k_trace_shadow_pf<8>, n), kTraceBlock, 0, s>>>(bvh, q,
+                                                                                                      (int)n, d_occ);
     else if (v == 210)
         k_trace_shadow_o<10><<<trace_grid((const void *)k_trace_shadow_o<10>, n), kTraceBlock, 0, s>>>(bvh, q, (int)n,
                                                                                                     d_occ);

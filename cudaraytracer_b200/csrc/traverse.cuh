@@ -30,7 +30,7 @@ namespace crt {
 
 #ifdef __CUDACC__
 
-template <bool kCull, bool kQuant, class Job, class Stack>
+template <bool kCull, bool kQuant, class Job, class Stack, bool kPipe = false>
 __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st);
 
 // The stack in local memory, float nodes.
@@ -41,8 +41,10 @@ __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
 }
 
 // Over a given per-lane stack (LocalStack or ShortStack, bvh.cuh), and over
-// the float nodes or (kQuant) their 16-bit quantised copy (bvh16.cuh).
-template <bool kCull, bool kQuant, class Job, class Stack>
+// the float nodes or (kQuant) their 16-bit quantised copy (bvh16.cuh). With
+// kPipe the leaf loop loads triangle k + 1 before testing triangle k, so its
+// 48 B are in flight during the test (same tests in the same order).
+template <bool kCull, bool kQuant, class Job, class Stack, bool kPipe>
 __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
     const unsigned lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -137,14 +139,36 @@ __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
         if (!finished) {
             const int code = ~link;
             const int first = code >> 4, count = code & 15;
-            for (int k = 0; k < count; ++k) {
-                const int slot = first + k;
-                const float4 *tp = bvh.tris + 3 * (size_t)slot;
+            if (kPipe && count > 0) {
+                // [first, first + count) checked against num_tris above
+                const float4 *tp = bvh.tris + 3 * (size_t)first;
                 float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
-                const bool acc = intersect_triangle<kCull>(o, d, a, b, c, slot, hit);
-                if (acc && hit.t < t_exit) {
-                    finished = true;
-                    break;
+                for (int k = 0; k < count; ++k) {
+                    float4 na = a, nb = b, nc = c;
+                    if (k + 1 < count) {
+                        na = __ldg(tp + 3 * (k + 1));
+                        nb = __ldg(tp + 3 * (k + 1) + 1);
+                        nc = __ldg(tp + 3 * (k + 1) + 2);
+                    }
+                    const bool acc = intersect_triangle<kCull>(o, d, a, b, c, first + k, hit);
+                    if (acc && hit.t < t_exit) {
+                        finished = true;
+                        break;
+                    }
+                    a = na;
+                    b = nb;
+                    c = nc;
+                }
+            } else if (!kPipe) {
+                for (int k = 0; k < count; ++k) {
+                    const int slot = first + k;
+                    const float4 *tp = bvh.tris + 3 * (size_t)slot;
+                    float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                    const bool acc = intersect_triangle<kCull>(o, d, a, b, c, slot, hit);
+                    if (acc && hit.t < t_exit) {
+                        finished = true;
+                        break;
+                    }
                 }
             }
             if (!finished) {
