@@ -379,8 +379,9 @@ def batch_leg(ctx, stream):
     """Batched persistent wavefront (the multi-view batch workload): 64 orbit views of
     the Cornell box (radius 3, elevation U[-30, 30] deg, seeded), 512x512,
     16 spp, depth 12, all views in shared wavefronts with a CUDA graph per
-    pass and an autotuned wavefront size and stage block size, against 64 sequential single-view
-    renders of the same cameras."""
+    pass and an autotuned wavefront size, stage block size and stage
+    traversal (stack placement, node format), against 64 sequential
+    single-view renders of the same cameras with the same settings."""
     import tempfile
 
     import torch
@@ -419,7 +420,9 @@ def batch_leg(ctx, stream):
             "batched_msamples_per_s": round(samples / (bms * 1e-3) / 1e6, 1),
             "sequential_msamples_per_s": round(samples / (sms * 1e-3) / 1e6, 1),
             "paths_per_pass": tune["paths_per_pass"], "stage_block": tune["stage_block"],
-            "autotune_ms": tune.get("timings_ms"), "autotune_block_ms": tune.get("block_timings_ms")}
+            "stage_traversal": tune["stage_traversal"],
+            "autotune_ms": tune.get("timings_ms"), "autotune_block_ms": tune.get("block_timings_ms"),
+            "autotune_traversal_ms": tune.get("traversal_timings_ms")}
 
 
 def serve_leg(ctx, quick=False):

@@ -72,6 +72,7 @@ class RenderParams(C.Structure):
         ("spp_per_pass", C.c_int32),
         ("paths_per_pass", C.c_int32),
         ("stage_block", C.c_int32),
+        ("stage_traversal", C.c_int32),
     ]
 
 

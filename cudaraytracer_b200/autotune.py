@@ -1,12 +1,14 @@
 """Autotuner for the batched renderer: picks the wavefront size (paths per
-pass, the queue capacity) and then the thread-block size of the
-extend/shade/shadow stage kernels for Scene.render_views, by timing a short
-probe render of each candidate with CUDA events, and caches the choice in a
-JSON file keyed by GPU name, scene triangle count (power-of-two bucket),
-image size and view count. The traversal stack depth (a compile-time array
-of 64 entries; only the entries a ray uses are touched) and the BVH node
-width (binary; a 4-wide collapse measured slower) are not tuned. No
-counterpart in the reference (its wavefront is one frame of one view)."""
+pass, the queue capacity), then the thread-block size of the
+extend/shade/shadow stage kernels, then their BVH traversal (stack depth
+and placement: a 64-entry stack in local memory or the top 8 entries in
+shared memory; node width: 64 B float child boxes or 32 B 16-bit quantised
+ones) for Scene.render_views, by timing a short probe render of each
+candidate with CUDA events, and caches the choice in a JSON file keyed by
+GPU name, scene triangle count (power-of-two bucket), image size and view
+count. The branching factor stays binary (the 4- and 8-wide collapses
+measured slower). No counterpart in the reference (its wavefront is one
+frame of one view)."""
 from __future__ import annotations
 
 import json
@@ -15,6 +17,9 @@ import os
 
 DEFAULT_CANDIDATES = (1 << 20, 2 << 20, 4 << 20, 8 << 20, 16 << 20)
 BLOCK_CANDIDATES = (64, 128, 256)
+# crt_render_params.stage_traversal: CRT_STAGE_LOCAL, _SHARED, _LOCAL_QUANT,
+# _SHARED_QUANT (include/crt.h)
+TRAVERSAL_CANDIDATES = {1: "local", 2: "shared", 3: "local-quant", 4: "shared-quant"}
 
 
 def cache_key(scene, n_views: int) -> str:
@@ -28,12 +33,14 @@ def cache_key(scene, n_views: int) -> str:
 
 
 def autotune_paths_per_pass(scene, cameras, probe_spp: int = 1, candidates=DEFAULT_CANDIDATES,
-                            cache_path: str | None = None, blocks=BLOCK_CANDIDATES) -> dict:
+                            cache_path: str | None = None, blocks=BLOCK_CANDIDATES,
+                            traversals=tuple(TRAVERSAL_CANDIDATES)) -> dict:
     """Times render_views(cameras, probe_spp) for each candidate wavefront
-    size (at the scene's current stage block size), then for each stage
-    block size at the fastest wavefront size; sets the winners on the scene
-    and returns {"paths_per_pass", "stage_block", "timings_ms",
-    "block_timings_ms", "cached"}."""
+    size (at the scene's current stage block size and traversal), then for
+    each stage block size at the fastest wavefront size, then for each stage
+    traversal at both; sets the winners on the scene and returns
+    {"paths_per_pass", "stage_block", "stage_traversal", "timings_ms",
+    "block_timings_ms", "traversal_timings_ms", "cached"}."""
     import torch
 
     key = cache_key(scene, len(cameras))
@@ -42,7 +49,8 @@ def autotune_paths_per_pass(scene, cameras, probe_spp: int = 1, candidates=DEFAU
             cache = json.load(f)
         if key in cache:
             scene.set_render_params(paths_per_pass=int(cache[key]["paths_per_pass"]),
-                                    stage_block=int(cache[key].get("stage_block", 0)))
+                                    stage_block=int(cache[key].get("stage_block", 0)),
+                                    stage_traversal=int(cache[key].get("stage_traversal", 0)))
             return {**cache[key], "cached": True}
     rp = scene.render_params()
     shape = (len(cameras), rp["height"], rp["width"], 4)
@@ -75,9 +83,17 @@ def autotune_paths_per_pass(scene, cameras, probe_spp: int = 1, candidates=DEFAU
         block_timings[int(b)] = probe_ms()
     best_block = min(block_timings, key=block_timings.get)
     scene.set_render_params(stage_block=best_block)
-    entry = {"paths_per_pass": best, "stage_block": best_block,
+    trav_timings = {}
+    for t in traversals:
+        scene.set_render_params(stage_traversal=int(t))
+        trav_timings[int(t)] = probe_ms()
+    best_trav = min(trav_timings, key=trav_timings.get) if trav_timings else 0
+    scene.set_render_params(stage_traversal=best_trav)
+    entry = {"paths_per_pass": best, "stage_block": best_block, "stage_traversal": best_trav,
              "timings_ms": {str(k): round(v, 3) for k, v in timings.items()},
-             "block_timings_ms": {str(k): round(v, 3) for k, v in block_timings.items()}}
+             "block_timings_ms": {str(k): round(v, 3) for k, v in block_timings.items()},
+             "traversal_timings_ms": {TRAVERSAL_CANDIDATES.get(k, str(k)): round(v, 3)
+                                      for k, v in trav_timings.items()}}
     if cache_path:
         cache = {}
         if os.path.exists(cache_path):

@@ -485,6 +485,7 @@ crt_status crt_get_render_params(const crt_scene *scene, crt_render_params *p) {
         p->spp_per_pass = scene->rp.spp_per_pass;
         p->paths_per_pass = scene->rp.paths_per_pass;
         p->stage_block = scene->rp.stage_block;
+        p->stage_traversal = scene->rp.stage_traversal;
     });
 }
 
@@ -497,6 +498,8 @@ crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p) {
                   CRT_ERR_INVALID, "crt_set_render_params: negative count");
         CRT_CHECK(p->stage_block == 0 || p->stage_block == 64 || p->stage_block == 128 || p->stage_block == 256,
                   CRT_ERR_INVALID, "crt_set_render_params: stage_block must be 0, 64, 128 or 256");
+        CRT_CHECK(p->stage_traversal >= CRT_STAGE_DEFAULT && p->stage_traversal <= CRT_STAGE_SHARED_QUANT,
+                  CRT_ERR_INVALID, "crt_set_render_params: stage_traversal must be 0-4");
         bool resized = p->width != scene->rp.width || p->height != scene->rp.height;
         scene->rp.width = p->width;
         scene->rp.height = p->height;
@@ -508,6 +511,7 @@ crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p) {
         scene->rp.spp_per_pass = p->spp_per_pass;
         scene->rp.paths_per_pass = p->paths_per_pass;
         scene->rp.stage_block = p->stage_block;
+        scene->rp.stage_traversal = p->stage_traversal;
         if (resized) {
             scene->cam.width = p->width;
             scene->cam.height = p->height;

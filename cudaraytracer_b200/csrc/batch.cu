@@ -100,7 +100,7 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
         for (int k = 0; k < 5; ++k) q[j].p[k] = sc.wf.q[j][k];
     ShadowView sh{{sc.wf.shadow[0], sc.wf.shadow[1], sc.wf.shadow[2], sc.wf.shadow[3]}};
     const int blk = sc.rp.block();
-    const int smem = stage_traversal();
+    const int smem = sc.rp.traversal();
     const int g_ext = persistent_grid((const void *)k_extend, blk);
     const int g_sh = persistent_grid((const void *)k_shade, blk);
     const int g_sd = persistent_grid((const void *)k_shadow, blk);

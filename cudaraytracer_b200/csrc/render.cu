@@ -521,7 +521,7 @@ __global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, cons
     }
 }
 
-int stage_traversal() {
+int stage_traversal_env() {
     const char *e = getenv("CRT_STAGE_TRAVERSAL");
     if (!e) return kStageTraversalDefault;
     const std::string v(e);
@@ -530,6 +530,11 @@ int stage_traversal() {
     if (v == "local-quant") return kStageLocalQuant;
     if (v == "shared-quant") return kStageSharedQuant;
     return kStageTraversalDefault;
+}
+
+int RenderParams::traversal() const {
+    // CRT_STAGE_LOCAL..CRT_STAGE_SHARED_QUANT are the StageTraversal modes + 1
+    return stage_traversal > 0 ? stage_traversal - 1 : stage_traversal_env();
 }
 
 int persistent_grid(const void *kernel, int block) {
@@ -568,7 +573,7 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
         for (int k = 0; k < 5; ++k) q[j].p[k] = wf.q[j][k];
     ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
     const int blk = rp.block();
-    const int smem = stage_traversal();
+    const int smem = rp.traversal();
     const int g_ext = persistent_grid((const void *)k_extend, blk);
     const int mb = shade_min_blocks(blk);
     const void *shade_fn = mb == 4    ? (const void *)k_shade_mb<4>

@@ -16,7 +16,10 @@ struct RenderParams {
     int spp_per_pass = 0;     // samples per wavefront; 0 = automatic
     int paths_per_pass = 0;   // paths per wavefront of multi-view batches; 0 = 8M
     int stage_block = 0;      // threads per block of the wavefront stage kernels; 0 = 128
+    int stage_traversal = 0;  // CRT_STAGE_*: 0 = stage_traversal_env() (environment or default)
     int block() const { return stage_block ? stage_block : 128; }
+    // The StageTraversal mode (render_kernels.cuh) of the extend/shadow stages.
+    int traversal() const;
 };
 
 // Device-resident render data of a scene (everything but the BVH).

@@ -69,9 +69,10 @@ enum StageTraversal : int {
 };
 constexpr int kStageTraversalDefault = kStageLocal;
 
-// The mode for the next launches: kStageTraversalDefault, or the one named
-// by CRT_STAGE_TRAVERSAL (local, shared, local-quant, shared-quant).
-int stage_traversal();
+// The mode for launches whose render parameters leave it open (and for the
+// server): kStageTraversalDefault, or the one named by CRT_STAGE_TRAVERSAL
+// (local, shared, local-quant, shared-quant).
+int stage_traversal_env();
 
 #ifdef __CUDACC__
 // Closest hit and Light::Visible in the given mode (`sst` is the lane's

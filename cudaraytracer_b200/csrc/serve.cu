@@ -421,7 +421,7 @@ struct crt_server {
             for (int c = 0; c < 5; ++c) q[j].p[c] = wf.q[j][c];
         ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
         ks_raygen<<<(n + 255) / 256, 256, 0, stream>>>(d_reqs, ds, nseg, n, q[0], wf.counters);
-        const int smem = stage_traversal();
+        const int smem = stage_traversal_env();
         for (int b = 0; b < max_b; ++b) {
             const int in = b & 1, out = 1 - in;
             ks_extend<<<g_ext, 128, 0, stream>>>(d_scenes, q[in], wf.counters + in, wf.hits, wf.counters, out, smem);

@@ -203,7 +203,17 @@ typedef struct crt_render_params {
     int32_t paths_per_pass;   /* paths per wavefront of crt_render_views; 0 = 8M */
     int32_t stage_block;      /* threads per block of the extend/shade/shadow wavefront stages
                                  (64, 128 or 256); 0 = 128 */
+    int32_t stage_traversal;  /* BVH traversal of the extend and shadow stages: 0 = library
+                                 default, else one of CRT_STAGE_* below */
 } crt_render_params;
+
+/* crt_render_params.stage_traversal: where each path's traversal stack lives
+ * and which node layout it reads. */
+#define CRT_STAGE_DEFAULT 0       /* CRT_STAGE_TRAVERSAL from the environment, else LOCAL */
+#define CRT_STAGE_LOCAL 1         /* 64-entry stack in local memory, 64 B float nodes */
+#define CRT_STAGE_SHARED 2        /* top 8 entries in shared memory, 64 B float nodes */
+#define CRT_STAGE_LOCAL_QUANT 3   /* local stack, 32 B nodes with 16-bit quantised boxes */
+#define CRT_STAGE_SHARED_QUANT 4  /* shared short stack, 32 B quantised nodes */
 
 crt_status crt_get_render_params(const crt_scene *scene, crt_render_params *p);
 crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p);
