@@ -43,6 +43,16 @@ struct SceneView {
 #ifdef __CUDACC__
 
 // --- small vector helpers (plain float arithmetic) --------------------------
+// The large shading functions the shade stage calls from two or three
+// sites each: inlined (default) or, with CRT_SHADE_NOINLINE, compiled once
+// per translation unit and called (a smaller instruction footprint for the
+// fetch-bound shade kernels, against call overhead).
+#ifdef CRT_SHADE_NOINLINE
+#define CRT_SHADE_FN static __device__ __noinline__
+#else
+#define CRT_SHADE_FN __device__ __forceinline__
+#endif
+
 __device__ __forceinline__ V3 operator+(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
 __device__ __forceinline__ V3 operator-(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
 __device__ __forceinline__ V3 operator-(V3 a) { return V3{-a.x, -a.y, -a.z}; }
@@ -118,7 +128,7 @@ __device__ __forceinline__ float fresnel_dielectric(float cosI, float etaI, floa
 }
 
 // Fresnel (material.cu:116-119): reflectance for cos = n.wi, eta 1 -> ior.
-__device__ __forceinline__ float fresnel_mat(const DMaterial &m, V3 wi, V3 n) {
+CRT_SHADE_FN float fresnel_mat(const DMaterial &m, V3 wi, V3 n) {
     return fresnel_dielectric(dot(n, wi), 1.0f, m.ior);
 }
 
@@ -133,7 +143,7 @@ __device__ __forceinline__ bool refract_dir(V3 incident, V3 n, float eta, V3 &ou
 }
 
 // SampleDielectric (material.cu:155-192). wi points toward the viewer.
-__device__ __forceinline__ void sample_dielectric(const DMaterial &m, V3 wi, V3 normal, V3 &wo, float &pdf, V3 &weight,
+CRT_SHADE_FN void sample_dielectric(const DMaterial &m, V3 wi, V3 normal, V3 &wo, float &pdf, V3 &weight,
                                                   Pcg32 &rng) {
     V3 incident = -normalized(wi);
     V3 on = normalized(normal);
@@ -263,17 +273,17 @@ __device__ __forceinline__ void sample_pbr(const DMaterial &m, V3 wi, V3 n, V3 &
 }
 
 // Material::Evaluate / Pdf / Sample dispatch (material.cu:14-64).
-__device__ __forceinline__ V3 mat_eval(const DMaterial &m, V3 wi, V3 n, V3 wo) {
+CRT_SHADE_FN V3 mat_eval(const DMaterial &m, V3 wi, V3 n, V3 wo) {
     if (m.type == MAT_PBR) return eval_pbr(m, wi, n, wo);
     if (m.type == MAT_DIELECTRIC) return V3{0.f, 0.f, 0.f};
     return eval_diffuse(m, n, wo);
 }
-__device__ __forceinline__ float mat_pdf(const DMaterial &m, V3 wi, V3 n, V3 wo) {
+CRT_SHADE_FN float mat_pdf(const DMaterial &m, V3 wi, V3 n, V3 wo) {
     if (m.type == MAT_PBR) return pdf_pbr(m, wi, n, wo);
     if (m.type == MAT_DIELECTRIC) return 0.f;
     return pdf_diffuse(n, wo);
 }
-__device__ __forceinline__ void mat_sample(const DMaterial &m, V3 wi, V3 n, V3 &wo, float &pdf, Pcg32 &rng) {
+CRT_SHADE_FN void mat_sample(const DMaterial &m, V3 wi, V3 n, V3 &wo, float &pdf, Pcg32 &rng) {
     if (m.type == MAT_PBR)
         sample_pbr(m, wi, n, wo, pdf, rng);
     else
@@ -327,7 +337,7 @@ __device__ __forceinline__ void env_sample_uv(const EnvView &e, Pcg32 &rng, floa
 
 // Light::Emission for the environment (light.cu:141-155): u = phi/2pi,
 // v = theta/pi, hardware bilinear fetch (wrap u, clamp v).
-__device__ __forceinline__ V3 env_emission(const EnvView &e, V3 wi) {
+CRT_SHADE_FN V3 env_emission(const EnvView &e, V3 wi) {
     float theta = acosf(wi.y);
     float phi = atan2f(wi.x, wi.z);
     if (phi < 0) phi = (float)((double)phi + 2.0 * kPiD);
@@ -361,7 +371,7 @@ __device__ __forceinline__ void sample_triangle(const SceneView &s, int prim, Pc
 }
 
 // Light::SamplePoint (light.cu:29-41).
-__device__ __forceinline__ void light_sample_point(const SceneView &s, const DLight &L, Pcg32 &rng,
+CRT_SHADE_FN void light_sample_point(const SceneView &s, const DLight &L, Pcg32 &rng,
                                                    LightSample &ls) {
     if (L.type == LIGHT_AREA) {
         // SampleAreaLight (light.cu:60-69): triangle uniform by index.
@@ -383,7 +393,7 @@ __device__ __forceinline__ void light_sample_point(const SceneView &s, const DLi
 }
 
 // Light::SampleSolidAnglePDF (light.cu:50-58) with origin = the shading point.
-__device__ __forceinline__ float light_solid_angle_pdf(const SceneView &s, const DLight &L, V3 origin, V3 lp,
+CRT_SHADE_FN float light_solid_angle_pdf(const SceneView &s, const DLight &L, V3 origin, V3 lp,
                                                        V3 ln) {
     if (L.type == LIGHT_AREA) {
         // SampleAreaLightSolidAnglePDF (light.cu:79-89)
@@ -403,7 +413,7 @@ __device__ __forceinline__ float light_solid_angle_pdf(const SceneView &s, const
 }
 
 // Light::Emission (light.cu:141-155).
-__device__ __forceinline__ V3 light_emission(const SceneView &s, const DLight &L, V3 wi) {
+CRT_SHADE_FN V3 light_emission(const SceneView &s, const DLight &L, V3 wi) {
     if (L.type == LIGHT_ENV) return env_emission(s.env, wi);
     return ld3(L.emission);
 }
