@@ -30,7 +30,11 @@ __global__ void k_raygen_views(const CamView *cams, int n_views, StepParams sp, 
     const int64_t left = total - base;
     const int n = (int)(left < chunk ? (left > 0 ? left : 0) : chunk);
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) counters[0] = n;
+    if (i == 0) {
+        counters[0] = n;
+        counters[kHitCounter] = 0;
+        counters[kMissCounter] = 0;
+    }
     if (i >= n) return;
     const int64_t g = base + i;
     const int64_t per_view = total / n_views;  // spp * pixels
@@ -99,6 +103,7 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
     for (int j = 0; j < 2; ++j)
         for (int k = 0; k < 5; ++k) q[j].p[k] = sc.wf.q[j][k];
     ShadowView sh{{sc.wf.shadow[0], sc.wf.shadow[1], sc.wf.shadow[2], sc.wf.shadow[3]}};
+    const ShadeOrder ord{sc.wf.order, (int)sc.wf.cap};
     const int blk = sc.rp.block();
     const int smem = sc.rp.traversal();
     const int g_ext = persistent_grid((const void *)k_extend, blk);
@@ -119,9 +124,9 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
             StepParams bp = sp;
             bp.bounce = b;
             k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], sc.wf.counters + in, sc.wf.hits, sc.wf.counters, out,
-                                           smem);
+                                           smem, ord);
             k_shade<<<g_sh, blk, 0, s>>>(view, bp, q[in], sc.wf.hits, sc.wf.counters + in, q[out], sc.wf.counters,
-                                         out, sh, sc.wf.term[0], sc.wf.term[1], av);
+                                         out, sh, sc.wf.term[0], sc.wf.term[1], av, ord);
             k_shadow<<<g_sd, blk, 0, s>>>(view.bvh, sh, sc.wf.counters, q[out], sc.wf.term[0], sc.wf.term[1], av,
                                           smem);
         }

@@ -318,6 +318,7 @@ void Wavefront::reserve(size_t paths) {
     CRT_CUDA(cudaMalloc(&hits, paths * sizeof(float4)));
     for (int k = 0; k < 4; ++k) CRT_CUDA(cudaMalloc(&shadow[k], paths * sizeof(float4)));
     for (int k = 0; k < 2; ++k) CRT_CUDA(cudaMalloc(&term[k], paths * sizeof(float4)));
+    CRT_CUDA(cudaMalloc(&order, paths * sizeof(int)));
     cap = paths;
 }
 
@@ -335,6 +336,7 @@ void Wavefront::release_paths() {
         if (shadow[k]) cudaFree(shadow[k]), shadow[k] = nullptr;
     for (int k = 0; k < 2; ++k)
         if (term[k]) cudaFree(term[k]), term[k] = nullptr;
+    if (order) cudaFree(order), order = nullptr;
     cap = 0;
 }
 
@@ -346,7 +348,11 @@ void Wavefront::release_paths() {
 // camera.cu:27-35): jitter (u, v), pixel (i + u, j + v) from the bottom-left.
 __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *counters) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) counters[0] = n;
+    if (i == 0) {
+        counters[0] = n;
+        counters[kHitCounter] = 0;
+        counters[kMissCounter] = 0;
+    }
     if (i >= n) return;
     uint32_t pixel = (uint32_t)(i % sp.pixels);
     uint32_t sample = (uint32_t)(sp.first_sample + i / sp.pixels);
@@ -368,9 +374,10 @@ __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *co
 }
 
 // Extend: closest hit of every live path (TraceRay, renderer.cuh:124-130:
-// tMin 0, closest starts at 1e8). Also clears the next bounce's counters.
+// tMin 0, closest starts at 1e8), and the path's place in the shade order.
+// Also clears the next bounce's queue counters.
 __global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters,
-                                                int out_idx, int mode) {
+                                                int out_idx, int mode, ShadeOrder ord) {
     __shared__ unsigned s_stack[kStageShort * kStageMaxBlock];
     ShortStack<kStageShort> st;
     st.col = s_stack + threadIdx.x;
@@ -387,15 +394,21 @@ __global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const 
         const V3 o{a.x, a.y, a.z}, d{b.x, b.y, b.z};
         Hit h = stage_closest<false>(bvh, st, mode, o, d, 0.f, kTriTMax);
         hits[i] = make_float4(h.t, __int_as_float(h.slot), h.b1, h.b2);
+        const bool hit = h.slot >= 0;
+        const int hs = warp_alloc(&counters[kHitCounter], hit);
+        const int ms = warp_alloc(&counters[kMissCounter], !hit);
+        ord.idx[hit ? hs : ord.cap - 1 - ms] = i;
     }
 }
 
 __device__ __forceinline__ void shade_body(const SceneView &s, const StepParams &sp, const QueueView &qin,
                                            const float4 *hits, const int *n_in, const QueueView &qout, int *counters,
                                            int out_idx, const ShadowView &sh, float4 *term0, float4 *term1,
-                                           const AccumView &acc) {
-    const int n = *n_in;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+                                           const AccumView &acc, const ShadeOrder &ord) {
+    const int n = *n_in, nhit = counters[kHitCounter];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        // hits first, then misses (each in the order extend placed them)
+        const int i = __ldg(ord.idx + (t < nhit ? t : ord.cap - 1 - (t - nhit)));
         PathState ps = load_path(qin, i);
         float4 hr = hits[i];
         Hit h;
@@ -449,8 +462,9 @@ __device__ __forceinline__ void shade_body(const SceneView &s, const StepParams 
 // 5% faster per 1080p frame).
 __global__ void __launch_bounds__(256, 4) k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits,
                                                   const int *n_in, QueueView qout, int *counters, int out_idx,
-                                                  ShadowView sh, float4 *term0, float4 *term1, AccumView acc) {
-    shade_body(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc);
+                                                  ShadowView sh, float4 *term0, float4 *term1, AccumView acc,
+                                                  ShadeOrder ord) {
+    shade_body(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc, ord);
 }
 
 // The same compiled for kMinBlocks resident 128-thread blocks per SM (4: no
@@ -460,8 +474,9 @@ template <int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) k_shade_mb(SceneView s, StepParams sp, QueueView qin,
                                                                const float4 *hits, const int *n_in, QueueView qout,
                                                                int *counters, int out_idx, ShadowView sh,
-                                                               float4 *term0, float4 *term1, AccumView acc) {
-    shade_body(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc);
+                                                               float4 *term0, float4 *term1, AccumView acc,
+                                                               ShadeOrder ord) {
+    shade_body(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc, ord);
 }
 
 static int shade_min_blocks(int block) {
@@ -473,16 +488,19 @@ static int shade_min_blocks(int block) {
 // Shadow: Light::Visible for each deferred NEE sample; a visible sample's
 // contribution joins its path's direct or indirect radiance; a path that
 // already terminated is then added to its pixel.
-__global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueView qout,
+__global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, int *counters, QueueView qout,
                                                 float4 *term0, float4 *term1, AccumView acc, int mode) {
     __shared__ unsigned s_stack[kStageShort * kStageMaxBlock];
     ShortStack<kStageShort> st;
     st.col = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     const int n = counters[2];
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        atomicAdd(reinterpret_cast<unsigned long long *>(const_cast<int *>(counters) + kShadowRaysCounter),
-                  (unsigned long long)n);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long *>(counters + kShadowRaysCounter), (unsigned long long)n);
+        // the shade order of the next bounce starts empty (shade has read it)
+        counters[kHitCounter] = 0;
+        counters[kMissCounter] = 0;
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = sh.r[0][i], b = sh.r[1][i], c = sh.r[2][i], d = sh.r[3][i];
         const V3 hp{a.x, a.y, a.z}, hn{a.w, b.x, b.y}, lp{b.z, b.w, c.x}, ln{c.y, c.z, c.w};
@@ -572,6 +590,7 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
     for (int j = 0; j < 2; ++j)
         for (int k = 0; k < 5; ++k) q[j].p[k] = wf.q[j][k];
     ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
+    const ShadeOrder ord{wf.order, (int)wf.cap};
     const int blk = rp.block();
     const int smem = rp.traversal();
     const int g_ext = persistent_grid((const void *)k_extend, blk);
@@ -598,19 +617,20 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
         for (int b = 0; b < rp.max_bounces; ++b) {
             int in = b & 1, out = 1 - in;
             sp.bounce = b;
-            k_extend<<<g_ext, blk, 0, stream>>>(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out, smem);
+            k_extend<<<g_ext, blk, 0, stream>>>(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out, smem,
+                                                ord);
             if (mb == 4)
                 k_shade_mb<4><<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out],
-                                                        wf.counters, out, sh, wf.term[0], wf.term[1], av);
+                                                        wf.counters, out, sh, wf.term[0], wf.term[1], av, ord);
             else if (mb == 6)
                 k_shade_mb<6><<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out],
-                                                        wf.counters, out, sh, wf.term[0], wf.term[1], av);
+                                                        wf.counters, out, sh, wf.term[0], wf.term[1], av, ord);
             else if (mb == 10)
                 k_shade_mb<10><<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out],
-                                                         wf.counters, out, sh, wf.term[0], wf.term[1], av);
+                                                         wf.counters, out, sh, wf.term[0], wf.term[1], av, ord);
             else
                 k_shade<<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out], wf.counters,
-                                                  out, sh, wf.term[0], wf.term[1], av);
+                                                  out, sh, wf.term[0], wf.term[1], av, ord);
             k_shadow<<<g_sd, blk, 0, stream>>>(view.bvh, sh, wf.counters, q[out], wf.term[0], wf.term[1], av, smem);
             launches += 3;
         }

@@ -42,11 +42,14 @@ struct RenderData {
 };
 
 // Path-state buffers of one wavefront, reused across renders.
-// Words of a wavefront's counter block: queue counts in [0, 4), and two
-// 64-bit running totals of the rays the stage kernels traced (extend rays
-// at word 8, shadow rays at word 10; the subsurface probe rays that the
-// shade stage traces inline are not counted).
+// Words of a wavefront's counter block: queue counts in [0, 4), the counts
+// of the bounce's hit and miss paths in the shade order at kHitCounter and
+// kMissCounter, and two 64-bit running totals of the rays the stage kernels
+// traced (extend rays at word 8, shadow rays at word 10; the subsurface
+// probe rays that the shade stage traces inline are not counted).
 constexpr int kWavefrontCounters = 16;
+constexpr int kHitCounter = 4;
+constexpr int kMissCounter = 5;
 constexpr int kExtendRaysCounter = 8;
 constexpr int kShadowRaysCounter = 10;
 
@@ -56,7 +59,8 @@ struct Wavefront {
     float4 *hits = nullptr;    // (t, slot, b1, b2)
     float4 *shadow[4] = {};    // shadow-test records
     float4 *term[2] = {};      // terminated paths waiting for their shadow test
-    int *counters = nullptr;   // [in0, in1, shadow, term] per bounce parity; ray counters at 8 and 10
+    int *order = nullptr;      // shade order: hit paths' queue indices from the front, misses' from the back
+    int *counters = nullptr;   // [in0, in1, shadow, term] per bounce parity, hit/miss counts; ray counters
     void reserve(size_t paths);
     void release();
     void release_paths();

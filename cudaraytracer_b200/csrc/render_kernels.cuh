@@ -41,13 +41,26 @@ struct ShadowView {
     float4 *r[4];
 };
 
+// The order in which the shade stage visits a bounce's paths, written by
+// the extend stage: the queue indices of paths that hit a triangle in
+// idx[0 .. hits) and of paths that missed in idx[cap - misses .. cap), the
+// two counts at kHitCounter and kMissCounter of the counter block (reset by
+// raygen and by the shadow stage for the next bounce). Misses only add the
+// environment, so most warps of a sparse scene's first bounce are
+// miss-only and the hit warps run the material code with full lanes.
+struct ShadeOrder {
+    int *idx;
+    int cap;
+};
+
 __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *counters);
 __global__ void k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters, int out_idx,
-                         int mode);
+                         int mode, ShadeOrder ord);
 __global__ void k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits, const int *n_in, QueueView qout,
-                        int *counters, int out_idx, ShadowView sh, float4 *term0, float4 *term1, AccumView acc);
-__global__ void k_shadow(BvhView bvh, ShadowView sh, const int *counters, QueueView qout, float4 *term0,
-                         float4 *term1, AccumView acc, int mode);
+                        int *counters, int out_idx, ShadowView sh, float4 *term0, float4 *term1, AccumView acc,
+                        ShadeOrder ord);
+__global__ void k_shadow(BvhView bvh, ShadowView sh, int *counters, QueueView qout, float4 *term0, float4 *term1,
+                         AccumView acc, int mode);
 
 // Blocks per grid for a persistent launch of `kernel` (all SMs at full
 // occupancy).

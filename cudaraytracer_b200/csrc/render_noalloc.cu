@@ -11,9 +11,9 @@
 // point instead runs the same stage kernels over a fixed scratch area that
 // is part of the library's device image.
 //
-// The scratch is a file-scope __device__ array of kNoAllocBytes (17.8 MB)
+// The scratch is a file-scope __device__ array of kNoAllocBytes (18.1 MB)
 // holding the path queues, hit records, shadow records, terminated-path
-// records and counters for at most kNoAllocMaxPaths = 65,536 paths per
+// records, the shade order and counters for at most kNoAllocMaxPaths = 65,536 paths per
 // wavefront (pixels x samples per pass). Every GPU that loads the library
 // holds this array until the process exits. Images with more than 65,536
 // pixels are rejected with CRT_ERR_CAPACITY. The caller still provides the
@@ -24,8 +24,9 @@
 // so that first call must come before any stream capture on that device.
 // All calls share the one array and it keeps the previous call's contents.
 // Nothing stale is read: the stage kernels set every queue counter before
-// it is used (k_raygen the input count, k_extend the next bounce's output,
-// shadow and terminal counts), and the counter block is also zeroed at the
+// it is used (k_raygen the input count and the shade-order counts, k_extend
+// the next bounce's output, shadow and terminal counts, k_shadow the next
+// bounce's shade-order counts), and the counter block is also zeroed at the
 // start of every call as a defensive measure. Calls whose GPU work overlaps
 // (two streams, two host threads, two scenes) race on the array, so they
 // must be ordered by the caller.
@@ -42,10 +43,12 @@ namespace crt {
 namespace {
 
 constexpr size_t kNoAllocMaxPaths = 65536;
-// per path: 2 queues x 5 float4 + hit + 4 shadow + 2 terminal float4 = 272 B
+// per path: 2 queues x 5 float4 + hit + 4 shadow + 2 terminal float4 = 272 B,
+// and a 4 B shade-order entry
 constexpr size_t kPlane = kNoAllocMaxPaths * sizeof(float4);
 constexpr size_t kCounterBytes = 256;
-constexpr size_t kNoAllocBytes = 17 * kPlane + kCounterBytes;
+constexpr size_t kOrderBytes = kNoAllocMaxPaths * sizeof(int);
+constexpr size_t kNoAllocBytes = 17 * kPlane + kCounterBytes + kOrderBytes;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
@@ -92,6 +95,7 @@ extern "C" crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_
         float4 *plane[17];
         for (int k = 0; k < 17; ++k) plane[k] = reinterpret_cast<float4 *>(base + k * kPlane);
         int *counters = reinterpret_cast<int *>(base + 17 * kPlane);
+        const ShadeOrder ord{reinterpret_cast<int *>(base + 17 * kPlane + kCounterBytes), (int)kNoAllocMaxPaths};
         QueueView q[2];
         for (int k = 0; k < 5; ++k) {
             q[0].p[k] = plane[k];
@@ -136,9 +140,9 @@ extern "C" crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_
             for (int b = 0; b < rp.max_bounces; ++b) {
                 const int in = b & 1, out = 1 - in;
                 sp.bounce = b;
-                k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], counters + in, hits, counters, out, smem);
+                k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], counters + in, hits, counters, out, smem, ord);
                 k_shade<<<g_sh, blk, 0, s>>>(view, sp, q[in], hits, counters + in, q[out], counters, out, sh, term0,
-                                            term1, av);
+                                            term1, av, ord);
                 k_shadow<<<g_sd, blk, 0, s>>>(view.bvh, sh, counters, q[out], term0, term1, av, smem);
             }
             CRT_CUDA(cudaGetLastError());

@@ -53,7 +53,11 @@ __device__ __forceinline__ uint32_t path_tag(const QueueView &q, int i) { return
 // camera.cu:27-35) for the request that owns wavefront entry i.
 __global__ void ks_raygen(const ReqDesc *reqs, const Segment *segs, int nseg, int n, QueueView q, int *counters) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) counters[0] = n;
+    if (i == 0) {
+        counters[0] = n;
+        counters[kHitCounter] = 0;
+        counters[kMissCounter] = 0;
+    }
     if (i >= n) return;
     int lo = 0, hi = nseg - 1;
     while (lo < hi) {
@@ -87,7 +91,7 @@ __global__ void ks_raygen(const ReqDesc *reqs, const Segment *segs, int nseg, in
 }
 
 __global__ void __launch_bounds__(128) ks_extend(const SceneView *scenes, QueueView q, const int *n_in, float4 *hits,
-                                                 int *counters, int out_idx, int mode) {
+                                                 int *counters, int out_idx, int mode, ShadeOrder ord) {
     __shared__ unsigned s_stack[kStageShort * 128];
     ShortStack<kStageShort> st;
     st.col = s_stack + threadIdx.x;
@@ -104,6 +108,10 @@ __global__ void __launch_bounds__(128) ks_extend(const SceneView *scenes, QueueV
         const V3 o{a.x, a.y, a.z}, d{b.x, b.y, b.z};
         Hit h = stage_closest<false>(bvh, st, mode, o, d, 0.f, kTriTMax);
         hits[i] = make_float4(h.t, __int_as_float(h.slot), h.b1, h.b2);
+        const bool hit = h.slot >= 0;
+        const int hs = warp_alloc(&counters[kHitCounter], hit);
+        const int ms = warp_alloc(&counters[kMissCounter], !hit);
+        ord.idx[hit ? hs : ord.cap - 1 - ms] = i;  // the shade order (render_kernels.cuh)
     }
 }
 
@@ -115,9 +123,10 @@ __global__ void __launch_bounds__(128) ks_extend(const SceneView *scenes, QueueV
 __global__ void __launch_bounds__(128, 8) ks_shade(const SceneView *scenes, const ReqDesc *reqs, int bounce,
                                                 QueueView qin, const float4 *hits, const int *n_in, QueueView qout,
                                                 int *counters, int out_idx, ShadowView sh, float4 *term0,
-                                                float4 *term1) {
-    const int n = *n_in;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+                                                float4 *term1, ShadeOrder ord) {
+    const int n = *n_in, nhit = counters[kHitCounter];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int i = __ldg(ord.idx + (t < nhit ? t : ord.cap - 1 - (t - nhit)));  // hits, then misses
         PathState ps = load_path(qin, i);
         const uint32_t tag = path_tag(qin, i);
         const SceneView &s = scenes[tag >> kSlotBits];
@@ -178,13 +187,17 @@ __global__ void __launch_bounds__(128, 8) ks_shade(const SceneView *scenes, cons
 // Light::Visible for each deferred NEE sample against the scene of the path
 // it belongs to; then as k_shadow in render.cu.
 __global__ void __launch_bounds__(128) ks_shadow(const SceneView *scenes, const ReqDesc *reqs, ShadowView sh,
-                                                 const int *counters, QueueView qout, float4 *term0, float4 *term1,
+                                                 int *counters, QueueView qout, float4 *term0, float4 *term1,
                                                  int mode) {
     __shared__ unsigned s_stack[kStageShort * 128];
     ShortStack<kStageShort> st;
     st.col = s_stack + threadIdx.x;
     st.stride = blockDim.x;
     const int n = counters[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counters[kHitCounter] = 0;  // the next bounce's shade order starts empty
+        counters[kMissCounter] = 0;
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 d = sh.r[3][i];
         uint32_t target = __float_as_uint(d.w);
@@ -244,7 +257,9 @@ size_t scene_device_bytes(const Scene &sc) {
     return b;
 }
 
-constexpr size_t kWavefrontBytesPerPath = 2 * 5 * 16 + 16 + 4 * 16 + 2 * 16;
+// Per wavefront path: two queues of 5 float4, the hit record, 4 shadow and
+// 2 terminal float4, and the shade-order entry.
+constexpr size_t kWavefrontBytesPerPath = 2 * 5 * 16 + 16 + 4 * 16 + 2 * 16 + 4;
 
 }  // namespace
 }  // namespace crt
@@ -420,13 +435,15 @@ struct crt_server {
         for (int j = 0; j < 2; ++j)
             for (int c = 0; c < 5; ++c) q[j].p[c] = wf.q[j][c];
         ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
+        const ShadeOrder ord{wf.order, (int)wf.cap};
         ks_raygen<<<(n + 255) / 256, 256, 0, stream>>>(d_reqs, ds, nseg, n, q[0], wf.counters);
         const int smem = stage_traversal_env();
         for (int b = 0; b < max_b; ++b) {
             const int in = b & 1, out = 1 - in;
-            ks_extend<<<g_ext, 128, 0, stream>>>(d_scenes, q[in], wf.counters + in, wf.hits, wf.counters, out, smem);
+            ks_extend<<<g_ext, 128, 0, stream>>>(d_scenes, q[in], wf.counters + in, wf.hits, wf.counters, out, smem,
+                                                 ord);
             ks_shade<<<g_sh, 128, 0, stream>>>(d_scenes, d_reqs, b, q[in], wf.hits, wf.counters + in, q[out],
-                                               wf.counters, out, sh, wf.term[0], wf.term[1]);
+                                               wf.counters, out, sh, wf.term[0], wf.term[1], ord);
             ks_shadow<<<g_sd, 128, 0, stream>>>(d_scenes, d_reqs, sh, wf.counters, q[out], wf.term[0], wf.term[1],
                                                 smem);
         }
