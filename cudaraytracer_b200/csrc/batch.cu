@@ -108,6 +108,7 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
     const int smem = sc.rp.traversal();
     const int g_ext = persistent_grid((const void *)k_extend, blk);
     const int g_sh = persistent_grid((const void *)k_shade, blk);
+    const int g_sm = persistent_grid((const void *)k_shade_miss, blk);
     const int g_sd = persistent_grid((const void *)k_shadow, blk);
     StepParams sp;
     sp.bounce = 0;
@@ -127,6 +128,8 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
                                            smem, ord);
             k_shade<<<g_sh, blk, 0, s>>>(view, bp, q[in], sc.wf.hits, sc.wf.counters + in, q[out], sc.wf.counters,
                                          out, sh, sc.wf.term[0], sc.wf.term[1], av, ord);
+            k_shade_miss<<<g_sm, blk, 0, s>>>(view, bp, q[in], sc.wf.hits, sc.wf.counters + in, q[out],
+                                              sc.wf.counters, out, sh, sc.wf.term[0], sc.wf.term[1], av, ord);
             k_shadow<<<g_sd, blk, 0, s>>>(view.bvh, sh, sc.wf.counters, q[out], sc.wf.term[0], sc.wf.term[1], av,
                                           smem);
         }

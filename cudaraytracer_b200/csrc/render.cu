@@ -401,13 +401,23 @@ __global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const 
     }
 }
 
+// One shade launch over the hits (the full material code) or over the
+// misses (the environment only) of a bounce's shade order: the two sets in
+// separate kernels keep the misses' warps out of the hit kernel's large
+// instruction footprint.
+enum ShadeSet { kShadeHits = 1, kShadeMisses = 2 };
+
+template <int kSet>
 __device__ __forceinline__ void shade_body(const SceneView &s, const StepParams &sp, const QueueView &qin,
                                            const float4 *hits, const int *n_in, const QueueView &qout, int *counters,
                                            int out_idx, const ShadowView &sh, float4 *term0, float4 *term1,
                                            const AccumView &acc, const ShadeOrder &ord) {
     const int n = *n_in, nhit = counters[kHitCounter];
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        // hits first, then misses (each in the order extend placed them)
+    const int t_end = kSet == kShadeHits ? nhit : n;
+    for (int t = (kSet == kShadeHits ? 0 : nhit) + blockIdx.x * blockDim.x + threadIdx.x; t < t_end;
+         t += gridDim.x * blockDim.x) {
+        // hits in order[0, nhit), misses from the back (each in the order
+        // extend placed them)
         const int i = __ldg(ord.idx + (t < nhit ? t : ord.cap - 1 - (t - nhit)));
         PathState ps = load_path(qin, i);
         float4 hr = hits[i];
@@ -419,7 +429,7 @@ __device__ __forceinline__ void shade_body(const SceneView &s, const StepParams 
         NeeRecord nee;
         nee.valid = false;
         StepResult res;
-        if (h.slot < 0) {
+        if (kSet == kShadeMisses) {
             // miss (IntersectionKernel, renderer.cuh:139-157): environment
             // radiance weighted into direct (first bounce) or indirect.
             if (s.env_light >= 0) {
@@ -464,7 +474,7 @@ __global__ void __launch_bounds__(256, 4) k_shade(SceneView s, StepParams sp, Qu
                                                   const int *n_in, QueueView qout, int *counters, int out_idx,
                                                   ShadowView sh, float4 *term0, float4 *term1, AccumView acc,
                                                   ShadeOrder ord) {
-    shade_body(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc, ord);
+    shade_body<kShadeHits>(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc, ord);
 }
 
 // The same compiled for kMinBlocks resident 128-thread blocks per SM (4: no
@@ -476,7 +486,16 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_shade_mb(SceneView s, StepP
                                                                int *counters, int out_idx, ShadowView sh,
                                                                float4 *term0, float4 *term1, AccumView acc,
                                                                ShadeOrder ord) {
-    shade_body(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc, ord);
+    shade_body<kShadeHits>(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc, ord);
+}
+
+// The misses of the shade order: a small kernel (environment lookup and
+// accumulation), at full occupancy.
+__global__ void __launch_bounds__(256) k_shade_miss(SceneView s, StepParams sp, QueueView qin, const float4 *hits,
+                                                    const int *n_in, QueueView qout, int *counters, int out_idx,
+                                                    ShadowView sh, float4 *term0, float4 *term1, AccumView acc,
+                                                    ShadeOrder ord) {
+    shade_body<kShadeMisses>(s, sp, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, acc, ord);
 }
 
 static int shade_min_blocks(int block) {
@@ -600,6 +619,7 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
                            : mb == 10 ? (const void *)k_shade_mb<10>
                                       : (const void *)k_shade;
     const int g_sh = persistent_grid(shade_fn, blk);
+    const int g_sm = persistent_grid((const void *)k_shade_miss, blk);
     const int g_sd = persistent_grid((const void *)k_shadow, blk);
     int launches = 0;
     for (int done = 0; done < spp; done += per_pass) {
@@ -631,8 +651,10 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
             else
                 k_shade<<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out], wf.counters,
                                                   out, sh, wf.term[0], wf.term[1], av, ord);
+            k_shade_miss<<<g_sm, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out], wf.counters,
+                                                   out, sh, wf.term[0], wf.term[1], av, ord);
             k_shadow<<<g_sd, blk, 0, stream>>>(view.bvh, sh, wf.counters, q[out], wf.term[0], wf.term[1], av, smem);
-            launches += 3;
+            launches += 4;
         }
         CRT_CUDA(cudaGetLastError());
     }

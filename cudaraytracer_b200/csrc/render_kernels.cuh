@@ -56,9 +56,14 @@ struct ShadeOrder {
 __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *counters);
 __global__ void k_extend(BvhView bvh, QueueView q, const int *n_in, float4 *hits, int *counters, int out_idx,
                          int mode, ShadeOrder ord);
+// Shade runs as two launches per bounce: k_shade over the shade order's
+// hits, then k_shade_miss over its misses.
 __global__ void k_shade(SceneView s, StepParams sp, QueueView qin, const float4 *hits, const int *n_in, QueueView qout,
                         int *counters, int out_idx, ShadowView sh, float4 *term0, float4 *term1, AccumView acc,
                         ShadeOrder ord);
+__global__ void k_shade_miss(SceneView s, StepParams sp, QueueView qin, const float4 *hits, const int *n_in,
+                             QueueView qout, int *counters, int out_idx, ShadowView sh, float4 *term0, float4 *term1,
+                             AccumView acc, ShadeOrder ord);
 __global__ void k_shadow(BvhView bvh, ShadowView sh, int *counters, QueueView qout, float4 *term0, float4 *term1,
                          AccumView acc, int mode);
 

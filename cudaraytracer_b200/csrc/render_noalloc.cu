@@ -126,6 +126,7 @@ extern "C" crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_
         const int smem = rp.traversal();
         const int g_ext = persistent_grid((const void *)k_extend, blk);
         const int g_sh = persistent_grid((const void *)k_shade, blk);
+        const int g_sm = persistent_grid((const void *)k_shade_miss, blk);
         const int g_sd = persistent_grid((const void *)k_shadow, blk);
         for (int done = 0; done < spp; done += per_pass) {
             const int n = (int)pixels * std::min(per_pass, spp - done);
@@ -143,6 +144,8 @@ extern "C" crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_
                 k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], counters + in, hits, counters, out, smem, ord);
                 k_shade<<<g_sh, blk, 0, s>>>(view, sp, q[in], hits, counters + in, q[out], counters, out, sh, term0,
                                             term1, av, ord);
+                k_shade_miss<<<g_sm, blk, 0, s>>>(view, sp, q[in], hits, counters + in, q[out], counters, out, sh,
+                                                 term0, term1, av, ord);
                 k_shadow<<<g_sd, blk, 0, s>>>(view.bvh, sh, counters, q[out], term0, term1, av, smem);
             }
             CRT_CUDA(cudaGetLastError());
