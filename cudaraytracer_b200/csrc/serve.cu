@@ -118,15 +118,19 @@ __global__ void __launch_bounds__(128) ks_extend(const SceneView *scenes, QueueV
 // The single-scene shade (k_shade in render.cu) with per-path scene and
 // request. A path still alive after its request's last bounce is dropped
 // with its pending NEE sample, as the reference drops survivors
-// (renderer.cuh:1166-1193). Registers capped for 8 resident blocks per
-// SM, as k_shade.
-__global__ void __launch_bounds__(128, 8) ks_shade(const SceneView *scenes, const ReqDesc *reqs, int bounce,
-                                                QueueView qin, const float4 *hits, const int *n_in, QueueView qout,
-                                                int *counters, int out_idx, ShadowView sh, float4 *term0,
-                                                float4 *term1, ShadeOrder ord) {
+// (renderer.cuh:1166-1193). As in render.cu, one launch over the shade
+// order's hits (ks_shade, registers capped for 8 resident blocks per SM)
+// and one over its misses (ks_shade_miss).
+template <bool kMisses>
+__device__ __forceinline__ void ks_shade_body(const SceneView *scenes, const ReqDesc *reqs, int bounce,
+                                              const QueueView &qin, const float4 *hits, const int *n_in,
+                                              const QueueView &qout, int *counters, int out_idx, const ShadowView &sh,
+                                              float4 *term0, float4 *term1, const ShadeOrder &ord) {
     const int n = *n_in, nhit = counters[kHitCounter];
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const int i = __ldg(ord.idx + (t < nhit ? t : ord.cap - 1 - (t - nhit)));  // hits, then misses
+    const int t_end = kMisses ? n : nhit;
+    for (int t = (kMisses ? nhit : 0) + blockIdx.x * blockDim.x + threadIdx.x; t < t_end;
+         t += gridDim.x * blockDim.x) {
+        const int i = __ldg(ord.idx + (t < nhit ? t : ord.cap - 1 - (t - nhit)));
         PathState ps = load_path(qin, i);
         const uint32_t tag = path_tag(qin, i);
         const SceneView &s = scenes[tag >> kSlotBits];
@@ -144,7 +148,7 @@ __global__ void __launch_bounds__(128, 8) ks_shade(const SceneView *scenes, cons
         NeeRecord nee;
         nee.valid = false;
         StepResult res;
-        if (h.slot < 0) {
+        if (kMisses) {
             if (s.env_light >= 0) {
                 V3 bg = env_emission(s.env, ps.d);
                 if (ps.first)
@@ -182,6 +186,20 @@ __global__ void __launch_bounds__(128, 8) ks_shade(const SceneView *scenes, cons
             sh.r[3][sslot] = make_float4(nee.C.x, nee.C.y, nee.C.z, __uint_as_float(target));
         }
     }
+}
+
+__global__ void __launch_bounds__(128, 8) ks_shade(const SceneView *scenes, const ReqDesc *reqs, int bounce,
+                                                QueueView qin, const float4 *hits, const int *n_in, QueueView qout,
+                                                int *counters, int out_idx, ShadowView sh, float4 *term0,
+                                                float4 *term1, ShadeOrder ord) {
+    ks_shade_body<false>(scenes, reqs, bounce, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, ord);
+}
+
+__global__ void __launch_bounds__(128) ks_shade_miss(const SceneView *scenes, const ReqDesc *reqs, int bounce,
+                                                     QueueView qin, const float4 *hits, const int *n_in,
+                                                     QueueView qout, int *counters, int out_idx, ShadowView sh,
+                                                     float4 *term0, float4 *term1, ShadeOrder ord) {
+    ks_shade_body<true>(scenes, reqs, bounce, qin, hits, n_in, qout, counters, out_idx, sh, term0, term1, ord);
 }
 
 // Light::Visible for each deferred NEE sample against the scene of the path
@@ -301,7 +319,7 @@ struct crt_server {
     std::multimap<size_t, float4 *> pool;  // released accumulator buffers by size
     size_t bytes_scenes = 0, bytes_wavefront = 0, bytes_requests = 0, bytes_pool = 0;
     int64_t n_running = 0, n_done = 0;
-    int g_ext = 0, g_sh = 0, g_sd = 0;
+    int g_ext = 0, g_sh = 0, g_sm = 0, g_sd = 0;
 
     ~crt_server() {
         if (stream) cudaStreamSynchronize(stream);
@@ -444,6 +462,8 @@ struct crt_server {
                                                  ord);
             ks_shade<<<g_sh, 128, 0, stream>>>(d_scenes, d_reqs, b, q[in], wf.hits, wf.counters + in, q[out],
                                                wf.counters, out, sh, wf.term[0], wf.term[1], ord);
+            ks_shade_miss<<<g_sm, 128, 0, stream>>>(d_scenes, d_reqs, b, q[in], wf.hits, wf.counters + in, q[out],
+                                                    wf.counters, out, sh, wf.term[0], wf.term[1], ord);
             ks_shadow<<<g_sd, 128, 0, stream>>>(d_scenes, d_reqs, sh, wf.counters, q[out], wf.term[0], wf.term[1],
                                                 smem);
         }
@@ -508,6 +528,7 @@ extern "C" crt_status crt_server_create(crt_ctx *ctx, const crt_server_config *c
         for (int i = c.max_requests - 1; i >= 0; --i) s->free_slots.push_back(i);
         s->g_ext = persistent_grid((const void *)ks_extend, 128);
         s->g_sh = persistent_grid((const void *)ks_shade, 128);
+        s->g_sm = persistent_grid((const void *)ks_shade_miss, 128);
         s->g_sd = persistent_grid((const void *)ks_shadow, 128);
         *out = s.release();
     });
