@@ -267,6 +267,8 @@ void finish_scene(crt_scene *s) {
     s->bvh.err = s->ctx->d_err;
     build_bvh(s->d_verts, (int)n, s->ctx->stream, s->bvh);
     upload_render_data(h, s->rd);
+    build_slot_class(s->bvh, h, s->rd, s->ctx->stream);
+    CRT_CUDA(cudaStreamSynchronize(s->ctx->stream));
     s->rp.width = h.width;
     s->rp.height = h.height;
     s->rp.spp = h.spp;

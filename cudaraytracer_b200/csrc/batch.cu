@@ -34,6 +34,7 @@ __global__ void k_raygen_views(const CamView *cams, int n_views, StepParams sp, 
         counters[0] = n;
         counters[kHitCounter] = 0;
         counters[kMissCounter] = 0;
+        counters[kSssCounter] = 0;
     }
     if (i >= n) return;
     const int64_t g = base + i;
@@ -103,7 +104,7 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
     for (int j = 0; j < 2; ++j)
         for (int k = 0; k < 5; ++k) q[j].p[k] = sc.wf.q[j][k];
     ShadowView sh{{sc.wf.shadow[0], sc.wf.shadow[1], sc.wf.shadow[2], sc.wf.shadow[3]}};
-    const ShadeOrder ord{sc.wf.order, (int)sc.wf.cap};
+    const ShadeOrder ord{sc.wf.order, (int)sc.wf.cap, sc.rd.slot_class};
     const int blk = sc.rp.block();
     const int smem = sc.rp.traversal();
     const int g_ext = persistent_grid((const void *)k_extend, blk);

@@ -74,8 +74,28 @@ __device__ __forceinline__ int warp_alloc(int *counter, bool want) {
     return want ? base + __popc(m & ((1u << lane) - 1u)) : -1;
 }
 
+// The path that shade thread t visits: the hits (other materials, then
+// subsurface) or the misses of the shade order.
+__device__ __forceinline__ int shade_hit_index(const ShadeOrder &o, int t, int nhit) {
+    return __ldg(o.idx + (t < nhit ? t : o.cap + (t - nhit)));
+}
+__device__ __forceinline__ int shade_miss_index(const ShadeOrder &o, int t) { return __ldg(o.idx + (o.cap - 1 - t)); }
 
-
+// Places path i, whose closest hit is in slot (< 0: a miss), into the shade
+// order (every lane of the warp calls it).
+__device__ __forceinline__ void shade_order_put(const ShadeOrder &o, int *counters, int slot, int i) {
+    const bool hit = slot >= 0;
+    const int ms = warp_alloc(&counters[kMissCounter], !hit);
+    if (!o.cls) {  // no subsurface material in the scene (uniform branch)
+        const int hs = warp_alloc(&counters[kHitCounter], hit);
+        o.idx[hit ? hs : o.cap - 1 - ms] = i;
+        return;
+    }
+    const bool sss = hit && o.cls[slot];
+    const int hs = warp_alloc(&counters[kHitCounter], hit && !sss);
+    const int ss = warp_alloc(&counters[kSssCounter], sss);
+    o.idx[sss ? o.cap + ss : (hit ? hs : o.cap - 1 - ms)] = i;
+}
 
 struct NeeRecord {
     V3 hp, hn, lp, ln, C;

@@ -29,6 +29,7 @@ namespace crt {
 // ---------------------------------------------------------------------------
 RenderData::~RenderData() {
     if (attr) cudaFree(attr);
+    if (slot_class) cudaFree(slot_class);
     if (meshes) cudaFree(meshes);
     if (materials) cudaFree(materials);
     if (lights) cudaFree(lights);
@@ -198,12 +199,36 @@ void upload_render_data(const HostScene &hs, RenderData &rd) {
     }
 }
 
+namespace {
+__global__ void k_slot_class(const float4 *tris, const float4 *attr, const DMesh *meshes, const DMaterial *mats, int n,
+                             uint8_t *cls) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const int prim = __float_as_int(tris[3 * (size_t)s].w);
+        const int mesh = __float_as_int(attr[4 * (size_t)prim + 3].w);
+        cls[s] = mats[meshes[mesh].material].type == MAT_SUBSURFACE ? 1 : 0;
+    }
+}
+}  // namespace
+
+void build_slot_class(const BvhBuffers &bvh, const HostScene &hs, RenderData &rd, cudaStream_t stream) {
+    if (rd.slot_class) cudaFree(rd.slot_class), rd.slot_class = nullptr;
+    const int n = (int)bvh.num_tris;
+    bool any_sss = false;
+    for (const DMaterial &m : hs.materials) any_sss = any_sss || m.type == MAT_SUBSURFACE;
+    if (n <= 0 || !any_sss) return;  // no class array: every hit goes to the first region
+    CRT_CUDA(cudaMalloc(&rd.slot_class, (size_t)n));
+    k_slot_class<<<std::min((n + 255) / 256, 148 * 8), 256, 0, stream>>>(bvh.tris, rd.attr, rd.meshes, rd.materials,
+                                                                          n, rd.slot_class);
+    CRT_CUDA(cudaGetLastError());
+}
+
 SceneView make_view(const BvhBuffers &bvh, const RenderData &rd) {
     SceneView s;
     std::memset(&s, 0, sizeof(s));
     s.bvh = bvh.view();
     s.slot_of_prim = bvh.slot_of_prim;
     s.attr = rd.attr;
+    s.slot_class = rd.slot_class;
     s.meshes = rd.meshes;
     s.materials = rd.materials;
     s.lights = rd.lights;
@@ -318,7 +343,7 @@ void Wavefront::reserve(size_t paths) {
     CRT_CUDA(cudaMalloc(&hits, paths * sizeof(float4)));
     for (int k = 0; k < 4; ++k) CRT_CUDA(cudaMalloc(&shadow[k], paths * sizeof(float4)));
     for (int k = 0; k < 2; ++k) CRT_CUDA(cudaMalloc(&term[k], paths * sizeof(float4)));
-    CRT_CUDA(cudaMalloc(&order, paths * sizeof(int)));
+    CRT_CUDA(cudaMalloc(&order, 2 * paths * sizeof(int)));
     cap = paths;
 }
 
@@ -352,6 +377,7 @@ __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *co
         counters[0] = n;
         counters[kHitCounter] = 0;
         counters[kMissCounter] = 0;
+        counters[kSssCounter] = 0;
     }
     if (i >= n) return;
     uint32_t pixel = (uint32_t)(i % sp.pixels);
@@ -394,10 +420,7 @@ __global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const 
         const V3 o{a.x, a.y, a.z}, d{b.x, b.y, b.z};
         Hit h = stage_closest<false>(bvh, st, mode, o, d, 0.f, kTriTMax);
         hits[i] = make_float4(h.t, __int_as_float(h.slot), h.b1, h.b2);
-        const bool hit = h.slot >= 0;
-        const int hs = warp_alloc(&counters[kHitCounter], hit);
-        const int ms = warp_alloc(&counters[kMissCounter], !hit);
-        ord.idx[hit ? hs : ord.cap - 1 - ms] = i;
+        shade_order_put(ord, counters, h.slot, i);
     }
 }
 
@@ -412,13 +435,11 @@ __device__ __forceinline__ void shade_body(const SceneView &s, const StepParams 
                                            const float4 *hits, const int *n_in, const QueueView &qout, int *counters,
                                            int out_idx, const ShadowView &sh, float4 *term0, float4 *term1,
                                            const AccumView &acc, const ShadeOrder &ord) {
-    const int n = *n_in, nhit = counters[kHitCounter];
-    const int t_end = kSet == kShadeHits ? nhit : n;
-    for (int t = (kSet == kShadeHits ? 0 : nhit) + blockIdx.x * blockDim.x + threadIdx.x; t < t_end;
-         t += gridDim.x * blockDim.x) {
-        // hits in order[0, nhit), misses from the back (each in the order
-        // extend placed them)
-        const int i = __ldg(ord.idx + (t < nhit ? t : ord.cap - 1 - (t - nhit)));
+    (void)n_in;
+    const int nhit = counters[kHitCounter];
+    const int t_end = kSet == kShadeHits ? nhit + counters[kSssCounter] : counters[kMissCounter];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < t_end; t += gridDim.x * blockDim.x) {
+        const int i = kSet == kShadeHits ? shade_hit_index(ord, t, nhit) : shade_miss_index(ord, t);
         PathState ps = load_path(qin, i);
         float4 hr = hits[i];
         Hit h;
@@ -519,6 +540,7 @@ __global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, int 
         // the shade order of the next bounce starts empty (shade has read it)
         counters[kHitCounter] = 0;
         counters[kMissCounter] = 0;
+        counters[kSssCounter] = 0;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = sh.r[0][i], b = sh.r[1][i], c = sh.r[2][i], d = sh.r[3][i];
@@ -609,7 +631,7 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
     for (int j = 0; j < 2; ++j)
         for (int k = 0; k < 5; ++k) q[j].p[k] = wf.q[j][k];
     ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
-    const ShadeOrder ord{wf.order, (int)wf.cap};
+    const ShadeOrder ord{wf.order, (int)wf.cap, view.slot_class};
     const int blk = rp.block();
     const int smem = rp.traversal();
     const int g_ext = persistent_grid((const void *)k_extend, blk);

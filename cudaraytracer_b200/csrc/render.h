@@ -25,6 +25,7 @@ struct RenderParams {
 // Device-resident render data of a scene (everything but the BVH).
 struct RenderData {
     float4 *attr = nullptr;
+    uint8_t *slot_class = nullptr;  // per leaf-ordered triangle slot: 1 = subsurface material (build_slot_class)
     DMesh *meshes = nullptr;
     DMaterial *materials = nullptr;
     DLight *lights = nullptr;
@@ -43,13 +44,15 @@ struct RenderData {
 
 // Path-state buffers of one wavefront, reused across renders.
 // Words of a wavefront's counter block: queue counts in [0, 4), the counts
-// of the bounce's hit and miss paths in the shade order at kHitCounter and
-// kMissCounter, and two 64-bit running totals of the rays the stage kernels
+// of the bounce's hit (other than subsurface), miss and subsurface-hit
+// paths in the shade order at kHitCounter, kMissCounter and kSssCounter,
+// and two 64-bit running totals of the rays the stage kernels
 // traced (extend rays at word 8, shadow rays at word 10; the subsurface
 // probe rays that the shade stage traces inline are not counted).
 constexpr int kWavefrontCounters = 16;
 constexpr int kHitCounter = 4;
 constexpr int kMissCounter = 5;
+constexpr int kSssCounter = 6;
 constexpr int kExtendRaysCounter = 8;
 constexpr int kShadowRaysCounter = 10;
 
@@ -59,7 +62,7 @@ struct Wavefront {
     float4 *hits = nullptr;    // (t, slot, b1, b2)
     float4 *shadow[4] = {};    // shadow-test records
     float4 *term[2] = {};      // terminated paths waiting for their shadow test
-    int *order = nullptr;      // shade order: hit paths' queue indices from the front, misses' from the back
+    int *order = nullptr;      // shade order, 2 x cap (render_kernels.cuh)
     int *counters = nullptr;   // [in0, in1, shadow, term] per bounce parity, hit/miss counts; ray counters
     void reserve(size_t paths);
     void release();
@@ -74,6 +77,10 @@ struct Accum {
 };
 
 void upload_render_data(const HostScene &hs, RenderData &rd);
+// rd.slot_class from the BVH's leaf-ordered triangles and the uploaded
+// meshes and materials (after upload_render_data); left null when no
+// material is subsurface.
+void build_slot_class(const BvhBuffers &bvh, const HostScene &hs, RenderData &rd, cudaStream_t stream);
 SceneView make_view(const BvhBuffers &bvh, const RenderData &rd);
 // ComputeCameraParam (Src/Core/camera.h:58-84) from the orbit parameters.
 void compute_camera(CameraState &c);

@@ -42,15 +42,19 @@ struct ShadowView {
 };
 
 // The order in which the shade stage visits a bounce's paths, written by
-// the extend stage: the queue indices of paths that hit a triangle in
-// idx[0 .. hits) and of paths that missed in idx[cap - misses .. cap), the
-// two counts at kHitCounter and kMissCounter of the counter block (reset by
-// raygen and by the shadow stage for the next bounce). Misses only add the
-// environment, so most warps of a sparse scene's first bounce are
-// miss-only and the hit warps run the material code with full lanes.
+// the extend stage into idx (2 x cap entries): the queue indices of paths
+// that hit a triangle of any material but subsurface in idx[0 .. hits), of
+// paths that missed in idx[cap - misses .. cap), and of subsurface hits in
+// idx[cap .. cap + sss); the counts at kHitCounter, kMissCounter and
+// kSssCounter of the counter block (reset by raygen and by the shadow stage
+// for the next bounce). cls is the scene's slot class (1 = subsurface) or
+// null. Misses only add the environment, so most warps of a sparse scene's
+// first bounce are miss-only; subsurface hits trace probe rays inside the
+// shade stage, so they run in warps of their own.
 struct ShadeOrder {
     int *idx;
     int cap;
+    const uint8_t *cls;
 };
 
 __global__ void k_raygen(CamView cam, StepParams sp, int n, QueueView q, int *counters);

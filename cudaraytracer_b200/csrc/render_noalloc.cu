@@ -11,7 +11,7 @@
 // point instead runs the same stage kernels over a fixed scratch area that
 // is part of the library's device image.
 //
-// The scratch is a file-scope __device__ array of kNoAllocBytes (18.1 MB)
+// The scratch is a file-scope __device__ array of kNoAllocBytes (18.4 MB)
 // holding the path queues, hit records, shadow records, terminated-path
 // records, the shade order and counters for at most kNoAllocMaxPaths = 65,536 paths per
 // wavefront (pixels x samples per pass). Every GPU that loads the library
@@ -44,10 +44,10 @@ namespace {
 
 constexpr size_t kNoAllocMaxPaths = 65536;
 // per path: 2 queues x 5 float4 + hit + 4 shadow + 2 terminal float4 = 272 B,
-// and a 4 B shade-order entry
+// and 8 B of shade order
 constexpr size_t kPlane = kNoAllocMaxPaths * sizeof(float4);
 constexpr size_t kCounterBytes = 256;
-constexpr size_t kOrderBytes = kNoAllocMaxPaths * sizeof(int);
+constexpr size_t kOrderBytes = 2 * kNoAllocMaxPaths * sizeof(int);
 constexpr size_t kNoAllocBytes = 17 * kPlane + kCounterBytes + kOrderBytes;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
@@ -95,7 +95,8 @@ extern "C" crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_
         float4 *plane[17];
         for (int k = 0; k < 17; ++k) plane[k] = reinterpret_cast<float4 *>(base + k * kPlane);
         int *counters = reinterpret_cast<int *>(base + 17 * kPlane);
-        const ShadeOrder ord{reinterpret_cast<int *>(base + 17 * kPlane + kCounterBytes), (int)kNoAllocMaxPaths};
+        const ShadeOrder ord{reinterpret_cast<int *>(base + 17 * kPlane + kCounterBytes), (int)kNoAllocMaxPaths,
+                             scene->rd.slot_class};
         QueueView q[2];
         for (int k = 0; k < 5; ++k) {
             q[0].p[k] = plane[k];

@@ -57,6 +57,7 @@ __global__ void ks_raygen(const ReqDesc *reqs, const Segment *segs, int nseg, in
         counters[0] = n;
         counters[kHitCounter] = 0;
         counters[kMissCounter] = 0;
+        counters[kSssCounter] = 0;
     }
     if (i >= n) return;
     int lo = 0, hi = nseg - 1;
@@ -104,14 +105,14 @@ __global__ void __launch_bounds__(128) ks_extend(const SceneView *scenes, QueueV
     const int n = *n_in;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = q.p[0][i], b = q.p[1][i];
-        const BvhView bvh = scenes[path_tag(q, i) >> kSlotBits].bvh;
+        const SceneView &sv = scenes[path_tag(q, i) >> kSlotBits];
+        const BvhView bvh = sv.bvh;
         const V3 o{a.x, a.y, a.z}, d{b.x, b.y, b.z};
         Hit h = stage_closest<false>(bvh, st, mode, o, d, 0.f, kTriTMax);
         hits[i] = make_float4(h.t, __int_as_float(h.slot), h.b1, h.b2);
-        const bool hit = h.slot >= 0;
-        const int hs = warp_alloc(&counters[kHitCounter], hit);
-        const int ms = warp_alloc(&counters[kMissCounter], !hit);
-        ord.idx[hit ? hs : ord.cap - 1 - ms] = i;  // the shade order (render_kernels.cuh)
+        ShadeOrder so = ord;
+        so.cls = sv.slot_class;
+        shade_order_put(so, counters, h.slot, i);  // the shade order (render_kernels.cuh)
     }
 }
 
@@ -126,11 +127,11 @@ __device__ __forceinline__ void ks_shade_body(const SceneView *scenes, const Req
                                               const QueueView &qin, const float4 *hits, const int *n_in,
                                               const QueueView &qout, int *counters, int out_idx, const ShadowView &sh,
                                               float4 *term0, float4 *term1, const ShadeOrder &ord) {
-    const int n = *n_in, nhit = counters[kHitCounter];
-    const int t_end = kMisses ? n : nhit;
-    for (int t = (kMisses ? nhit : 0) + blockIdx.x * blockDim.x + threadIdx.x; t < t_end;
-         t += gridDim.x * blockDim.x) {
-        const int i = __ldg(ord.idx + (t < nhit ? t : ord.cap - 1 - (t - nhit)));
+    (void)n_in;
+    const int nhit = counters[kHitCounter];
+    const int t_end = kMisses ? counters[kMissCounter] : nhit + counters[kSssCounter];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < t_end; t += gridDim.x * blockDim.x) {
+        const int i = kMisses ? shade_miss_index(ord, t) : shade_hit_index(ord, t, nhit);
         PathState ps = load_path(qin, i);
         const uint32_t tag = path_tag(qin, i);
         const SceneView &s = scenes[tag >> kSlotBits];
@@ -215,6 +216,7 @@ __global__ void __launch_bounds__(128) ks_shadow(const SceneView *scenes, const 
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         counters[kHitCounter] = 0;  // the next bounce's shade order starts empty
         counters[kMissCounter] = 0;
+        counters[kSssCounter] = 0;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 d = sh.r[3][i];
@@ -276,8 +278,8 @@ size_t scene_device_bytes(const Scene &sc) {
 }
 
 // Per wavefront path: two queues of 5 float4, the hit record, 4 shadow and
-// 2 terminal float4, and the shade-order entry.
-constexpr size_t kWavefrontBytesPerPath = 2 * 5 * 16 + 16 + 4 * 16 + 2 * 16 + 4;
+// 2 terminal float4, and two shade-order entries.
+constexpr size_t kWavefrontBytesPerPath = 2 * 5 * 16 + 16 + 4 * 16 + 2 * 16 + 8;
 
 }  // namespace
 }  // namespace crt
@@ -453,7 +455,7 @@ struct crt_server {
         for (int j = 0; j < 2; ++j)
             for (int c = 0; c < 5; ++c) q[j].p[c] = wf.q[j][c];
         ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
-        const ShadeOrder ord{wf.order, (int)wf.cap};
+        const ShadeOrder ord{wf.order, (int)wf.cap, nullptr};  // ks_extend takes each path's scene's classes
         ks_raygen<<<(n + 255) / 256, 256, 0, stream>>>(d_reqs, ds, nseg, n, q[0], wf.counters);
         const int smem = stage_traversal_env();
         for (int b = 0; b < max_b; ++b) {

@@ -38,6 +38,8 @@ struct SceneView {
     float center[3];
     float diag;
     const cudaTextureObject_t *textures;  // DMaterial::tex indexes this
+    const uint8_t *slot_class;             // per triangle slot: 1 = subsurface material (shade order); null
+                                           // when the scene has no subsurface material
 };
 
 #ifdef __CUDACC__

@@ -253,7 +253,7 @@ crt_status crt_render_device(crt_scene *scene, int32_t first_sample, int32_t spp
 crt_status crt_scene_ray_counts(crt_scene *scene, void *stream, int64_t *extend_rays, int64_t *shadow_rays);
 
 /* Same as crt_render_device but allocates no device memory: the path queues
- * live in a fixed scratch area inside the library's device image (18.1 MB
+ * live in a fixed scratch area inside the library's device image (18.4 MB
  * per GPU that loads the library, held until exit), for hosts that own the
  * GPU memory pool and forbid foreign cudaMalloc/cudaFree during a frame
  * (engines, viewport plugins, real-time services). At most 65,536 paths per
