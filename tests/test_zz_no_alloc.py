@@ -12,7 +12,9 @@ entry point crt_render_device on the same samples:
   the scratch queues across passes;
 * an explicit spp_per_pass below the scratch limit and a 64-thread stage
   block, which the entry point honours as crt_render_device does;
-* 65,537 pixels, one beyond the limit, rejected with CRT_ERR_CAPACITY."""
+* 65,537 pixels, one beyond the limit, rejected with CRT_ERR_CAPACITY;
+* a scene with all four materials and an environment light, whose shade
+  order has all three regions (hits, subsurface hits, misses)."""
 import numpy as np
 import pytest
 
@@ -54,6 +56,15 @@ def test_noalloc_render_matches_allocating_entry_point(ctx, tmp_path):
     sc.set_render_params(seed=13)
     for first in (0, 4):  # two calls in a row, different sample ranges
         _pair(sc, 4, first)
+    sc.close()
+
+
+def test_noalloc_render_all_materials(ctx, tmp_path):
+    spec = scenes.icosphere_field(n_spheres=8, level=2, width=48, height=48, env_size=(256, 128), spp=4,
+                                  max_bounces=6)
+    sc = Scene.load(ctx, spec.write(str(tmp_path), "ico"))
+    sc.set_render_params(seed=17)
+    _pair(sc, 4, 0)
     sc.close()
 
 
