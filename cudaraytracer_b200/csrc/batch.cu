@@ -126,7 +126,7 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
             StepParams bp = sp;
             bp.bounce = b;
             k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], sc.wf.counters + in, sc.wf.hits, sc.wf.counters, out,
-                                           smem, ord);
+                                           extend_mode(smem, b), ord);
             k_shade<<<g_sh, blk, 0, s>>>(view, bp, q[in], sc.wf.hits, sc.wf.counters + in, q[out], sc.wf.counters,
                                          out, sh, sc.wf.term[0], sc.wf.term[1], av, ord);
             k_shade_miss<<<g_sm, blk, 0, s>>>(view, bp, q[in], sc.wf.hits, sc.wf.counters + in, q[out],

@@ -291,6 +291,101 @@ __device__ __forceinline__ Hit closest_hit_st(const BvhView &bvh, Stack &st, V3 
     return hit;
 }
 
+// Warp-coherent closest hit: the 32 lanes of a warp traverse the tree as
+// one packet (for the extend stage's primary rays, which sit in pixel
+// order). Every lane of the current node's mask tests the node's two child
+// boxes against its own ray interval [tmin, own closest]; the warp descends
+// into a child that some lane hit (the one most of the lanes hitting both
+// reach first) and pushes the other, with the mask of lanes that hit it,
+// onto a stack of (link, mask) entries kept for the warp in shared memory
+// (ws_link / ws_mask, kStackSize entries each, touched by lane 0 only and
+// broadcast by shuffles). A leaf's triangles are tested by the lanes of its
+// mask. Each lane prunes and tests exactly as closest_hit<false> does on its
+// own ray; it may enter boxes its own ray would not, which only adds
+// triangle tests whose accepted hits are real intersections, so its closest
+// hit is closest_hit's up to the choice between triangles at equal t. All
+// 32 lanes call it together; lanes with `active` false only vote.
+template <bool kCull = true>
+__device__ __forceinline__ Hit closest_hit_warp(const BvhView &bvh, int *ws_link, unsigned *ws_mask, bool active, V3 o,
+                                                V3 d, float tmin, float tmax) {
+    Hit hit;
+    hit.t = tmax;
+    hit.slot = -1;
+    hit.b1 = hit.b2 = 0.f;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned lane_bit = 1u << lane;
+    const V3 inv = v3(rrcp(d.x), rrcp(d.y), rrcp(d.z));
+    unsigned mask = __ballot_sync(full, active);
+    int link = 0, sp = 0;  // warp-uniform: current link, stack depth
+    while (mask) {
+        bool pop = true;
+        if (link >= 0) {
+            if (link >= bvh.num_nodes) {
+                report_traversal_bounds(bvh);
+                return hit;
+            }
+            float4 n0, n1, n2;
+            int4 n3;
+            load_node(bvh.nodes + 4 * (size_t)link, n0, n1, n2, n3);
+            float t0 = 0.f, t1 = 0.f;
+            bool h0 = false, h1 = false;
+            if (mask & lane_bit) {
+                h0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, tmin, hit.t, t0);
+                h1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, tmin, hit.t, t1);
+            }
+            const unsigned m0 = __ballot_sync(full, h0), m1 = __ballot_sync(full, h1);
+            if (m0 && m1) {
+                const unsigned near1 = __ballot_sync(full, h0 && h1 && t1 < t0);
+                const bool go1 = 2 * __popc(near1) > __popc(m0 & m1);
+                if (sp >= kStackSize) {
+                    report_traversal_bounds(bvh);
+                    return hit;
+                }
+                if (lane == 0) {
+                    ws_link[sp] = go1 ? n3.x : n3.y;
+                    ws_mask[sp] = go1 ? m0 : m1;
+                }
+                ++sp;
+                link = go1 ? n3.y : n3.x;
+                mask = go1 ? m1 : m0;
+                pop = false;
+            } else if (m0 | m1) {
+                link = m0 ? n3.x : n3.y;
+                mask = m0 ? m0 : m1;
+                pop = false;
+            }
+        } else {
+            const int code = ~link;
+            const int first = code >> 4, count = code & 15;
+            if (first + count > bvh.num_tris) {
+                report_traversal_bounds(bvh);
+                return hit;
+            }
+            if (mask & lane_bit)
+                for (int k = 0; k < count; ++k) {
+                    const int slot = first + k;
+                    const float4 *tp = bvh.tris + 3 * (size_t)slot;
+                    const float4 a = __ldg(tp + 0), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                    intersect_triangle<kCull>(o, d, a, b, c, slot, hit);
+                }
+        }
+        if (pop) {
+            if (sp == 0) break;
+            --sp;
+            int l = 0;
+            unsigned mk = 0;
+            if (lane == 0) {
+                l = ws_link[sp];
+                mk = ws_mask[sp];
+            }
+            link = __shfl_sync(full, l, 0);
+            mask = __shfl_sync(full, mk, 0);
+        }
+    }
+    return hit;
+}
+
 __device__ __forceinline__ int tri_prim(const BvhView &bvh, int slot) {
     return __float_as_int(__ldg(bvh.tris + 3 * (size_t)slot).w);
 }

@@ -415,6 +415,29 @@ __global__ void __launch_bounds__(256) k_extend(BvhView bvh, QueueView q, const 
         counters[3] = 0;
         atomicAdd(reinterpret_cast<unsigned long long *>(counters + kExtendRaysCounter), (unsigned long long)n);
     }
+    if (mode == kStageWarp) {
+        // whole warps over 32 consecutive paths; the warp's (link, mask)
+        // stack takes 2 x kStackSize words of s_stack
+        static_assert(kStageShort * kStageMaxBlock >= (kStageMaxBlock / 32) * 2 * kStackSize, "warp stacks");
+        int *ws_link = reinterpret_cast<int *>(s_stack) + (threadIdx.x >> 5) * 2 * kStackSize;
+        unsigned *ws_mask = reinterpret_cast<unsigned *>(ws_link + kStackSize);
+        for (int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < n; i0 += gridDim.x * blockDim.x) {
+            const int i = i0 + (threadIdx.x & 31);
+            const bool active = i < n;
+            V3 o{0.f, 0.f, 0.f}, d{0.f, 0.f, 1.f};
+            if (active) {
+                const float4 a = q.p[0][i], b = q.p[1][i];
+                o = V3{a.x, a.y, a.z};
+                d = V3{b.x, b.y, b.z};
+            }
+            const Hit h = closest_hit_warp(bvh, ws_link, ws_mask, active, o, d, 0.f, kTriTMax);
+            if (active) {
+                hits[i] = make_float4(h.t, __int_as_float(h.slot), h.b1, h.b2);
+                shade_order_put(ord, counters, h.slot, i);
+            }
+        }
+        return;
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 a = q.p[0][i], b = q.p[1][i];
         const V3 o{a.x, a.y, a.z}, d{b.x, b.y, b.z};
@@ -588,11 +611,12 @@ int stage_traversal_env() {
     if (v == "shared") return kStageShared;
     if (v == "local-quant") return kStageLocalQuant;
     if (v == "shared-quant") return kStageSharedQuant;
+    if (v == "warp") return kStageWarp;
     return kStageTraversalDefault;
 }
 
 int RenderParams::traversal() const {
-    // CRT_STAGE_LOCAL..CRT_STAGE_SHARED_QUANT are the StageTraversal modes + 1
+    // CRT_STAGE_LOCAL..CRT_STAGE_WARP are the StageTraversal modes + 1
     return stage_traversal > 0 ? stage_traversal - 1 : stage_traversal_env();
 }
 
@@ -659,8 +683,8 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
         for (int b = 0; b < rp.max_bounces; ++b) {
             int in = b & 1, out = 1 - in;
             sp.bounce = b;
-            k_extend<<<g_ext, blk, 0, stream>>>(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out, smem,
-                                                ord);
+            k_extend<<<g_ext, blk, 0, stream>>>(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out,
+                                                extend_mode(smem, b), ord);
             if (mb == 4)
                 k_shade_mb<4><<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out],
                                                         wf.counters, out, sh, wf.term[0], wf.term[1], av, ord);

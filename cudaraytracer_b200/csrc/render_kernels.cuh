@@ -82,18 +82,25 @@ constexpr int kStageShort = 8;
 constexpr int kStageMaxBlock = 256;
 // How the extend and shadow stages traverse: the top of each lane's stack
 // in shared memory (ShortStack) or the whole stack in local memory
-// (LocalStack), over the float nodes or their 16-bit quantised copy.
+// (LocalStack), over the float nodes or their 16-bit quantised copy; or
+// (kStageWarp) the primary rays of bounce 0 as warp-coherent packets with
+// one stack per warp in shared memory (closest_hit_warp, bvh.cuh), every
+// later bounce and every shadow ray with the local stack.
 enum StageTraversal : int {
     kStageLocal = 0,
     kStageShared = 1,
     kStageLocalQuant = 2,
     kStageSharedQuant = 3,
+    kStageWarp = 4,
 };
 constexpr int kStageTraversalDefault = kStageLocal;
 
+// The extend stage's mode at bounce `bounce` (kStageWarp covers bounce 0).
+inline int extend_mode(int mode, int bounce) { return (mode == kStageWarp && bounce > 0) ? kStageLocal : mode; }
+
 // The mode for launches whose render parameters leave it open (and for the
 // server): kStageTraversalDefault, or the one named by CRT_STAGE_TRAVERSAL
-// (local, shared, local-quant, shared-quant).
+// (local, shared, local-quant, shared-quant, warp).
 int stage_traversal_env();
 
 #ifdef __CUDACC__

@@ -142,7 +142,8 @@ extern "C" crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_
             for (int b = 0; b < rp.max_bounces; ++b) {
                 const int in = b & 1, out = 1 - in;
                 sp.bounce = b;
-                k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], counters + in, hits, counters, out, smem, ord);
+                k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], counters + in, hits, counters, out,
+                                               extend_mode(smem, b), ord);
                 k_shade<<<g_sh, blk, 0, s>>>(view, sp, q[in], hits, counters + in, q[out], counters, out, sh, term0,
                                             term1, av, ord);
                 k_shade_miss<<<g_sm, blk, 0, s>>>(view, sp, q[in], hits, counters + in, q[out], counters, out, sh,

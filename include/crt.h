@@ -214,6 +214,8 @@ typedef struct crt_render_params {
 #define CRT_STAGE_SHARED 2        /* top 8 entries in shared memory, 64 B float nodes */
 #define CRT_STAGE_LOCAL_QUANT 3   /* local stack, 32 B nodes with 16-bit quantised boxes */
 #define CRT_STAGE_SHARED_QUANT 4  /* shared short stack, 32 B quantised nodes */
+#define CRT_STAGE_WARP 5          /* primary rays as warp-coherent packets, one stack per warp in shared
+                                     memory; later bounces and shadow rays as LOCAL */
 
 crt_status crt_get_render_params(const crt_scene *scene, crt_render_params *p);
 crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p);
