@@ -18,8 +18,8 @@ import os
 DEFAULT_CANDIDATES = (1 << 20, 2 << 20, 4 << 20, 8 << 20, 16 << 20)
 BLOCK_CANDIDATES = (64, 128, 256)
 # crt_render_params.stage_traversal: CRT_STAGE_LOCAL, _SHARED, _LOCAL_QUANT,
-# _SHARED_QUANT, _WARP (include/crt.h)
-TRAVERSAL_CANDIDATES = {1: "local", 2: "shared", 3: "local-quant", 4: "shared-quant", 5: "warp"}
+# _SHARED_QUANT, _WARP, _REFILL (include/crt.h)
+TRAVERSAL_CANDIDATES = {1: "local", 2: "shared", 3: "local-quant", 4: "shared-quant", 5: "warp", 6: "refill"}
 
 
 def cache_key(scene, n_views: int) -> str:

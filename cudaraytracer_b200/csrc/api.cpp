@@ -500,8 +500,8 @@ crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p) {
                   CRT_ERR_INVALID, "crt_set_render_params: negative count");
         CRT_CHECK(p->stage_block == 0 || p->stage_block == 64 || p->stage_block == 128 || p->stage_block == 256,
                   CRT_ERR_INVALID, "crt_set_render_params: stage_block must be 0, 64, 128 or 256");
-        CRT_CHECK(p->stage_traversal >= CRT_STAGE_DEFAULT && p->stage_traversal <= CRT_STAGE_WARP,
-                  CRT_ERR_INVALID, "crt_set_render_params: stage_traversal must be 0-5");
+        CRT_CHECK(p->stage_traversal >= CRT_STAGE_DEFAULT && p->stage_traversal <= CRT_STAGE_REFILL,
+                  CRT_ERR_INVALID, "crt_set_render_params: stage_traversal must be 0-6");
         bool resized = p->width != scene->rp.width || p->height != scene->rp.height;
         scene->rp.width = p->width;
         scene->rp.height = p->height;

@@ -106,11 +106,9 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
     ShadowView sh{{sc.wf.shadow[0], sc.wf.shadow[1], sc.wf.shadow[2], sc.wf.shadow[3]}};
     const ShadeOrder ord{sc.wf.order, (int)sc.wf.cap, sc.rd.slot_class};
     const int blk = sc.rp.block();
-    const int smem = sc.rp.traversal();
-    const int g_ext = persistent_grid((const void *)k_extend, blk);
+    const int smem = sc.rp.traversal(sc.bvh.num_tris);
     const int g_sh = persistent_grid((const void *)k_shade, blk);
     const int g_sm = persistent_grid((const void *)k_shade_miss, blk);
-    const int g_sd = persistent_grid((const void *)k_shadow, blk);
     StepParams sp;
     sp.bounce = 0;
     sp.rr = sc.rp.rr;
@@ -125,14 +123,14 @@ int render_views(Scene &sc, const std::vector<CameraState> &cams, int first_samp
             const int in = b & 1, out = 1 - in;
             StepParams bp = sp;
             bp.bounce = b;
-            k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], sc.wf.counters + in, sc.wf.hits, sc.wf.counters, out,
-                                           extend_mode(smem, b), ord);
+            launch_extend_stage(view.bvh, q[in], sc.wf.counters + in, sc.wf.hits, sc.wf.counters, out, smem, b,
+                                ord, blk, s);
             k_shade<<<g_sh, blk, 0, s>>>(view, bp, q[in], sc.wf.hits, sc.wf.counters + in, q[out], sc.wf.counters,
                                          out, sh, sc.wf.term[0], sc.wf.term[1], av, ord);
             k_shade_miss<<<g_sm, blk, 0, s>>>(view, bp, q[in], sc.wf.hits, sc.wf.counters + in, q[out],
                                               sc.wf.counters, out, sh, sc.wf.term[0], sc.wf.term[1], av, ord);
-            k_shadow<<<g_sd, blk, 0, s>>>(view.bvh, sh, sc.wf.counters, q[out], sc.wf.term[0], sc.wf.term[1], av,
-                                          smem);
+            launch_shadow_stage(view.bvh, sh, sc.wf.counters, q[out], sc.wf.term[0], sc.wf.term[1], av, smem,
+                                blk, s);
         }
         k_advance_pass<<<1, 1, 0, s>>>(d_pass, chunk);
     };

@@ -18,6 +18,7 @@
 // Rows are bottom-up (pixel j = 0 is the bottom row), as the reference's
 // accumulation buffers.
 #include "path.cuh"
+#include "traverse.cuh"
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -548,6 +549,45 @@ static int shade_min_blocks(int block) {
     return (block <= 128 && (v == 4 || v == 6 || v == 10)) ? v : 0;
 }
 
+// The effect of deferred NEE sample i once its visibility is known: a
+// visible sample's contribution joins its path's direct or indirect
+// radiance; a path that already terminated is then added to its pixel.
+__device__ __forceinline__ void shadow_apply(const ShadowView &sh, int i, bool vis, const QueueView &qout,
+                                             float4 *term0, float4 *term1, const AccumView &acc) {
+    const float4 d = sh.r[3][i];
+    uint32_t target = __float_as_uint(d.w);
+    uint32_t idx = target & kIndexMask;
+    bool direct = (target & kDirectBit) != 0;
+    V3 C{d.x, d.y, d.z};
+    if (target & kTermBit) {
+        float4 t0 = term0[idx], t1 = term1[idx];
+        V3 dc{t0.x, t0.y, t0.z}, ic{t1.x, t1.y, t1.z};
+        if (vis) {
+            if (direct)
+                dc = dc + C;
+            else
+                ic = ic + C;
+        }
+        accumulate(acc, __float_as_uint(t0.w), dc, ic);
+    } else if (vis) {
+        if (direct) {
+            float4 p2 = qout.p[2][idx], p3 = qout.p[3][idx];
+            p2.w += C.x;
+            p3.x += C.y;
+            p3.y += C.z;
+            qout.p[2][idx] = p2;
+            qout.p[3][idx] = p3;
+        } else {
+            float4 p3 = qout.p[3][idx], p4 = qout.p[4][idx];
+            p3.z += C.x;
+            p3.w += C.y;
+            p4.x += C.z;
+            qout.p[3][idx] = p3;
+            qout.p[4][idx] = p4;
+        }
+    }
+}
+
 // Shadow: Light::Visible for each deferred NEE sample; a visible sample's
 // contribution joins its path's direct or indirect radiance; a path that
 // already terminated is then added to its pixel.
@@ -566,58 +606,137 @@ __global__ void __launch_bounds__(256) k_shadow(BvhView bvh, ShadowView sh, int 
         counters[kSssCounter] = 0;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 a = sh.r[0][i], b = sh.r[1][i], c = sh.r[2][i], d = sh.r[3][i];
+        float4 a = sh.r[0][i], b = sh.r[1][i], c = sh.r[2][i];
         const V3 hp{a.x, a.y, a.z}, hn{a.w, b.x, b.y}, lp{b.z, b.w, c.x}, ln{c.y, c.z, c.w};
         const bool vis = stage_visible(bvh, st, mode, hp, hn, lp, ln);
-        uint32_t target = __float_as_uint(d.w);
-        uint32_t idx = target & kIndexMask;
-        bool direct = (target & kDirectBit) != 0;
-        V3 C{d.x, d.y, d.z};
-        if (target & kTermBit) {
-            float4 t0 = term0[idx], t1 = term1[idx];
-            V3 dc{t0.x, t0.y, t0.z}, ic{t1.x, t1.y, t1.z};
-            if (vis) {
-                if (direct)
-                    dc = dc + C;
-                else
-                    ic = ic + C;
-            }
-            accumulate(acc, __float_as_uint(t0.w), dc, ic);
-        } else if (vis) {
-            if (direct) {
-                float4 p2 = qout.p[2][idx], p3 = qout.p[3][idx];
-                p2.w += C.x;
-                p3.x += C.y;
-                p3.y += C.z;
-                qout.p[2][idx] = p2;
-                qout.p[3][idx] = p3;
-            } else {
-                float4 p3 = qout.p[3][idx], p4 = qout.p[4][idx];
-                p3.z += C.x;
-                p3.w += C.y;
-                p4.x += C.z;
-                qout.p[3][idx] = p3;
-                qout.p[4][idx] = p4;
-            }
-        }
+        shadow_apply(sh, i, vis, qout, term0, term1, acc);
     }
 }
 
-int stage_traversal_env() {
+// Extend and shadow with per-lane ray refill (trace_dynamic, traverse.cuh):
+// each warp keeps 32 rays in flight over its share of the queue and a lane
+// whose ray finished takes the next one. For the incoherent rays after the
+// first bounce and for shadow rays (kStageRefill); same traversal and the
+// same results as the one-path-per-thread kernels.
+struct StageExtendJob {
+    BvhView bvh;
+    QueueView q;
+    float4 *hits;
+    int *counters;
+    ShadeOrder ord;
+    __device__ void setup(int i, BvhView &b, V3 &o, V3 &d, float &tmin, float &tmax, float &t_exit) {
+        b = bvh;
+        const float4 a = q.p[0][i], bb = q.p[1][i];
+        o = V3{a.x, a.y, a.z};
+        d = V3{bb.x, bb.y, bb.z};
+        tmin = 0.f;
+        tmax = kTriTMax;
+        t_exit = 0.f;
+    }
+    __device__ void finish(int i, const BvhView &, const Hit &h) {
+        hits[i] = make_float4(h.t, __int_as_float(h.slot), h.b1, h.b2);
+        shade_order_put(ord, counters, h.slot, i);
+    }
+};
+
+struct StageShadowJob {
+    BvhView bvh;
+    ShadowView sh;
+    QueueView qout;
+    float4 *term0, *term1;
+    AccumView acc;
+    ShadowRay r;
+    __device__ void setup(int i, BvhView &b, V3 &o, V3 &d, float &tmin, float &tmax, float &t_exit) {
+        b = bvh;
+        const float4 a = sh.r[0][i], bb = sh.r[1][i], c = sh.r[2][i];
+        shadow_ray_init(r, V3{a.x, a.y, a.z}, V3{a.w, bb.x, bb.y}, V3{bb.z, bb.w, c.x}, V3{c.y, c.z, c.w});
+        o = r.o;
+        d = r.dir;
+        tmin = 1e-6f;
+        tmax = 1e8f;
+        t_exit = r.t_exit;
+    }
+    __device__ void finish(int i, const BvhView &b, const Hit &h) {
+        shadow_apply(sh, i, shadow_ray_visible(r, b, h), qout, term0, term1, acc);
+    }
+};
+
+__global__ void __launch_bounds__(256) k_extend_refill(BvhView bvh, QueueView q, const int *n_in, float4 *hits,
+                                                       int *counters, int out_idx, ShadeOrder ord) {
+    const int n = *n_in;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counters[out_idx] = 0;
+        counters[2] = 0;
+        counters[3] = 0;
+        atomicAdd(reinterpret_cast<unsigned long long *>(counters + kExtendRaysCounter), (unsigned long long)n);
+    }
+    StageExtendJob job{bvh, q, hits, counters, ord};
+    trace_dynamic<true>(job, n);
+}
+
+__global__ void __launch_bounds__(256) k_shadow_refill(BvhView bvh, ShadowView sh, int *counters, QueueView qout,
+                                                       float4 *term0, float4 *term1, AccumView acc) {
+    const int n = counters[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long *>(counters + kShadowRaysCounter), (unsigned long long)n);
+        counters[kHitCounter] = 0;  // the shade order of the next bounce starts empty
+        counters[kMissCounter] = 0;
+        counters[kSssCounter] = 0;
+    }
+    StageShadowJob job{bvh, sh, qout, term0, term1, acc, {}};
+    trace_dynamic<true>(job, n);
+}
+
+void launch_extend_stage(const BvhView &bvh, const QueueView &q, const int *n_in, float4 *hits, int *counters,
+                         int out_idx, int mode, int bounce, const ShadeOrder &ord, int block, cudaStream_t s) {
+    if (mode == kStageRefill && bounce > 0) {
+        k_extend_refill<<<persistent_grid((const void *)k_extend_refill, block), block, 0, s>>>(bvh, q, n_in, hits,
+                                                                                             counters, out_idx, ord);
+    } else {
+        k_extend<<<persistent_grid((const void *)k_extend, block), block, 0, s>>>(bvh, q, n_in, hits, counters,
+                                                                                   out_idx, extend_mode(mode, bounce),
+                                                                                   ord);
+    }
+}
+
+void launch_shadow_stage(const BvhView &bvh, const ShadowView &sh, int *counters, const QueueView &qout,
+                         float4 *term0, float4 *term1, const AccumView &acc, int mode, int block, cudaStream_t s) {
+    if (mode == kStageRefill)
+        k_shadow_refill<<<persistent_grid((const void *)k_shadow_refill, block), block, 0, s>>>(bvh, sh, counters,
+                                                                                             qout, term0, term1, acc);
+    else
+        k_shadow<<<persistent_grid((const void *)k_shadow, block), block, 0, s>>>(bvh, sh, counters, qout, term0,
+                                                                                   term1, acc, mode);
+}
+
+// The mode named by CRT_STAGE_TRAVERSAL, or -1.
+static int env_traversal() {
     const char *e = getenv("CRT_STAGE_TRAVERSAL");
-    if (!e) return kStageTraversalDefault;
+    if (!e) return -1;
     const std::string v(e);
     if (v == "local") return kStageLocal;
     if (v == "shared") return kStageShared;
     if (v == "local-quant") return kStageLocalQuant;
     if (v == "shared-quant") return kStageSharedQuant;
     if (v == "warp") return kStageWarp;
-    return kStageTraversalDefault;
+    if (v == "refill") return kStageRefill;
+    return -1;
 }
 
-int RenderParams::traversal() const {
-    // CRT_STAGE_LOCAL..CRT_STAGE_WARP are the StageTraversal modes + 1
-    return stage_traversal > 0 ? stage_traversal - 1 : stage_traversal_env();
+int stage_traversal_env() {
+    const int e = env_traversal();
+    return e >= 0 ? e : kStageTraversalDefault;
+}
+
+int RenderParams::traversal(int64_t num_tris) const {
+    // CRT_STAGE_LOCAL..CRT_STAGE_REFILL are the StageTraversal modes + 1
+    if (stage_traversal > 0) return stage_traversal - 1;
+    const int e = env_traversal();
+    if (e >= 0) return e;
+    // Per-lane refill pays for its bookkeeping once traversals are long:
+    // measured 8% faster per 1080p frame on the 1.31M-triangle icosphere
+    // field and 26% slower on the 36-triangle Cornell box.
+    return num_tris >= kRefillMinTriangles ? kStageRefill : kStageLocal;
 }
 
 int persistent_grid(const void *kernel, int block) {
@@ -657,8 +776,7 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
     ShadowView sh{{wf.shadow[0], wf.shadow[1], wf.shadow[2], wf.shadow[3]}};
     const ShadeOrder ord{wf.order, (int)wf.cap, view.slot_class};
     const int blk = rp.block();
-    const int smem = rp.traversal();
-    const int g_ext = persistent_grid((const void *)k_extend, blk);
+    const int smem = rp.traversal(view.bvh.num_tris);
     const int mb = shade_min_blocks(blk);
     const void *shade_fn = mb == 4    ? (const void *)k_shade_mb<4>
                            : mb == 6  ? (const void *)k_shade_mb<6>
@@ -666,7 +784,6 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
                                       : (const void *)k_shade;
     const int g_sh = persistent_grid(shade_fn, blk);
     const int g_sm = persistent_grid((const void *)k_shade_miss, blk);
-    const int g_sd = persistent_grid((const void *)k_shadow, blk);
     int launches = 0;
     for (int done = 0; done < spp; done += per_pass) {
         int s_here = std::min(per_pass, spp - done);
@@ -683,8 +800,8 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
         for (int b = 0; b < rp.max_bounces; ++b) {
             int in = b & 1, out = 1 - in;
             sp.bounce = b;
-            k_extend<<<g_ext, blk, 0, stream>>>(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out,
-                                                extend_mode(smem, b), ord);
+            launch_extend_stage(view.bvh, q[in], wf.counters + in, wf.hits, wf.counters, out, smem, b, ord, blk,
+                                stream);
             if (mb == 4)
                 k_shade_mb<4><<<g_sh, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out],
                                                         wf.counters, out, sh, wf.term[0], wf.term[1], av, ord);
@@ -699,7 +816,7 @@ int render_samples(const SceneView &view, const CameraState &cam, const RenderPa
                                                   out, sh, wf.term[0], wf.term[1], av, ord);
             k_shade_miss<<<g_sm, blk, 0, stream>>>(view, sp, q[in], wf.hits, wf.counters + in, q[out], wf.counters,
                                                    out, sh, wf.term[0], wf.term[1], av, ord);
-            k_shadow<<<g_sd, blk, 0, stream>>>(view.bvh, sh, wf.counters, q[out], wf.term[0], wf.term[1], av, smem);
+            launch_shadow_stage(view.bvh, sh, wf.counters, q[out], wf.term[0], wf.term[1], av, smem, blk, stream);
             launches += 4;
         }
         CRT_CUDA(cudaGetLastError());

@@ -6,6 +6,8 @@
 
 namespace crt {
 
+constexpr int64_t kRefillMinTriangles = 65536;
+
 struct RenderParams {
     int width = 0, height = 0;
     int spp = 16;
@@ -18,8 +20,11 @@ struct RenderParams {
     int stage_block = 0;      // threads per block of the wavefront stage kernels; 0 = 128
     int stage_traversal = 0;  // CRT_STAGE_*: 0 = stage_traversal_env() (environment or default)
     int block() const { return stage_block ? stage_block : 128; }
-    // The StageTraversal mode (render_kernels.cuh) of the extend/shadow stages.
-    int traversal() const;
+    // The StageTraversal mode (render_kernels.cuh) of the extend/shadow
+    // stages for a scene of num_tris triangles: stage_traversal if set, else
+    // CRT_STAGE_TRAVERSAL, else per-lane refill from kRefillMinTriangles up
+    // and the local stack below.
+    int traversal(int64_t num_tris) const;
 };
 
 // Device-resident render data of a scene (everything but the BVH).

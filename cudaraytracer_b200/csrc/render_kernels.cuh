@@ -70,6 +70,13 @@ __global__ void k_shade_miss(SceneView s, StepParams sp, QueueView qin, const fl
                              AccumView acc, ShadeOrder ord);
 __global__ void k_shadow(BvhView bvh, ShadowView sh, int *counters, QueueView qout, float4 *term0, float4 *term1,
                          AccumView acc, int mode);
+// The extend stage of bounce `bounce` and the shadow stage in traversal
+// mode `mode` (StageTraversal below): picks the kernel (one path per thread
+// or per-lane refill) and its persistent grid for `block` threads.
+void launch_extend_stage(const BvhView &bvh, const QueueView &q, const int *n_in, float4 *hits, int *counters,
+                         int out_idx, int mode, int bounce, const ShadeOrder &ord, int block, cudaStream_t s);
+void launch_shadow_stage(const BvhView &bvh, const ShadowView &sh, int *counters, const QueueView &qout,
+                         float4 *term0, float4 *term1, const AccumView &acc, int mode, int block, cudaStream_t s);
 
 // Blocks per grid for a persistent launch of `kernel` (all SMs at full
 // occupancy).
@@ -85,22 +92,28 @@ constexpr int kStageMaxBlock = 256;
 // (LocalStack), over the float nodes or their 16-bit quantised copy; or
 // (kStageWarp) the primary rays of bounce 0 as warp-coherent packets with
 // one stack per warp in shared memory (closest_hit_warp, bvh.cuh), every
-// later bounce and every shadow ray with the local stack.
+// later bounce and every shadow ray with the local stack; or (kStageRefill)
+// bounce 0 one path per thread and every later extend and every shadow ray
+// with per-lane ray refill (trace_dynamic, traverse.cuh), local stack.
 enum StageTraversal : int {
     kStageLocal = 0,
     kStageShared = 1,
     kStageLocalQuant = 2,
     kStageSharedQuant = 3,
     kStageWarp = 4,
+    kStageRefill = 5,
 };
 constexpr int kStageTraversalDefault = kStageLocal;
 
 // The extend stage's mode at bounce `bounce` (kStageWarp covers bounce 0).
-inline int extend_mode(int mode, int bounce) { return (mode == kStageWarp && bounce > 0) ? kStageLocal : mode; }
+inline int extend_mode(int mode, int bounce) {
+    return ((mode == kStageWarp && bounce > 0) || mode == kStageRefill) ? kStageLocal : mode;
+}
 
-// The mode for launches whose render parameters leave it open (and for the
-// server): kStageTraversalDefault, or the one named by CRT_STAGE_TRAVERSAL
-// (local, shared, local-quant, shared-quant, warp).
+// The server's mode: kStageTraversalDefault, or the one named by
+// CRT_STAGE_TRAVERSAL (local, shared, local-quant, shared-quant, warp,
+// refill; the server's stages treat warp and refill as local). The
+// renderers resolve theirs with RenderParams::traversal (render.h).
 int stage_traversal_env();
 
 #ifdef __CUDACC__

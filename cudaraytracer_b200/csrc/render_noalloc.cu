@@ -124,11 +124,9 @@ extern "C" crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_
         const int fit = (int)(kNoAllocMaxPaths / pixels);
         const int per_pass = std::max(1, std::min(spp, rp.spp_per_pass > 0 ? std::min(rp.spp_per_pass, fit) : fit));
         const int blk = rp.block();
-        const int smem = rp.traversal();
-        const int g_ext = persistent_grid((const void *)k_extend, blk);
+        const int smem = rp.traversal(scene->bvh.num_tris);
         const int g_sh = persistent_grid((const void *)k_shade, blk);
         const int g_sm = persistent_grid((const void *)k_shade_miss, blk);
-        const int g_sd = persistent_grid((const void *)k_shadow, blk);
         for (int done = 0; done < spp; done += per_pass) {
             const int n = (int)pixels * std::min(per_pass, spp - done);
             StepParams sp;
@@ -142,13 +140,12 @@ extern "C" crt_status crt_render_device_noalloc(crt_scene *scene, int32_t first_
             for (int b = 0; b < rp.max_bounces; ++b) {
                 const int in = b & 1, out = 1 - in;
                 sp.bounce = b;
-                k_extend<<<g_ext, blk, 0, s>>>(view.bvh, q[in], counters + in, hits, counters, out,
-                                               extend_mode(smem, b), ord);
+                launch_extend_stage(view.bvh, q[in], counters + in, hits, counters, out, smem, b, ord, blk, s);
                 k_shade<<<g_sh, blk, 0, s>>>(view, sp, q[in], hits, counters + in, q[out], counters, out, sh, term0,
                                             term1, av, ord);
                 k_shade_miss<<<g_sm, blk, 0, s>>>(view, sp, q[in], hits, counters + in, q[out], counters, out, sh,
                                                  term0, term1, av, ord);
-                k_shadow<<<g_sd, blk, 0, s>>>(view.bvh, sh, counters, q[out], term0, term1, av, smem);
+                launch_shadow_stage(view.bvh, sh, counters, q[out], term0, term1, av, smem, blk, s);
             }
             CRT_CUDA(cudaGetLastError());
         }

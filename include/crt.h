@@ -216,6 +216,8 @@ typedef struct crt_render_params {
 #define CRT_STAGE_SHARED_QUANT 4  /* shared short stack, 32 B quantised nodes */
 #define CRT_STAGE_WARP 5          /* primary rays as warp-coherent packets, one stack per warp in shared
                                      memory; later bounces and shadow rays as LOCAL */
+#define CRT_STAGE_REFILL 6        /* primary rays as LOCAL; later bounces and shadow rays with per-lane
+                                     ray refill (each warp keeps 32 rays in flight), local stack */
 
 crt_status crt_get_render_params(const crt_scene *scene, crt_render_params *p);
 crt_status crt_set_render_params(crt_scene *scene, const crt_render_params *p);

@@ -82,7 +82,7 @@ def test_autotuner_picks_and_caches(cornell, tmp_path):
     assert not r["cached"] and r["paths_per_pass"] in (1 << 14, 1 << 16)
     assert cornell.render_params()["paths_per_pass"] == r["paths_per_pass"]
     assert r["stage_block"] in (64, 128, 256) and cornell.render_params()["stage_block"] == r["stage_block"]
-    assert r["stage_traversal"] in (1, 2, 3, 4, 5) and len(r["traversal_timings_ms"]) == 5
+    assert r["stage_traversal"] in (1, 2, 3, 4, 5, 6) and len(r["traversal_timings_ms"]) == 6
     assert cornell.render_params()["stage_traversal"] == r["stage_traversal"]
     cornell.set_render_params(stage_traversal=0)
     r2 = autotune_paths_per_pass(cornell, views, candidates=(1 << 14, 1 << 16), cache_path=cache)
@@ -123,13 +123,13 @@ def test_stage_traversal_param_does_not_change_the_image(cornell):
 
     cornell.set_render_params(stage_traversal=0, seed=29)
     d0, i0 = cornell.render(4)
-    for t in (1, 2, 3, 4, 5):
+    for t in (1, 2, 3, 4, 5, 6):
         cornell.set_render_params(stage_traversal=t)
         d1, i1 = cornell.render(4)
         for a, b in ((d1, d0), (i1, i0)):
             err = np.abs(a - b)[..., :3] / np.maximum(np.abs(b[..., :3]), 1e-3)
             assert (err > 1e-4).any(-1).mean() <= 0.002, t
     cornell.set_render_params(stage_traversal=0)
-    for bad in (-1, 6):
+    for bad in (-1, 7):
         with pytest.raises(CrtError):
             cornell.set_render_params(stage_traversal=bad)

@@ -162,12 +162,12 @@ def test_textured_two_light_render_matches_oracle(crt_ctx, textured_json):
     assert back.std(0).max() > 0.02
 
 
-@pytest.mark.parametrize("mode", ["local", "local-quant", "shared-quant", "warp"])  # each against "shared"
+@pytest.mark.parametrize("mode", ["local", "local-quant", "shared-quant", "warp", "refill"])  # against "shared"
 def test_stage_traversal_modes_agree(crt_ctx, ico_json, monkeypatch, mode):
     """The extend and shadow stages give the same frame in every traversal
     mode (the whole stack in local memory, the default, or its top in
     shared memory; float nodes or their 16-bit quantised copy; primary rays
-    as warp-coherent packets), up to the
+    as warp-coherent packets; later rays with per-lane refill), up to the
     order of the float atomics that add paths into pixels and the rare tie between equal-t triangles, and no traversal records an
     out-of-range index."""
     sc = Scene.load(crt_ctx, ico_json)
