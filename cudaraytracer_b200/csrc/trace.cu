@@ -53,6 +53,46 @@ struct ShadowJob {
     __device__ void finish(int i, const BvhView &b, const Hit &h) { occ[i] = shadow_ray_visible(r, b, h) ? 0 : 1; }
 };
 
+// Light::Visible in two passes, with the same answer. Pass 1 looks for the
+// closest hit on [0, sd + 0.2] only (sd = distance from the light point to
+// the shading point), which prunes every box beyond the shading point from
+// the start; a hit found there is the closest hit of the whole ray, and the
+// predicate is evaluated on it as before. With no hit there, the closest
+// hit of the whole ray is absent (visible) or at t >= sd + 0.2, more than
+// 0.1 from the shading point and from the sample distance (occluded), so
+// pass 2 only asks whether any triangle is hit on [sd + 0.2, 1e8] and stops
+// at the first.
+struct ShadowJob2 {
+    BvhView bvh;
+    const float4 *q;
+    uint8_t *occ;
+    ShadowRay r;
+    bool second;
+    __device__ void setup(int i, BvhView &b, V3 &o, V3 &d, float &tmin, float &tmax, float &t_exit) {
+        b = bvh;
+        float4 a = __ldg(q + 3 * (size_t)i), bb = __ldg(q + 3 * (size_t)i + 1), c = __ldg(q + 3 * (size_t)i + 2);
+        shadow_ray_init(r, v3(a.x, a.y, a.z), v3(a.w, bb.x, bb.y), v3(bb.z, bb.w, c.x), v3(c.y, c.z, c.w));
+        o = r.o;
+        d = r.dir;
+        tmin = 1e-6f;
+        tmax = r.sd + 0.2f;
+        t_exit = r.t_exit;
+        second = false;
+    }
+    __device__ bool again(int, Hit &hit, float &tmin, float &t_exit) {
+        if (second || hit.slot >= 0) return false;
+        second = true;
+        tmin = r.sd + 0.2f;
+        hit.t = 1e8f;
+        hit.slot = -1;
+        t_exit = 1e8f;  // any accepted hit ends pass 2
+        return true;
+    }
+    __device__ void finish(int i, const BvhView &b, const Hit &h) {
+        occ[i] = second ? (h.slot >= 0 ? 1 : 0) : (shadow_ray_visible(r, b, h) ? 0 : 1);
+    }
+};
+
 }  // namespace
 
 // Each warp traces its contiguous share of the batch, refilling lanes as
@@ -100,6 +140,17 @@ __global__ void __launch_bounds__(kTraceBlock, 8) k_trace_shadow_q(BvhView bvh, 
     ShadowJob job{bvh, q, occ, {}};
     LocalStack st;
     trace_dynamic_st<true, true>(job, n, st);
+}
+
+// Light::Visible in two passes (ShadowJob2), local stack, for at least
+// kMinBlocks resident blocks per SM (1: no register cap).
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTraceBlock, kMinBlocks) k_trace_shadow_2p(BvhView bvh,
+                                                                            const float4 *__restrict__ q, int n,
+                                                                            uint8_t *__restrict__ occ) {
+    ShadowJob2 job{bvh, q, occ, {}, false};
+    LocalStack st;
+    trace_dynamic_st<true, false, ShadowJob2, LocalStack, false, true>(job, n, st);
 }
 
 // The binary traversal with the local stack and pipelined triangle loads,
@@ -198,7 +249,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8r(BvhView bvh, con
 // default kTraceVariant): 2 = binary tree, stack in local memory
 // (210 / 212: the same capped at 51 / 42 registers for 10 / 12 blocks per SM;
 // 3: with postponed leaves; 5 / 58: with pipelined triangle loads (no
-// register cap / 8 blocks per SM); 4 / 416: over
+// register cap / 8 blocks per SM); 6 / 68: shadow queries in two passes
+// (ShadowJob2; no register cap / 8 blocks per SM; extend as 2); 4 / 416: over
 // the 16-bit quantised nodes with
 // the stack in local / shared memory);
 // 28 / 216 = binary tree, top 8 / 16 stack entries per lane in shared
@@ -284,6 +336,12 @@ void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_
         k_trace_shadow_p<<<trace_grid((const void *)k_trace_shadow_p, n), kTraceBlock, 0, s>>>(bvh, q, (int)n, d_occ);
     else if (v == 5)
         k_trace_shadow_pf<1><<<trace_grid((const void *)k_trace_shadow_pf<1>, n), kTraceBlock, 0, s>>>(bvh, q,
+                                                                                                      (int)n, d_occ);
+    else if (v == 6)
+        k_trace_shadow_2p<1><<<trace_grid((const void *)k_trace_shadow_2p<1>, n), kTraceBlock, 0, s>>>(bvh, q,
+                                                                                                      (int)n, d_occ);
+    else if (v == 68)
+        k_trace_shadow_2p<8><<<trace_grid((const void *)k_trace_shadow_2p<8>, n), kTraceBlock, 0, s>>>(bvh, q,
                                                                                                       (int)n, d_occ);
     else if (v == 58)
         k_trace_shadow_pf<8><<<trace_grid((const void *)k_trace_shadow_pf<8>, n), kTraceBlock, 0, s>>>(bvh, q,

@@ -30,7 +30,7 @@ namespace crt {
 
 #ifdef __CUDACC__
 
-template <bool kCull, bool kQuant, class Job, class Stack, bool kPipe = false>
+template <bool kCull, bool kQuant, class Job, class Stack, bool kPipe = false, bool kMultiPass = false>
 __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st);
 
 // The stack in local memory, float nodes.
@@ -43,8 +43,13 @@ __device__ __forceinline__ void trace_dynamic(Job &job, int n) {
 // Over a given per-lane stack (LocalStack or ShortStack, bvh.cuh), and over
 // the float nodes or (kQuant) their 16-bit quantised copy (bvh16.cuh). With
 // kPipe the leaf loop loads triangle k + 1 before testing triangle k, so its
-// 48 B are in flight during the test (same tests in the same order).
-template <bool kCull, bool kQuant, class Job, class Stack, bool kPipe>
+// 48 B are in flight during the test (same tests in the same order). With
+// kMultiPass a finished ray is offered to
+//   __device__ bool again(int i, Hit &hit, float &tmin, float &t_exit);
+// which may set a new box interval start, closest bound (hit.t, with
+// hit.slot = -1) and exit distance and return true to traverse again from
+// the root before finish.
+template <bool kCull, bool kQuant, class Job, class Stack, bool kPipe, bool kMultiPass>
 __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
     const unsigned lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -177,8 +182,15 @@ __device__ __forceinline__ void trace_dynamic_st(Job &job, int n, Stack &st) {
             }
         }
         if (finished) {
-            job.finish(idx, bvh, hit);
-            idx = -1;
+            bool again = false;
+            if constexpr (kMultiPass) again = !bad && job.again(idx, hit, tmin, t_exit);
+            if (again) {
+                st.reset();
+                link = 0;
+            } else {
+                job.finish(idx, bvh, hit);
+                idx = -1;
+            }
         }
     }
 }
