@@ -81,20 +81,31 @@ __global__ void k_avgpool2(const __nv_bfloat16 *in, __nv_bfloat16 *out, int n, i
     }
 }
 
-// out[p] = concat(up2(low)[p] (Ca), skip[p] (Cb)).
-__global__ void k_up_concat(const __nv_bfloat16 *low, const __nv_bfloat16 *skip, __nv_bfloat16 *out, int n, int h,
-                            int w, int Ca, int Cb) {
+// out[p] = concat(up2(low)[p] (Ca), skip[p] (Cb)), 8 channels (16 B) per
+// thread step; index arithmetic in I (32-bit whenever the element count
+// allows: the divisions are most of the work).
+template <class I>
+__device__ __forceinline__ void up_concat(const __nv_bfloat16 *low, const __nv_bfloat16 *skip, __nv_bfloat16 *out,
+                                          int n, int h, int w, int Ca, int Cb) {
     const int C = Ca + Cb, G = C / 8;
-    const int64_t total = (int64_t)n * h * w * G;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const I total = (I)n * h * w * G;
+    for (I i = blockIdx.x * (I)blockDim.x + threadIdx.x; i < total; i += (I)gridDim.x * blockDim.x) {
         const int g = (int)(i % G);
-        const int64_t p = i / G;
-        const int x = (int)(p % w), y = (int)((p / w) % h), b = (int)(p / ((int64_t)w * h));
+        const I p = i / G;
+        const int x = (int)(p % w), y = (int)((p / w) % h), b = (int)(p / ((I)w * h));
         const __nv_bfloat16 *src = g * 8 < Ca
                                        ? low + (((int64_t)b * (h / 2) + y / 2) * (w / 2) + x / 2) * Ca + g * 8
-                                       : skip + p * Cb + (g * 8 - Ca);
-        *reinterpret_cast<uint4 *>(out + p * C + g * 8) = *reinterpret_cast<const uint4 *>(src);
+                                       : skip + (int64_t)p * Cb + (g * 8 - Ca);
+        *reinterpret_cast<uint4 *>(out + (int64_t)p * C + g * 8) = *reinterpret_cast<const uint4 *>(src);
     }
+}
+
+__global__ void k_up_concat(const __nv_bfloat16 *low, const __nv_bfloat16 *skip, __nv_bfloat16 *out, int n, int h,
+                            int w, int Ca, int Cb) {
+    if ((int64_t)n * h * w * ((Ca + Cb) / 8) < (int64_t)INT32_MAX - (int64_t)gridDim.x * blockDim.x)
+        up_concat<int>(low, skip, out, n, h, w, Ca, Cb);
+    else
+        up_concat<int64_t>(low, skip, out, n, h, w, Ca, Cb);
 }
 
 // Adjoint of up2 on the first Ca channels of gcat: glow[q] = sum of the 2x2
@@ -222,16 +233,31 @@ __global__ void k_features(FeatureArgs a) {
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// Softmax over the 25 logits of pixel p, weights in w.
+// Softmax over the 25 logits of one pixel (its 32-float row, 16-byte
+// aligned), weights in w. The row is read as 7 float4 loads (28 floats),
+// not 25 scalar loads that each touch a sector per lane.
 __device__ __forceinline__ void filter_weights(const float *logits, float (&w)[kTaps5]) {
-    float mx = logits[0];
-    for (int k = 1; k < kTaps5; ++k) mx = fmaxf(mx, logits[k]);
+    float l[28];
+    const float4 *lp = reinterpret_cast<const float4 *>(logits);
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+        const float4 v = lp[j];
+        l[4 * j] = v.x;
+        l[4 * j + 1] = v.y;
+        l[4 * j + 2] = v.z;
+        l[4 * j + 3] = v.w;
+    }
+    float mx = l[0];
+#pragma unroll
+    for (int k = 1; k < kTaps5; ++k) mx = fmaxf(mx, l[k]);
     float s = 0.f;
+#pragma unroll
     for (int k = 0; k < kTaps5; ++k) {
-        w[k] = expf(logits[k] - mx);
+        w[k] = expf(l[k] - mx);
         s += w[k];
     }
     const float inv = 1.f / s;
+#pragma unroll
     for (int k = 0; k < kTaps5; ++k) w[k] *= inv;
 }
 
@@ -244,6 +270,7 @@ __global__ void k_apply_filter(const float *logits, const float4 *noisy, float4 
         float wt[kTaps5];
         filter_weights(logits + p * kOutC, wt);
         float r = 0.f, g = 0.f, b = 0.f;
+#pragma unroll
         for (int k = 0; k < kTaps5; ++k) {
             const int sy = clampi(y + k / 5 - 2, 0, h - 1), sx = clampi(x + k % 5 - 2, 0, w - 1);
             const float4 v = noisy[base + (int64_t)sy * w + sx];
