@@ -142,6 +142,33 @@ __global__ void __launch_bounds__(kTraceBlock, 8) k_trace_shadow_q(BvhView bvh, 
     trace_dynamic_st<true, true>(job, n, st);
 }
 
+// One ray per thread, no refill (closest_hit / its early-exit form over the
+// local stack): for small scenes, whose traversals are a few nodes long and
+// do not repay the refill loop's bookkeeping.
+__global__ void __launch_bounds__(kTraceBlock) k_trace_closest_1(BvhView bvh, const float4 *__restrict__ rays, int n,
+                                                                 float4 *__restrict__ hits) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ClosestJob job{bvh, rays, hits};
+    BvhView b;
+    V3 o, d;
+    float tmin, tmax, t_exit;
+    job.setup(i, b, o, d, tmin, tmax, t_exit);
+    job.finish(i, b, closest_hit<false>(b, o, d, tmin, tmax));
+}
+
+__global__ void __launch_bounds__(kTraceBlock) k_trace_shadow_1(BvhView bvh, const float4 *__restrict__ q, int n,
+                                                                uint8_t *__restrict__ occ) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ShadowJob job{bvh, q, occ, {}};
+    BvhView b;
+    V3 o, d;
+    float tmin, tmax, t_exit;
+    job.setup(i, b, o, d, tmin, tmax, t_exit);
+    job.finish(i, b, closest_hit<true>(b, o, d, tmin, tmax, t_exit));
+}
+
 // Light::Visible in two passes (ShadowJob2), local stack, for at least
 // kMinBlocks resident blocks per SM (1: no register cap).
 template <int kMinBlocks>
@@ -248,7 +275,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8r(BvhView bvh, con
 // Traversal variant of the trace kernels (CRT_TRAVERSAL overrides the
 // default kTraceVariant): 2 = binary tree, stack in local memory
 // (210 / 212: the same capped at 51 / 42 registers for 10 / 12 blocks per SM;
-// 3: with postponed leaves; 5 / 58: with pipelined triangle loads (no
+// 1: one ray per thread without refill; 3: with postponed leaves; 5 / 58:
+// with pipelined triangle loads (no
 // register cap / 8 blocks per SM); 6 / 68: shadow queries in two passes
 // (ShadowJob2; no register cap / 8 blocks per SM; extend as 2); 4 / 416: over
 // the 16-bit quantised nodes with
@@ -287,6 +315,9 @@ void launch_trace_closest(const BvhView &bvh, const float4 *d_rays, int64_t n, f
     else if (v == 3)
         k_trace_closest_p<<<trace_grid((const void *)k_trace_closest_p, n), kTraceBlock, 0, s>>>(bvh, d_rays, (int)n,
                                                                                                 d_hits);
+    else if (v == 1)
+        k_trace_closest_1<<<(int)((n + kTraceBlock - 1) / kTraceBlock), kTraceBlock, 0, s>>>(bvh, d_rays, (int)n,
+                                                                                           d_hits);
     else if (v == 5)
         k_trace_closest_pf<1><<<trace_grid((const void *)k_trace_closest_pf<1>, n), kTraceBlock, 0, s>>>(
             bvh, d_rays, (int)n, d_hits);
@@ -334,6 +365,8 @@ void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_
             bvh, q, (int)n, d_occ);
     else if (v == 3)
         k_trace_shadow_p<<<trace_grid((const void *)k_trace_shadow_p, n), kTraceBlock, 0, s>>>(bvh, q, (int)n, d_occ);
+    else if (v == 1)
+        k_trace_shadow_1<<<(int)((n + kTraceBlock - 1) / kTraceBlock), kTraceBlock, 0, s>>>(bvh, q, (int)n, d_occ);
     else if (v == 5)
         k_trace_shadow_pf<1><<<trace_grid((const void *)k_trace_shadow_pf<1>, n), kTraceBlock, 0, s>>>(bvh, q,
                                                                                                       (int)n, d_occ);

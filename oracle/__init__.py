@@ -18,6 +18,9 @@ ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libcrtref.so")
 REF_CUDA_SO = os.path.join(HERE, "_ref", "libcrtref_cuda.so")
 REF_RENDER_SO = os.path.join(HERE, "_ref", "libcrtref_render.so")
+# the same builds with device link-time optimisation (oracle/Makefile)
+REF_CUDA_LTO_SO = os.path.join(HERE, "_ref", "libcrtref_cuda_lto.so")
+REF_RENDER_LTO_SO = os.path.join(HERE, "_ref", "libcrtref_render_lto.so")
 
 _VP = C.c_void_p
 
@@ -245,50 +248,53 @@ class RefScene:
             pass
 
 
-_refcuda = None
+_refcuda = {}
 
 
-def ref_cuda_available() -> bool:
-    return os.path.exists(REF_CUDA_SO)
+def ref_cuda_available(lto: bool = False) -> bool:
+    return os.path.exists(REF_CUDA_LTO_SO if lto else REF_CUDA_SO)
 
 
-def ref_cuda_lib() -> C.CDLL:
-    global _refcuda
-    if _refcuda is None:
-        L = C.CDLL(REF_CUDA_SO)
+def ref_cuda_lib(lto: bool = False) -> C.CDLL:
+    """The reference's traversal built for the GPU: -rdc, or (lto) with
+    device link-time optimisation."""
+    if lto not in _refcuda:
+        L = C.CDLL(REF_CUDA_LTO_SO if lto else REF_CUDA_SO)
         L.refcuda_scene_from_triangles.restype = _VP
         L.refcuda_scene_from_triangles.argtypes = [_VP, C.c_long]
         L.refcuda_scene_free.argtypes = [_VP]
         L.refcuda_trace.argtypes = [_VP, _VP, C.c_long, _VP, _VP]
         L.refcuda_visible.argtypes = [_VP, _VP, C.c_long, _VP, _VP]
-        _refcuda = L
-    return _refcuda
+        _refcuda[lto] = L
+    return _refcuda[lto]
 
 
 class RefCudaScene:
     """The reference's own traversal compiled for the GPU (headless build):
     host BVH build + CreateBVH upload, one thread per ray calling
-    BVH::IsIntersect / Light::Visible. Device pointers in, stream-ordered."""
+    BVH::IsIntersect / Light::Visible. Device pointers in, stream-ordered.
+    lto selects the device-LTO build."""
 
-    def __init__(self, tris):
+    def __init__(self, tris, lto: bool = False):
         self.tris = _f32(tris, 9)
+        self._lib = ref_cuda_lib(lto)
         with _quiet_stdout():
-            self._h = ref_cuda_lib().refcuda_scene_from_triangles(self.tris.ctypes.data, self.tris.shape[0])
+            self._h = self._lib.refcuda_scene_from_triangles(self.tris.ctypes.data, self.tris.shape[0])
 
     def trace(self, d_rays: int, n: int, d_out: int, stream: int = 0) -> None:
-        rc = ref_cuda_lib().refcuda_trace(self._h, d_rays, n, d_out, stream)
+        rc = self._lib.refcuda_trace(self._h, d_rays, n, d_out, stream)
         if rc:
             raise RuntimeError(f"reference CUDA trace failed: cudaError {rc}")
 
     def visible(self, d_q: int, n: int, d_occ: int, stream: int = 0) -> None:
-        rc = ref_cuda_lib().refcuda_visible(self._h, d_q, n, d_occ, stream)
+        rc = self._lib.refcuda_visible(self._h, d_q, n, d_occ, stream)
         if rc:
             raise RuntimeError(f"reference CUDA visible failed: cudaError {rc}")
 
     def close(self):
         if self._h:
             with _quiet_stdout():
-                ref_cuda_lib().refcuda_scene_free(self._h)
+                self._lib.refcuda_scene_free(self._h)
             self._h = None
 
     def __del__(self):
@@ -298,25 +304,26 @@ class RefCudaScene:
             pass
 
 
-_refrender = None
+_refrender = {}
 
 
-def ref_render_available() -> bool:
-    return os.path.exists(REF_RENDER_SO)
+def ref_render_available(lto: bool = False) -> bool:
+    return os.path.exists(REF_RENDER_LTO_SO if lto else REF_RENDER_SO)
 
 
-def ref_render_lib() -> C.CDLL:
-    global _refrender
-    if _refrender is None:
-        L = C.CDLL(REF_RENDER_SO)
+def ref_render_lib(lto: bool = False) -> C.CDLL:
+    """The reference's renderer and SVGF kernels built for the GPU: -rdc, or
+    (lto) with device link-time optimisation."""
+    if lto not in _refrender:
+        L = C.CDLL(REF_RENDER_LTO_SO if lto else REF_RENDER_SO)
         L.refr_load.restype = _VP
         L.refr_load.argtypes = [C.c_char_p]
         L.refr_info.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float), _VP]
         L.refr_render.argtypes = [_VP, C.c_int, C.c_int, _VP, _VP, _VP, C.POINTER(C.c_float)]
         L.refr_svgf.argtypes = [C.c_int, C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP, _VP, C.c_int, C.c_float,
                                 C.c_float, C.c_float, C.c_float, C.c_int, _VP, _VP, _VP]
-        _refrender = L
-    return _refrender
+        _refrender[lto] = L
+    return _refrender[lto]
 
 
 class RefRenderer:
@@ -325,14 +332,15 @@ class RefRenderer:
     sample per pixel per frame with its curand sampler (seed 1234). One
     scene per process (the reference keeps its scene in global state)."""
 
-    def __init__(self, json_path: str):
+    def __init__(self, json_path: str, lto: bool = False):
+        self._lib = ref_render_lib(lto)
         with _quiet_stdout():
-            self._h = ref_render_lib().refr_load(str(json_path).encode())
+            self._h = self._lib.refr_load(str(json_path).encode())
         if not self._h:
             raise RuntimeError(f"reference failed to load {json_path}")
         w, h, mb, rr = C.c_int(), C.c_int(), C.c_int(), C.c_float()
         cam = (C.c_float * 12)()
-        ref_render_lib().refr_info(C.byref(w), C.byref(h), C.byref(mb), C.byref(rr), cam)
+        self._lib.refr_info(C.byref(w), C.byref(h), C.byref(mb), C.byref(rr), cam)
         self.width, self.height, self.max_bounces, self.rr = w.value, h.value, mb.value, rr.value
         c = list(cam)
         self.camera = {"position": c[0:3], "left_down": c[3:6], "du": c[6:9], "dv": c[9:12]}
@@ -345,7 +353,7 @@ class RefRenderer:
         q = np.zeros_like(d) if with_sumsq else None
         ms = C.c_float()
         with _quiet_stdout():
-            rc = ref_render_lib().refr_render(self._h, spp, max_bounces, d.ctypes.data, i.ctypes.data,
+            rc = self._lib.refr_render(self._h, spp, max_bounces, d.ctypes.data, i.ctypes.data,
                                               q.ctypes.data if q is not None else None, C.byref(ms))
         if rc:
             raise RuntimeError(f"reference render failed: cudaError {rc}")
@@ -353,11 +361,12 @@ class RefRenderer:
 
 
 def ref_svgf(noisy_d, noisy_i, pos_tri, normal_mat, bary_mesh, motion_depth, max_history=24, sigma_light=8.0,
-             sigma_normal=256.0, sigma_depth=1.0, reproj=0.1, atrous=5, timing=False):
+             sigma_normal=256.0, sigma_depth=1.0, reproj=0.1, atrous=5, timing=False, lto=False):
     """The reference's SVGF kernels (headless CUDA build) over a frame
     sequence: arrays of shape (F, H, W, 4) (normal_mat / bary_mesh uint16).
     Returns (out_direct, out_indirect), float32 (F, H, W, 4), and with
-    timing=True also the GPU ms of each frame's denoise block."""
+    timing=True also the GPU ms of each frame's denoise block. lto selects
+    the device-LTO build."""
     nd = np.ascontiguousarray(noisy_d, np.float32)
     ni = np.ascontiguousarray(noisy_i, np.float32)
     gp = np.ascontiguousarray(pos_tri, np.float32)
@@ -368,7 +377,7 @@ def ref_svgf(noisy_d, noisy_i, pos_tri, normal_mat, bary_mesh, motion_depth, max
     od = np.zeros_like(nd)
     oi = np.zeros_like(ni)
     ms = np.zeros(f, np.float32)
-    rc = ref_render_lib().refr_svgf(w, h, f, nd.ctypes.data, ni.ctypes.data, gp.ctypes.data, gn.ctypes.data,
+    rc = ref_render_lib(lto).refr_svgf(w, h, f, nd.ctypes.data, ni.ctypes.data, gp.ctypes.data, gn.ctypes.data,
                                     gb.ctypes.data, gm.ctypes.data, max_history, sigma_light, sigma_normal,
                                     sigma_depth, reproj, atrous, od.ctypes.data, oi.ctypes.data, ms.ctypes.data)
     if rc:

@@ -149,7 +149,7 @@ def test_empty_batches_and_errors(crt_ctx, cornell_tris):
         Scene.from_triangles(crt_ctx, np.zeros((0, 9), np.float32))
 
 
-@pytest.mark.parametrize("variant", ["28", "216", "210", "212", "3", "5", "58", "6", "68", "4", "416", "8", "82", "83"])
+@pytest.mark.parametrize("variant", ["1", "28", "216", "210", "212", "3", "5", "58", "6", "68", "4", "416", "8", "82", "83"])
 def test_traversal_variants_agree(crt_ctx, ico_tris, variant, monkeypatch):
     """Every traversal variant of the trace kernels (binary tree with the
     top of each lane's stack in shared memory, 8 or 16 entries; capped
