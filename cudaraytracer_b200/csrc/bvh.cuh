@@ -12,7 +12,11 @@
 //   tris:  48 B per triangle in leaf order: v0 (w = original primitive index
 //          as int bits), v1, v2. Edges are formed in-kernel exactly as the
 //          reference does (e1 = v1 - v0, Src/Core/triangle.cu:102-103), so
-//          the stored vertices give bit-identical arithmetic.
+//          the stored vertices give bit-identical arithmetic. (A second
+//          leaf-order array of v0, e1, e2 saved the six subtractions but
+//          measured 6-8% slower on a 1.3M-triangle scene, whose traversal
+//          then keeps both arrays in L2; only the shared-memory copy of a
+//          small tree holds edges, trace.cu.)
 // The reference node is a 32 B {triIndex, count/right, Bounds3D} with the
 // child boxes stored in the children (Src/Core/bvh.h:25-33) and a 176 B AoS
 // triangle (Src/Core/triangle.h:43-57).
@@ -71,12 +75,12 @@ struct Hit {
 // visited. Returns true and updates `hit` when accepted.
 // kCull = false accepts both facings (det != 0), as a rasteriser without
 // face culling sees the nearest surface (used for the G-buffer only).
+// intersect_triangle_e takes the edges e1 = v1 - v0, e2 = v2 - v0 already
+// formed; intersect_triangle forms them from the three vertices. (One
+// predicate over all quantities instead of the early returns measured 4-6%
+// slower on a 1.3M-triangle scene and on the Cornell box.)
 template <bool kCull = true>
-__device__ __forceinline__ bool intersect_triangle(V3 o, V3 d, float4 a, float4 b, float4 c,
-                                                   int slot, Hit &hit) {
-    V3 v0 = v3(a.x, a.y, a.z);
-    V3 e1 = vsub(v3(b.x, b.y, b.z), v0);
-    V3 e2 = vsub(v3(c.x, c.y, c.z), v0);
+__device__ __forceinline__ bool intersect_triangle_e(V3 o, V3 d, V3 v0, V3 e1, V3 e2, int slot, Hit &hit) {
     V3 s = vsub(o, v0);
     V3 s1 = vcross(d, e2);
     V3 s2 = vcross(s, e1);
@@ -95,6 +99,13 @@ __device__ __forceinline__ bool intersect_triangle(V3 o, V3 d, float4 a, float4 
     hit.b1 = b1;
     hit.b2 = b2;
     return true;
+}
+
+template <bool kCull = true>
+__device__ __forceinline__ bool intersect_triangle(V3 o, V3 d, float4 a, float4 b, float4 c,
+                                                   int slot, Hit &hit) {
+    const V3 v0 = v3(a.x, a.y, a.z);
+    return intersect_triangle_e<kCull>(o, d, v0, vsub(v3(b.x, b.y, b.z), v0), vsub(v3(c.x, c.y, c.z), v0), slot, hit);
 }
 
 // Conservative slab test of one child box. Returns entry distance in `tnear`.

@@ -8,6 +8,7 @@
 #include "trace.cuh"
 #include "traverse.cuh"
 #include "render_kernels.cuh"  // persistent_grid
+#include <algorithm>
 #include <cstdlib>
 
 namespace crt {
@@ -169,6 +170,147 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow_1(BvhView bvh, con
     job.finish(i, b, closest_hit<true>(b, o, d, tmin, tmax, t_exit));
 }
 
+// --- Scenes whose tree fits in shared memory ---
+//
+// Interior nodes (4 float4 each) and triangles (3 float4 each: v0 with the
+// primitive index, e1 = v1 - v0, e2 = v2 - v0 rounded to nearest as the
+// triangle test forms them) of a scene of at most kTinyBytes are copied
+// into each block's shared memory once; the traversal then reads them there
+// (closest_hit's order, tests and bounds checks, so the same hits).
+constexpr int kTinyBytes = 32 * 1024;
+
+static int64_t tiny_bytes(const BvhView &bvh) {
+    return ((int64_t)4 * bvh.num_nodes + (int64_t)3 * bvh.num_tris) * (int64_t)sizeof(float4);
+}
+
+template <bool kEarlyExit, class Stack>
+__device__ __forceinline__ Hit closest_hit_tiny(const float4 *sn, const float4 *se, const BvhView &bvh, Stack &st,
+                                                V3 o, V3 d, float tmin, float tmax, float t_exit) {
+    Hit hit;
+    hit.t = tmax;
+    hit.slot = -1;
+    hit.b1 = hit.b2 = 0.f;
+    const V3 inv = v3(rrcp(d.x), rrcp(d.y), rrcp(d.z));
+    unsigned lm[Stack::kLocal];
+    st.reset();
+    int link = 0;
+    while (link != kSentinel) {
+        while (link >= 0) {
+            if (link >= bvh.num_nodes) {
+                report_traversal_bounds(bvh);
+                return hit;
+            }
+            const float4 *nd = sn + 4 * link;
+            const float4 n0 = nd[0], n1 = nd[1], n2 = nd[2];
+            const int4 n3 = reinterpret_cast<const int4 *>(nd)[3];
+            float t0, t1;
+            const bool h0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, inv, tmin, hit.t, t0);
+            const bool h1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, inv, tmin, hit.t, t1);
+            if (h0 && h1) {
+                int near = n3.x, far = n3.y;
+                if (t1 < t0) {
+                    near = n3.y;
+                    far = n3.x;
+                }
+                if (st.sp >= kStackSize) {
+                    report_traversal_bounds(bvh);
+                    return hit;
+                }
+                st.push((unsigned)far, lm);
+                link = near;
+            } else if (h0) {
+                link = n3.x;
+            } else if (h1) {
+                link = n3.y;
+            } else {
+                link = st.empty() ? kSentinel : (int)st.pop(lm);
+            }
+        }
+        if (link == kSentinel) break;
+        const int code = ~link;
+        const int first = code >> 4, count = code & 15;
+        if (first + count > bvh.num_tris) {
+            report_traversal_bounds(bvh);
+            return hit;
+        }
+        for (int k = 0; k < count; ++k) {
+            const int slot = first + k;
+            const float4 *tp = se + 3 * slot;
+            const float4 a = tp[0], b = tp[1], c = tp[2];
+            const bool acc = intersect_triangle_e<true>(o, d, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z),
+                                                        slot, hit);
+            if (kEarlyExit && acc && hit.t < t_exit) return hit;
+        }
+        link = st.empty() ? kSentinel : (int)st.pop(lm);
+    }
+    return hit;
+}
+
+// Copies the interior nodes and the triangles as (v0, e1, e2) records into
+// s_tree (the caller synchronises the block afterwards).
+__device__ __forceinline__ void tiny_fill(float4 *s_tree, const BvhView &bvh) {
+    const int nn = 4 * bvh.num_nodes;
+    for (int k = threadIdx.x; k < nn; k += blockDim.x) s_tree[k] = __ldg(bvh.nodes + k);
+    for (int k = threadIdx.x; k < bvh.num_tris; k += blockDim.x) {
+        const float4 a = __ldg(bvh.tris + 3 * k), b = __ldg(bvh.tris + 3 * k + 1), c = __ldg(bvh.tris + 3 * k + 2);
+        s_tree[nn + 3 * k] = a;
+        s_tree[nn + 3 * k + 1] = make_float4(rsub(b.x, a.x), rsub(b.y, a.y), rsub(b.z, a.z), 0.f);
+        s_tree[nn + 3 * k + 2] = make_float4(rsub(c.x, a.x), rsub(c.y, a.y), rsub(c.z, a.z), 0.f);
+    }
+}
+
+// Grid-stride over the batch (one ray per thread when the grid covers it);
+// kShort > 0 keeps the top kShort stack entries per lane in shared memory.
+template <class Job, bool kEarlyExit, int kShort>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_tiny(Job job, int n) {
+    extern __shared__ float4 s_tree[];
+    __shared__ unsigned s_stack[kShort > 0 ? kShort * kTraceBlock : 1];
+    const BvhView &bvh = job.bvh;
+    const int nn = 4 * bvh.num_nodes;
+    tiny_fill(s_tree, bvh);
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+        const int i = (int)r;
+        BvhView b;
+        V3 o, d;
+        float tmin, tmax, t_exit;
+        job.setup(i, b, o, d, tmin, tmax, t_exit);
+        Hit h;
+        if constexpr (kShort > 0) {
+            ShortStack<kShort> st;
+            st.col = s_stack + threadIdx.x;
+            st.stride = blockDim.x;
+            h = closest_hit_tiny<kEarlyExit>(s_tree, s_tree + nn, b, st, o, d, tmin, tmax, t_exit);
+        } else {
+            LocalStack st;
+            h = closest_hit_tiny<kEarlyExit>(s_tree, s_tree + nn, b, st, o, d, tmin, tmax, t_exit);
+        }
+        job.finish(i, b, h);
+    }
+}
+
+// Launches k_trace_tiny over n rays: one ray per thread (persistent false)
+// or a grid of all SMs at full occupancy.
+template <class Job, bool kEarlyExit, int kShort>
+static void launch_tiny(const Job &job, int64_t n, bool persistent, cudaStream_t s) {
+    const int smem = (int)tiny_bytes(job.bvh);
+    const void *kernel = (const void *)k_trace_tiny<Job, kEarlyExit, kShort>;
+    int64_t blocks = (n + kTraceBlock - 1) / kTraceBlock;
+    if (persistent) {
+        static int sms = 0;
+        if (!sms) {
+            int dev;
+            CRT_CUDA(cudaGetDevice(&dev));
+            CRT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        }
+        int per = 0;
+        CRT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kTraceBlock, smem));
+        blocks = std::min<int64_t>(blocks, (int64_t)sms * std::max(1, per));
+    }
+    k_trace_tiny<Job, kEarlyExit, kShort><<<(int)blocks, kTraceBlock, smem, s>>>(job, (int)n);
+}
+
 // Light::Visible in two passes (ShadowJob2), local stack, for at least
 // kMinBlocks resident blocks per SM (1: no register cap).
 template <int kMinBlocks>
@@ -284,12 +426,26 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8r(BvhView bvh, con
 // 28 / 216 = binary tree, top 8 / 16 stack entries per lane in shared
 // memory; 8 / 82 = 8-wide quantised tree (built only with CRT_BVH8=1),
 // 16 / 8 shared-memory entries; 83 = the same as 8 with the visited node's
-// links kept in registers.
+// links kept in registers; 11 / 12 / 13 = the tree in shared memory
+// (k_trace_tiny, scenes of at most kTinyBytes, else 2): one ray per thread
+// with the local stack / a persistent grid with the local stack / one ray
+// per thread with 8 stack entries per lane in shared memory. On the Cornell
+// box (36 triangles, 1M random rays) 11 issues from 85% of the scheduler
+// slots with 11-12 of 32 lanes active: divergence between the lanes'
+// paths, not memory, bounds it. Capping it at 40 / 32 registers (12 / 16
+// blocks per SM), and binning each block's rays by direction and origin
+// octant before tracing them, measured 8-20% and 2-10% slower.
 constexpr int kTraceVariant = 2;
+constexpr int kTinyVariant = 11;
 
-static int traversal_variant() {
+static int traversal_variant(const BvhView &bvh) {
     const char *e = getenv("CRT_TRAVERSAL");
-    return e ? atoi(e) : kTraceVariant;
+    const bool tiny = tiny_bytes(bvh) <= kTinyBytes;
+    int v = e ? atoi(e) : (tiny ? kTinyVariant : kTraceVariant);
+    if ((v == 8 || v == 82 || v == 83) && !bvh.wnodes) v = 2;
+    if ((v == 4 || v == 416) && !bvh.cnodes) v = 2;
+    if (v >= 11 && v <= 13 && !tiny) v = 2;
+    return v;
 }
 
 // Persistent grid (all SMs at full occupancy), fewer blocks for small
@@ -303,10 +459,14 @@ static int trace_grid(const void *kernel, int64_t n) {
 void launch_trace_closest(const BvhView &bvh, const float4 *d_rays, int64_t n, float4 *d_hits, cudaStream_t s) {
     if (n <= 0) return;
     CRT_CHECK(n < (int64_t)1 << 31, CRT_ERR_CAPACITY, "trace batch larger than 2^31 rays");
-    int v = traversal_variant();
-    if ((v == 8 || v == 82 || v == 83) && !bvh.wnodes) v = 2;
-    if ((v == 4 || v == 416) && !bvh.cnodes) v = 2;
-    if (v == 4)
+    const int v = traversal_variant(bvh);
+    if (v >= 11 && v <= 13) {
+        const ClosestJob job{bvh, d_rays, d_hits};
+        if (v == 13)
+            launch_tiny<ClosestJob, false, 8>(job, n, false, s);
+        else
+            launch_tiny<ClosestJob, false, 0>(job, n, v == 12, s);
+    } else if (v == 4)
         k_trace_closest_q<<<trace_grid((const void *)k_trace_closest_q, n), kTraceBlock, 0, s>>>(bvh, d_rays, (int)n,
                                                                                                 d_hits);
     else if (v == 416)
@@ -355,10 +515,14 @@ void launch_trace_shadow(const BvhView &bvh, const float *d_q, int64_t n, uint8_
     if (n <= 0) return;
     CRT_CHECK(n < (int64_t)1 << 31, CRT_ERR_CAPACITY, "trace batch larger than 2^31 queries");
     const float4 *q = reinterpret_cast<const float4 *>(d_q);
-    int v = traversal_variant();
-    if ((v == 8 || v == 82 || v == 83) && !bvh.wnodes) v = 2;
-    if ((v == 4 || v == 416) && !bvh.cnodes) v = 2;
-    if (v == 4)
+    const int v = traversal_variant(bvh);
+    if (v >= 11 && v <= 13) {
+        const ShadowJob job{bvh, q, d_occ, {}};
+        if (v == 13)
+            launch_tiny<ShadowJob, true, 8>(job, n, false, s);
+        else
+            launch_tiny<ShadowJob, true, 0>(job, n, v == 12, s);
+    } else if (v == 4)
         k_trace_shadow_q<<<trace_grid((const void *)k_trace_shadow_q, n), kTraceBlock, 0, s>>>(bvh, q, (int)n, d_occ);
     else if (v == 416)
         k_trace_shadow_s<16, true><<<trace_grid((const void *)k_trace_shadow_s<16, true>, n), kTraceBlock, 0, s>>>(

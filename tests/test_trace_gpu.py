@@ -174,3 +174,30 @@ def test_traversal_variants_agree(crt_ctx, ico_tris, variant, monkeypatch):
     assert_hits_match(h, base_h, ico_tris, rays)
     assert (o != base_o).sum() <= 2
     sc.close()
+
+
+@pytest.mark.parametrize("variant", ["11", "12", "13"])
+@pytest.mark.parametrize("ntris", [1, 15, 36, 150, 300])
+def test_tiny_scene_variants_agree(crt_ctx, cornell_tris, variant, ntris, monkeypatch):
+    """The traversals over a tree copied into shared memory (scenes of at
+    most 32 KB of nodes and edge records: one ray per thread or a
+    persistent grid, stack in local or shared memory) visit the tree in the
+    binary traversal's order, so their hit records and shadow answers equal
+    its own bit for bit."""
+    if ntris == 36:
+        tris = cornell_tris
+    else:
+        rng = np.random.default_rng(ntris)
+        c = rng.uniform(-1, 1, (ntris, 1, 3))
+        tris = (c + rng.normal(0, 0.2, (ntris, 3, 3))).reshape(-1, 9).astype(np.float32)
+    rays = scenes.random_rays(tris, 100_003, seed=ntris + 1)
+    q = scenes.random_shadow_queries(tris, 100_003, seed=ntris + 2)
+    sc = Scene.from_triangles(crt_ctx, tris)
+    monkeypatch.setenv("CRT_TRAVERSAL", "2")
+    base_h, base_o = sc.trace_closest(rays), sc.trace_shadow(q)
+    monkeypatch.setenv("CRT_TRAVERSAL", variant)
+    h, o = sc.trace_closest(rays), sc.trace_shadow(q)
+    crt_ctx.check_device_errors()
+    np.testing.assert_array_equal(h.view(np.uint32), base_h.view(np.uint32))
+    np.testing.assert_array_equal(o, base_o)
+    sc.close()
