@@ -624,13 +624,13 @@ def kpcn_layers_leg(ctx, reps=10):
             "peak_tflops": peak}
 
 
-def denoise_leg(ctx, train_steps=3000):
+def denoise_leg(ctx, train_steps=6000):
     """Learned denoiser against SVGF (the learned-denoiser workload, at
     256x256 instead of 1920x1080 and 16-frame instead of 60-frame
     sequences so the 4096-spp references fit the bench): the KPCN is
     trained on the GPU on 64 views of seeded Cornell variants (scene seeds
     100-163, one view each, 1-16 spp inputs, 4096-spp references) for
-    3000 Adam steps of 8 random 128x128 crops. Test: one 16-frame orbit
+    6000 Adam steps of 8 random 128x128 crops. Test: one 16-frame orbit
     sequence (1.5 deg per frame) per unseen scene (seeds 200-207), relMSE
     of every frame against its 4096-spp reference for raw and KPCN at 1-32
     spp and for SVGF run temporally over the sequence at 1 and 64 spp.
@@ -770,6 +770,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true", help="skip timing the reference's own CUDA traversal")
     ap.add_argument("--no-cornell", action="store_true", help="skip the Cornell-box 1M+1M traversal leg")
+    ap.add_argument("--train-steps", type=int, default=6000, help="Adam steps of the denoise leg's KPCN training")
     ap.add_argument("--no-render", action="store_true", help="skip the full-frame render leg")
     ap.add_argument("--no-svgf", action="store_true", help="skip the 1080p SVGF leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view leg")
@@ -802,7 +803,7 @@ def main():
                 "render": lambda: render_leg(ctx, max(2, min(args.steps, 8)), stream,
                                              with_reference=not args.no_ref_cuda),
                 "cornell": lambda: cornell_trace_leg(ctx, stream, with_reference=not args.no_ref_cuda),
-                "serve": lambda: serve_leg(ctx), "denoise": lambda: denoise_leg(ctx)}
+                "serve": lambda: serve_leg(ctx), "denoise": lambda: denoise_leg(ctx, args.train_steps)}
         print(json.dumps({args.only: legs[args.only]()}))
         ctx.close()
         return
@@ -885,7 +886,7 @@ def main():
         serve = serve_leg(ctx)
     denoise = None
     if rank == 0 and not args.no_denoise:
-        denoise = denoise_leg(ctx)
+        denoise = denoise_leg(ctx, args.train_steps)
         denoise["conv"] = conv_leg(ctx)
         denoise["kpcn_1080p"] = kpcn_layers_leg(ctx)
 
