@@ -414,26 +414,29 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8r(BvhView bvh, con
     trace_dynamic8<true, kShort, ShadowJob, true>(job, n, s_stack);
 }
 
-// Traversal variant of the trace kernels (CRT_TRAVERSAL overrides the
-// default kTraceVariant): 2 = binary tree, stack in local memory
-// (210 / 212: the same capped at 51 / 42 registers for 10 / 12 blocks per SM;
-// 1: one ray per thread without refill; 3: with postponed leaves; 5 / 58:
-// with pipelined triangle loads (no
-// register cap / 8 blocks per SM); 6 / 68: shadow queries in two passes
-// (ShadowJob2; no register cap / 8 blocks per SM; extend as 2); 4 / 416: over
-// the 16-bit quantised nodes with
-// the stack in local / shared memory);
-// 28 / 216 = binary tree, top 8 / 16 stack entries per lane in shared
-// memory; 8 / 82 = 8-wide quantised tree (built only with CRT_BVH8=1),
-// 16 / 8 shared-memory entries; 83 = the same as 8 with the visited node's
-// links kept in registers; 11 / 12 / 13 = the tree in shared memory
-// (k_trace_tiny, scenes of at most kTinyBytes, else 2): one ray per thread
-// with the local stack / a persistent grid with the local stack / one ray
-// per thread with 8 stack entries per lane in shared memory. On the Cornell
-// box (36 triangles, 1M random rays) 11 issues from 85% of the scheduler
-// slots with 11-12 of 32 lanes active: divergence between the lanes'
-// paths, not memory, bounds it. Capping it at 40 / 32 registers (12 / 16
-// blocks per SM), and binning each block's rays by direction and origin
+// Traversal variant of the trace kernels. The default is kTinyVariant for
+// scenes of at most kTinyBytes and kTraceVariant otherwise; CRT_TRAVERSAL
+// overrides it.
+//   2        binary tree, stack in local memory, per-lane refill;
+//   210/212  the same capped at 51 / 42 registers (10 / 12 blocks per SM);
+//   1        one ray per thread without refill;
+//   3        postponed leaves;
+//   5/58     pipelined triangle loads (no register cap / 8 blocks per SM);
+//   6/68     shadow queries in two passes (ShadowJob2; no cap / 8 blocks per
+//            SM; extend as 2);
+//   4/416    the 16-bit quantised nodes, stack in local / shared memory;
+//   28/216   top 8 / 16 stack entries per lane in shared memory;
+//   8/82     8-wide quantised tree (built only with CRT_BVH8=1), 16 / 8
+//            shared-memory entries; 83 as 8 with the visited node's links
+//            in registers;
+//   11/12/13 the tree in shared memory (k_trace_tiny; scenes of at most
+//            kTinyBytes, else 2): one ray per thread with the local stack /
+//            a persistent grid / one ray per thread with 8 stack entries
+//            per lane in shared memory.
+// On the Cornell box (36 triangles, 1M random rays) 11 issues from 85% of
+// the scheduler slots with 11-12 of 32 lanes active: divergence between the
+// lanes' paths, not memory, bounds it. Capping it at 40 / 32 registers (12 /
+// 16 blocks per SM), and binning each block's rays by direction and origin
 // octant before tracing them, measured 8-20% and 2-10% slower.
 constexpr int kTraceVariant = 2;
 constexpr int kTinyVariant = 11;
