@@ -176,8 +176,16 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow_1(BvhView bvh, con
 // primitive index, e1 = v1 - v0, e2 = v2 - v0 rounded to nearest as the
 // triangle test forms them) of a scene of at most kTinyBytes are copied
 // into each block's shared memory once; the traversal then reads them there
-// (closest_hit's order, tests and bounds checks, so the same hits).
+// (closest_hit's order, tests and bounds checks, so the same hits). It is
+// the default up to kTinyDefaultBytes. Over 1M random rays + 1M shadow
+// queries (extend + shadow ms, against the refill traversal from global
+// memory) it is faster on trees of 1.1 KB (0.169 vs 0.218), 2.1 KB (the
+// Cornell box, 0.248 vs 0.286) and 8.9 KB (0.183 vs 0.203), and slower at
+// 9.6 KB (0.280 vs 0.253), 19.3 KB (0.234 vs 0.214) and 29.1 KB (0.323 vs
+// 0.256): each block's copy of the tree grows with it, and deeper trees
+// gain more from the refill loop.
 constexpr int kTinyBytes = 32 * 1024;
+constexpr int kTinyDefaultBytes = 8 * 1024;
 
 static int64_t tiny_bytes(const BvhView &bvh) {
     return ((int64_t)4 * bvh.num_nodes + (int64_t)3 * bvh.num_tris) * (int64_t)sizeof(float4);
@@ -415,8 +423,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_shadow8r(BvhView bvh, con
 }
 
 // Traversal variant of the trace kernels. The default is kTinyVariant for
-// scenes of at most kTinyBytes and kTraceVariant otherwise; CRT_TRAVERSAL
-// overrides it.
+// scenes of at most kTinyDefaultBytes and kTraceVariant otherwise;
+// CRT_TRAVERSAL overrides it.
 //   2        binary tree, stack in local memory, per-lane refill;
 //   210/212  the same capped at 51 / 42 registers (10 / 12 blocks per SM);
 //   1        one ray per thread without refill;
@@ -443,8 +451,9 @@ constexpr int kTinyVariant = 11;
 
 static int traversal_variant(const BvhView &bvh) {
     const char *e = getenv("CRT_TRAVERSAL");
-    const bool tiny = tiny_bytes(bvh) <= kTinyBytes;
-    int v = e ? atoi(e) : (tiny ? kTinyVariant : kTraceVariant);
+    const int64_t tb = tiny_bytes(bvh);
+    const bool tiny = tb <= kTinyBytes;
+    int v = e ? atoi(e) : (tb <= kTinyDefaultBytes ? kTinyVariant : kTraceVariant);
     if ((v == 8 || v == 82 || v == 83) && !bvh.wnodes) v = 2;
     if ((v == 4 || v == 416) && !bvh.cnodes) v = 2;
     if (v >= 11 && v <= 13 && !tiny) v = 2;

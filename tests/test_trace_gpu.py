@@ -177,7 +177,7 @@ def test_traversal_variants_agree(crt_ctx, ico_tris, variant, monkeypatch):
 
 
 @pytest.mark.parametrize("variant", ["11", "12", "13"])
-@pytest.mark.parametrize("ntris", [1, 15, 36, 150, 300])
+@pytest.mark.parametrize("ntris", [1, 15, 36, 100, 150, 300])
 def test_tiny_scene_variants_agree(crt_ctx, cornell_tris, variant, ntris, monkeypatch):
     """The traversals over a tree copied into shared memory (scenes of at
     most 32 KB of nodes and edge records: one ray per thread or a
